@@ -1,0 +1,158 @@
+"""ctypes binding of libhv_b200.so (the C ABI declared in include/hv_b200.h).
+
+Loading fails loudly when the library has not been built: there is no CPU
+fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libhv_b200.so")
+
+HV_OK = 0
+HV_ERR_BAD_ARG = 1
+HV_ERR_CUDA = 2
+HV_ERR_NOT_CONVERGED = 3
+HV_ERR_NO_DEVICE = 4
+HV_ERR_OOM = 5
+HV_ERR_TIMEOUT = 6
+HV_ERR_UNSUPPORTED = 7
+HV_ERR_NONFINITE = 8
+
+HV_F64 = 0
+HV_F32 = 1
+HV_DEPOSIT_ATOMIC = 0
+HV_DEPOSIT_SORTED = 1
+HV_SOR_MAX_UPDATE = 0
+HV_SOR_REL_RESIDUAL = 1
+HV_PATH_PLAIN = 0
+HV_PATH_FUSED = 1
+
+HV_FIELD_DENSITY_RAW = 0
+HV_FIELD_DENSITY = 1
+HV_FIELD_POTENTIAL = 2
+HV_FIELD_COULOMB = 3
+HV_FIELD_FORCE_X = 4
+HV_FIELD_FORCE_Y = 5
+HV_FIELD_FORCE_Z = 6
+
+HV_PART = {"x": 0, "y": 1, "z": 2, "kx": 3, "ky": 4, "kz": 5, "fx": 6, "fy": 7, "fz": 8}
+HV_OBS_SOR_NOT_CONVERGED = 1
+
+
+class hv_world(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("d_max", C.c_double * 3)]
+
+
+class hv_skyrme(C.Structure):
+    _fields_ = [("A", C.c_double), ("B", C.c_double), ("C", C.c_double), ("gamma", C.c_double)]
+
+
+class hv_sor_params(C.Structure):
+    _fields_ = [("omega", C.c_double), ("tol", C.c_double), ("criterion", C.c_int), ("max_iter", C.c_int)]
+
+
+class hv_run_params(C.Structure):
+    _fields_ = [
+        ("z", C.c_int), ("n", C.c_int), ("part_per_nucleon", C.c_int),
+        ("sigma_r", C.c_double), ("dt", C.c_double), ("t_exc", C.c_double), ("eta_exc", C.c_double),
+        ("skyrme", hv_skyrme), ("sor", hv_sor_params), ("deposit_mode", C.c_int),
+    ]
+
+
+class hv_observables(C.Structure):
+    _fields_ = [
+        ("t", C.c_double), ("rms_p", C.c_double), ("rms_n", C.c_double),
+        ("zcm_p", C.c_double), ("zcm_n", C.c_double), ("dipole", C.c_double),
+        ("sor_iterations", C.c_int), ("flags", C.c_int),
+    ]
+
+
+OBS_DTYPE = np.dtype([
+    ("t", "f8"), ("rms_p", "f8"), ("rms_n", "f8"), ("zcm_p", "f8"), ("zcm_n", "f8"),
+    ("dipole", "f8"), ("sor_iterations", "i4"), ("flags", "i4"),
+])
+assert OBS_DTYPE.itemsize == C.sizeof(hv_observables)
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_S = C.c_int  # hv_status
+
+# name -> (restype, argtypes); every name here must be declared in include/hv_b200.h
+SIGNATURES = {
+    "hv_version": (C.c_char_p, []),
+    "hv_status_string": (C.c_char_p, [_S]),
+    "hv_last_error": (C.c_char_p, []),
+    "hv_device_count": (_I, []),
+    "hv_sor_reference_defaults": (None, [_P]),
+    "hv_skyrme_from_t0t3": (None, [_D, _D, _D, _D, _P]),
+    "hv_generate_nucleus_f64": (_S, [C.c_uint64, _I, _I, _D, _D, _P, _P, _P, _P, _P, _P]),
+    "hv_generate_nucleus_f32": (_S, [C.c_uint64, _I, _I, _D, _D, _P, _P, _P, _P, _P, _P]),
+    "hv_ctx_create": (_S, [_P, _I, _I, _I, _P, _I, _P]),
+    "hv_ctx_destroy": (_S, [_P]),
+    "hv_ctx_set_params": (_S, [_P, _P]),
+    "hv_ctx_get_params": (_S, [_P, _P]),
+    "hv_ctx_stream": (_P, [_P]),
+    "hv_ctx_synchronize": (_S, [_P]),
+    "hv_upload_particles": (_S, [_P, _P, _P, _P, _P, _P, _P]),
+    "hv_download_particles": (_S, [_P, _P, _P, _P, _P, _P, _P]),
+    "hv_upload_particle_array": (_S, [_P, _I, _P]),
+    "hv_download_particle_array": (_S, [_P, _I, _P]),
+    "hv_upload_field": (_S, [_P, _I, _P]),
+    "hv_download_field": (_S, [_P, _I, _P]),
+    "hv_field_device_ptr": (_S, [_P, _I, _P]),
+    "hv_deposit_cic": (_S, [_P]),
+    "hv_smooth_density": (_S, [_P]),
+    "hv_skyrme_potential": (_S, [_P]),
+    "hv_coulomb_boundary": (_S, [_P]),
+    "hv_coulomb_sor": (_S, [_P, _P, _P]),
+    "hv_merge_potentials": (_S, [_P]),
+    "hv_forces_fdm": (_S, [_P]),
+    "hv_gather_cic": (_S, [_P]),
+    "hv_kick_half": (_S, [_P, _D]),
+    "hv_drift": (_S, [_P, _D]),
+    "hv_excite": (_S, [_P, _D]),
+    "hv_observe": (_S, [_P, _P]),
+    "hv_initial_solve": (_S, [_P, _P]),
+    "hv_run": (_S, [_P, _I, _I, _P]),
+    "hv_simulate": (_S, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+}
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Loads and types the library once; raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"libhv_b200.so not built ({p}); run python hyper-vlasov_b200/build.py")
+    lib = C.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class HVError(RuntimeError):
+    def __init__(self, status, where=""):
+        lib = load()
+        msg = lib.hv_status_string(status).decode()
+        detail = lib.hv_last_error().decode()
+        super().__init__(f"{where}: {msg} ({status})" + (f" [{detail}]" if detail else ""))
+        self.status = status
+
+
+def check(status, where=""):
+    if status != HV_OK:
+        raise HVError(status, where)
+    return status

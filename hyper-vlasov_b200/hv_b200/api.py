@@ -1,0 +1,214 @@
+"""Python mirror of the reference's step interface over libhv_b200.so.
+
+``Session`` owns one device context (one nucleus on one GPU).  Its methods are
+the reference's routines, in the reference's vocabulary:
+
+=============================  =============================================
+Session method                 reference routine
+=============================  =============================================
+deposit()                      distribute_volumetric_particles_cic (tools.hpp:35-96)
+smooth()                       compute_volumetric_densities (physics.hpp:202-234)
+skyrme()                       compute_volumetric_skyrme_potentials (physics.hpp:272-281)
+coulomb_boundary()             set_initial_coulomb_boundaries (tools.hpp:283-300)
+coulomb_sor()                  compute_volumetric_coulomb_potentials_sor (physics.hpp:99-157)
+merge()                        merge_volumetric_potentials (tools.hpp:377-384)
+forces()                       compute_volumetric_forces_fdm (physics.hpp:159-200)
+gather()                       distribute_forces_to_particles_cic (tools.hpp:98-168)
+kick_half(dt) / drift(dt)      update_momenta_half / update_positions_full (physics.hpp:248-270)
+excite(eta)                    nuclear_excitation (physics.hpp:236-246)
+observe()                      center_of_mass / mean_squared_radius (tools.hpp:302-338)
+initial_solve() / run(steps)   cpu_simulate (src/hyper_vlasov.cpp:32-104)
+=============================  =============================================
+
+Arrays are numpy; the element type follows the session precision (float64 for
+HV_F64, float32 for HV_F32).  Errors raise ``HVError``; nothing falls back to
+the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .workloads import Workload
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def generate_nucleus(seed, protons, neutrons, radius, k_fermi, dtype=np.float64):
+    """Seeded synthetic nucleus (hv_generate_nucleus_*): six arrays x..kz."""
+    lib = L.load()
+    dt = np.dtype(dtype)
+    total = protons + neutrons
+    arrs = [np.zeros(total, dt) for _ in range(6)]
+    f = lib.hv_generate_nucleus_f64 if dt == np.float64 else lib.hv_generate_nucleus_f32
+    L.check(f(seed, protons, neutrons, radius, k_fermi, *[_p(a) for a in arrs]), "hv_generate_nucleus")
+    return arrs
+
+
+def workload_particles(w: Workload, dtype=np.float64):
+    return generate_nucleus(w.seed, w.protons, w.neutrons, w.radius, w.k_fermi, dtype)
+
+
+class Session:
+    """One hv_ctx: device-resident particles and fields of one run."""
+
+    def __init__(self, world: L.hv_world, protons: int, neutrons: int, params: L.hv_run_params,
+                 precision: int = L.HV_F64, device: int = -1):
+        self.lib = L.load()
+        self.world = world
+        self.protons, self.neutrons = protons, neutrons
+        self.total = protons + neutrons
+        self.precision = precision
+        self.dtype = np.dtype(np.float64 if precision == L.HV_F64 else np.float32)
+        self.G = world.n[0] * world.n[1] * world.n[2]
+        self._ctx = C.c_void_p()
+        L.check(self.lib.hv_ctx_create(C.byref(world), protons, neutrons, precision, C.byref(params), device,
+                                       C.byref(self._ctx)), "hv_ctx_create")
+        self.params = params
+
+    @classmethod
+    def from_workload(cls, w: Workload, precision=L.HV_F64, device=-1):
+        return cls(w.world(), w.protons, w.neutrons, w.run_params(), precision, device)
+
+    # -- lifetime ----------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            self.lib.hv_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    def set_params(self, params: L.hv_run_params):
+        L.check(self.lib.hv_ctx_set_params(self._ctx, C.byref(params)), "hv_ctx_set_params")
+        self.params = params
+
+    def synchronize(self):
+        L.check(self.lib.hv_ctx_synchronize(self._ctx), "hv_ctx_synchronize")
+
+    # -- transfers ----------------------------------------------------------
+    def _as(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        if a.size != self.total:
+            raise ValueError(f"expected {self.total} elements, got {a.size}")
+        return a
+
+    def upload_particles(self, x, y, z, kx, ky, kz):
+        arrs = [None if a is None else self._as(a) for a in (x, y, z, kx, ky, kz)]
+        L.check(self.lib.hv_upload_particles(self._ctx, *[_p(a) for a in arrs]), "hv_upload_particles")
+
+    def download_particles(self):
+        arrs = [np.empty(self.total, self.dtype) for _ in range(6)]
+        L.check(self.lib.hv_download_particles(self._ctx, *[_p(a) for a in arrs]), "hv_download_particles")
+        return arrs
+
+    def upload_array(self, name, a):
+        a = self._as(a)
+        L.check(self.lib.hv_upload_particle_array(self._ctx, L.HV_PART[name], _p(a)), "hv_upload_particle_array")
+
+    def download_array(self, name):
+        a = np.empty(self.total, self.dtype)
+        L.check(self.lib.hv_download_particle_array(self._ctx, L.HV_PART[name], _p(a)), "hv_download_particle_array")
+        return a
+
+    def _field_len(self, field):
+        return self.G if field == L.HV_FIELD_COULOMB else 2 * self.G
+
+    def upload_field(self, field, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        if a.size != self._field_len(field):
+            raise ValueError("field size")
+        L.check(self.lib.hv_upload_field(self._ctx, field, _p(a)), "hv_upload_field")
+
+    def download_field(self, field):
+        a = np.empty(self._field_len(field), self.dtype)
+        L.check(self.lib.hv_download_field(self._ctx, field, _p(a)), "hv_download_field")
+        return a
+
+    # -- routines ------------------------------------------------------------
+    def deposit(self):
+        L.check(self.lib.hv_deposit_cic(self._ctx), "hv_deposit_cic")
+
+    def smooth(self):
+        L.check(self.lib.hv_smooth_density(self._ctx), "hv_smooth_density")
+
+    def skyrme(self):
+        L.check(self.lib.hv_skyrme_potential(self._ctx), "hv_skyrme_potential")
+
+    def coulomb_boundary(self):
+        L.check(self.lib.hv_coulomb_boundary(self._ctx), "hv_coulomb_boundary")
+
+    def coulomb_sor(self, allow_not_converged=False):
+        it = C.c_int(0)
+        m = C.c_double(0.0)
+        st = self.lib.hv_coulomb_sor(self._ctx, C.byref(it), C.byref(m))
+        if st == L.HV_ERR_NOT_CONVERGED and allow_not_converged:
+            return it.value, m.value, False
+        L.check(st, "hv_coulomb_sor")
+        return it.value, m.value, True
+
+    def merge(self):
+        L.check(self.lib.hv_merge_potentials(self._ctx), "hv_merge_potentials")
+
+    def forces(self):
+        L.check(self.lib.hv_forces_fdm(self._ctx), "hv_forces_fdm")
+
+    def gather(self):
+        L.check(self.lib.hv_gather_cic(self._ctx), "hv_gather_cic")
+
+    def kick_half(self, dt):
+        L.check(self.lib.hv_kick_half(self._ctx, float(dt)), "hv_kick_half")
+
+    def drift(self, dt):
+        L.check(self.lib.hv_drift(self._ctx, float(dt)), "hv_drift")
+
+    def excite(self, eta):
+        L.check(self.lib.hv_excite(self._ctx, float(eta)), "hv_excite")
+
+    def observe(self):
+        o = L.hv_observables()
+        L.check(self.lib.hv_observe(self._ctx, C.byref(o)), "hv_observe")
+        return o
+
+    def initial_solve(self):
+        it = C.c_int(0)
+        L.check(self.lib.hv_initial_solve(self._ctx, C.byref(it)), "hv_initial_solve")
+        return it.value
+
+    def run(self, steps, path=L.HV_PATH_PLAIN):
+        obs = np.zeros(steps, L.OBS_DTYPE)
+        L.check(self.lib.hv_run(self._ctx, steps, path, C.c_void_p(obs.ctypes.data)), "hv_run")
+        return obs
+
+
+def simulate(w: Workload, x, y, z, kx, ky, kz, steps, precision=L.HV_F64, path=L.HV_PATH_PLAIN):
+    """hv_simulate: the whole GPU run with host buffers (advanced in place).
+    Returns the per-step observables."""
+    lib = L.load()
+    dt = np.dtype(np.float64 if precision == L.HV_F64 else np.float32)
+    arrs = (x, y, z, kx, ky, kz)
+    for a in arrs:
+        if a.dtype != dt or not a.flags.c_contiguous:
+            raise ValueError("particle arrays must be contiguous and match the precision")
+    obs = np.zeros(steps, L.OBS_DTYPE)
+    world, params = w.world(), w.run_params()
+    L.check(lib.hv_simulate(C.byref(world), w.protons, w.neutrons, precision, C.byref(params), path, steps,
+                            *[_p(a) for a in arrs], C.c_void_p(obs.ctypes.data)), "hv_simulate")
+    return obs

@@ -1,0 +1,128 @@
+"""Named synthetic workloads of the hyper-vlasov hot path.
+
+Each workload is a nucleus, a test-particle count, a box-centred cubic grid and
+a time step, with the Skyrme/Coulomb settings of the 40Ca definition below
+(t0 = -2645 MeV fm^3, t3 = 15595 MeV fm^(3+3 sigma), sigma = 1/6, a_sym = 32 MeV,
+SOR omega = 1.8 to relative residual 1e-6, dipole boost of 30 MeV/c, seed 0).
+Positions are uniform in a ball of radius 1.2 A^(1/3) fm and wavenumbers
+uniform in a ball of k_F = (3 pi^2 rho_q / 2)^(1/3) with rho_q = 0.08 fm^-3.
+
+The smoothing width is the reference's default FWHM of 1.444 fm
+(auto_compute.py:54), sigma_r = FWHM / (2 sqrt(2 ln 2)) (physics_formulas.hpp:59-63).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field, replace
+
+from . import _lib as L
+
+HBAR_C = 197.33
+RHO0 = 0.16
+
+
+def sigma_from_fwhm(fwhm: float) -> float:
+    return fwhm / (2.0 * math.sqrt(2.0 * math.log(2.0)))
+
+
+@dataclass
+class Workload:
+    name: str
+    Z: int
+    N: int
+    ppn: int
+    n: int            # grid nodes per axis
+    h: float          # grid spacing (fm); d_max = n h / 2
+    dt: float         # fm/c
+    steps: int
+    seed: int = 0
+    t0: float = -2645.0
+    t3: float = 15595.0
+    sigma: float = 1.0 / 6.0
+    a_sym: float = 32.0
+    boost_mev: float = 30.0
+    t_exc: float = 0.0
+    sigma_r: float = field(default_factory=lambda: sigma_from_fwhm(1.444))
+    sor_omega: float = 1.8
+    sor_tol: float = 1e-6
+    sor_criterion: int = L.HV_SOR_REL_RESIDUAL
+    sor_max_iter: int = 20000
+    deposit_mode: int = L.HV_DEPOSIT_ATOMIC
+
+    @property
+    def A_nucleons(self) -> int:
+        return self.Z + self.N
+
+    @property
+    def protons(self) -> int:
+        return self.Z * self.ppn
+
+    @property
+    def neutrons(self) -> int:
+        return self.N * self.ppn
+
+    @property
+    def particles(self) -> int:
+        return self.protons + self.neutrons
+
+    @property
+    def radius(self) -> float:
+        return 1.2 * self.A_nucleons ** (1.0 / 3.0)
+
+    @property
+    def k_fermi(self) -> float:
+        return (3.0 * math.pi ** 2 * 0.08 / 2.0) ** (1.0 / 3.0)
+
+    @property
+    def d_max(self) -> float:
+        return self.n * self.h / 2.0
+
+    @property
+    def G(self) -> int:
+        return self.n ** 3
+
+    @property
+    def eta(self) -> float:
+        """Dipole boost in fm^-1 (nuclear_excitation, include/physics.hpp:236-246)."""
+        return self.boost_mev / HBAR_C
+
+    def skyrme(self):
+        """(A, B, C, gamma) of Skyrme<T> from (t0, t3, sigma, a_sym)."""
+        A = 0.75 * self.t0 * RHO0
+        B = (self.sigma + 2.0) / 16.0 * self.t3 * RHO0 ** (self.sigma + 1.0)
+        return A, B, self.a_sym, self.sigma + 1.0
+
+    def world(self) -> L.hv_world:
+        w = L.hv_world()
+        for a in range(3):
+            w.n[a] = self.n
+            w.d_max[a] = self.d_max
+        return w
+
+    def world_tuple(self):
+        return ((self.n,) * 3, (self.d_max,) * 3)
+
+    def run_params(self) -> L.hv_run_params:
+        p = L.hv_run_params()
+        p.z, p.n, p.part_per_nucleon = self.Z, self.N, self.ppn
+        p.sigma_r, p.dt, p.t_exc, p.eta_exc = self.sigma_r, self.dt, self.t_exc, self.eta
+        A, B, Cc, g = self.skyrme()
+        p.skyrme = L.hv_skyrme(A, B, Cc, g)
+        p.sor = L.hv_sor_params(self.sor_omega, self.sor_tol, self.sor_criterion, self.sor_max_iter)
+        p.deposit_mode = self.deposit_mode
+        return p
+
+    def with_reference_sor(self):
+        """The reference's hard-wired SOR: omega 1.5, max|dphi| < 1e-4, 512
+        iterations (include/physics.hpp:103-104,152)."""
+        return replace(self, sor_omega=1.5, sor_tol=1e-4, sor_criterion=L.HV_SOR_MAX_UPDATE, sor_max_iter=512)
+
+
+# 40Ca, 100 test particles per nucleon, 32^3, h = 1 fm, dt = 0.5 fm/c, 200 steps
+CA40_SMALL = Workload("40Ca-4k-32^3", Z=20, N=20, ppn=100, n=32, h=1.0, dt=0.5, steps=200)
+# 208Pb, 500 per nucleon (104,000 particles), 64^3, h = 0.5 fm, dt = 0.25, 2000 steps
+PB208_104K = Workload("208Pb-104k-64^3", Z=82, N=126, ppn=500, n=64, h=0.5, dt=0.25, steps=2000)
+# 208Pb, 10,000 per nucleon (2.08M particles), 128^3, h = 0.25 fm, dt = 0.2, 1000 steps
+PB208_2M = Workload("208Pb-2.08M-128^3", Z=82, N=126, ppn=10000, n=128, h=0.25, dt=0.2, steps=1000)
+
+WORKLOADS = {w.name: w for w in (CA40_SMALL, PB208_104K, PB208_2M)}

@@ -1,0 +1,293 @@
+/*
+ * hv_b200.h -- C ABI of the B200 (sm_100a) implementation of the hyper-vlasov
+ * per-step hot path.
+ *
+ * The reference (BanuDarius/hyper-vlasov) has no FFI: its surface is a set of
+ * C++ function templates over the POD structs of include/sim_structs.hpp,
+ * called in a fixed order by cpu_simulate (src/hyper_vlasov.cpp:32-118), with
+ * an empty GPU slot gpu_simulate (src/hyper_vlasov.cpp:120-123).  Every entry
+ * point below replaces one of those routines (cited per function) and keeps
+ * its argument roles.  The C++ header hv_b200.hpp wraps these entry points
+ * with the reference's own call shapes (TestParticles<T>*, ScalarField<T>*,
+ * const World<T>& ...).
+ *
+ * Conventions
+ *  - Plain C types only.  Device buffers are owned by an hv_ctx; host buffers
+ *    are owned by the caller and are never retained after a call returns.
+ *  - Every function returns hv_status and never exits the process (the
+ *    reference prints and calls exit(1); include/init.hpp:94-96).
+ *  - All work of one context is ordered on the context's own CUDA stream.  A
+ *    context is not thread-safe; distinct contexts are independent.
+ *  - Particle arrays are structure-of-arrays with protons first, exactly as
+ *    TestParticles<T> (include/sim_structs.hpp:55-60).  Species grids are
+ *    stacked: protons at [0,G), neutrons at [G,2G), G = n[0]*n[1]*n[2], index
+ *    IDX(i,j,k) = (i*n[1] + j)*n[2] + k (include/sim_structs.hpp:38).
+ */
+#ifndef HV_B200_H
+#define HV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HV_API __attribute__((visibility("default")))
+#else
+#define HV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hv_status {
+    HV_OK = 0,
+    HV_ERR_BAD_ARG = 1,        /* invalid size, pointer or parameter            */
+    HV_ERR_CUDA = 2,           /* a CUDA runtime call failed                    */
+    HV_ERR_NOT_CONVERGED = 3,  /* SOR reached max_iter; fields are still written */
+    HV_ERR_NO_DEVICE = 4,      /* no usable sm_100 device                       */
+    HV_ERR_OOM = 5,            /* device allocation failed                      */
+    HV_ERR_TIMEOUT = 6,        /* a bounded device-side wait gave up            */
+    HV_ERR_UNSUPPORTED = 7,    /* combination of options not provided           */
+    HV_ERR_NONFINITE = 8       /* NaN/Inf detected in a checked quantity        */
+} hv_status;
+
+/* Arithmetic type of a context.  HV_F64 is the plain drop-in (the reference's
+ * default double instantiation); HV_F32 keeps particles, grids and stencils in
+ * float and uses double only for the SOR residual norm / convergence test, the
+ * Coulomb boundary monopole and the observable sums. */
+typedef enum hv_precision { HV_F64 = 0, HV_F32 = 1 } hv_precision;
+
+/* How the CIC deposit reduces contributions into the density grid. */
+typedef enum hv_deposit_mode {
+    HV_DEPOSIT_ATOMIC = 0,  /* warp-aggregated atomics; order not reproducible   */
+    HV_DEPOSIT_SORTED = 1   /* sort by cell, then per-node sum in particle-index
+                               order: deterministic and, in HV_F64, bit-identical
+                               to a single-threaded run of the reference         */
+} hv_deposit_mode;
+
+/* SOR stopping rule. */
+typedef enum hv_sor_criterion {
+    HV_SOR_MAX_UPDATE = 0,   /* stop when max|phi_new - phi_old| < tol over one
+                                red+black iteration (physics.hpp:152)            */
+    HV_SOR_REL_RESIDUAL = 1  /* stop when ||b + lap_h phi||_2 / ||b||_2 <= tol,
+                                b = 4*pi*1.44*rho_p on interior nodes (FP64)     */
+} hv_sor_criterion;
+
+/* How hv_run advances the state. */
+typedef enum hv_step_path {
+    HV_PATH_PLAIN = 0,  /* one kernel per reference routine, in cpu_simulate order,
+                           SOR convergence tested on the host each iteration     */
+    HV_PATH_FUSED = 1   /* fused particle kernel, fused field kernels, device-side
+                           SOR loop, whole step replayed from a CUDA graph       */
+} hv_step_path;
+
+/* World<T> (include/sim_structs.hpp:72-75).  Node i on axis a sits at
+ * d_max[a] * (2 i / n[a] - 1) (include/tools.hpp:394-401). */
+typedef struct hv_world {
+    int n[3];
+    double d_max[3];
+} hv_world;
+
+/* Skyrme<T> (include/sim_structs.hpp:82-84):
+ * U_q = A t + B t^gamma + 2 tau C (rho_n - rho_p)/rho0, t = rho/rho0,
+ * tau = -1 protons, +1 neutrons (include/physics_formulas.hpp:70-77). */
+typedef struct hv_skyrme {
+    double A, B, C, gamma;
+} hv_skyrme;
+
+/* Coulomb SOR controls.  The reference hard-codes omega = 1.5, tol = 1e-4,
+ * max_iter = 512 with HV_SOR_MAX_UPDATE (include/physics.hpp:103-104,152). */
+typedef struct hv_sor_params {
+    double omega;
+    double tol;
+    int criterion;   /* hv_sor_criterion */
+    int max_iter;
+} hv_sor_params;
+
+/* Parameters<T> fields that the step uses (include/sim_structs.hpp:49-53). */
+typedef struct hv_run_params {
+    int z, n;                 /* proton and neutron numbers of the nucleus     */
+    int part_per_nucleon;     /* test particles per nucleon                    */
+    double sigma_r;           /* Gaussian smoothing width (fm)                 */
+    double dt;                /* time step (fm/c); the reference uses t_f/steps */
+    double t_exc;             /* time of the one-shot dipole excitation (fm/c) */
+    double eta_exc;           /* excitation strength (fm^-1)                   */
+    hv_skyrme skyrme;
+    hv_sor_params sor;
+    int deposit_mode;         /* hv_deposit_mode                               */
+} hv_run_params;
+
+/* Fields held by a context.  Sizes: COULOMB has G nodes, all others 2G. */
+typedef enum hv_field {
+    HV_FIELD_DENSITY_RAW = 0,  /* CIC counts after the deposit                   */
+    HV_FIELD_DENSITY = 1,      /* smoothed density (fm^-3)                       */
+    HV_FIELD_POTENTIAL = 2,    /* mean-field potential U (MeV), Coulomb merged   */
+    HV_FIELD_COULOMB = 3,      /* Coulomb potential phi (MeV)                    */
+    HV_FIELD_FORCE_X = 4,      /* -dU/dx (MeV/fm)                                */
+    HV_FIELD_FORCE_Y = 5,
+    HV_FIELD_FORCE_Z = 6
+} hv_field;
+
+/* Particle arrays of TestParticles<T> that the step reads or writes. */
+typedef enum hv_particle_array {
+    HV_PART_X = 0, HV_PART_Y = 1, HV_PART_Z = 2,
+    HV_PART_KX = 3, HV_PART_KY = 4, HV_PART_KZ = 5,
+    HV_PART_FX = 6, HV_PART_FY = 7, HV_PART_FZ = 8
+} hv_particle_array;
+
+/* Per-step observables, one row per recorded step (src/hyper_vlasov.cpp:64-70
+ * writes t, rms_p, rms_n, zcm_p, zcm_n).  Sums are accumulated in double. */
+typedef struct hv_observables {
+    double t;
+    double rms_p, rms_n;   /* sqrt of mean_squared_radius (tools.hpp:302-325) */
+    double zcm_p, zcm_n;   /* center_of_mass (tools.hpp:327-338)              */
+    double dipole;         /* D = N Z / A (zcm_p - zcm_n) (scripts/programs.py:99) */
+    int sor_iterations;    /* SOR iterations spent in this step               */
+    int flags;             /* HV_OBS_* bits                                   */
+} hv_observables;
+
+/* hv_observables.flags: the step's SOR reached max_iter (the reference prints
+ * "SOR COULOMB DID NOT CONVERGE!" and carries on, include/physics.hpp:155-156). */
+#define HV_OBS_SOR_NOT_CONVERGED 1
+
+typedef struct hv_ctx hv_ctx;
+
+/* ---- library / device ------------------------------------------------- */
+
+/* Version string of the library. */
+HV_API const char *hv_version(void);
+/* Human-readable name of a status code. */
+HV_API const char *hv_status_string(hv_status s);
+/* Last CUDA error text recorded by this thread (empty if none). */
+HV_API const char *hv_last_error(void);
+/* Number of visible sm_100 devices (0 when none).  Never fails. */
+HV_API int hv_device_count(void);
+
+/* ---- defaults and parameter helpers ----------------------------------- */
+
+/* Fills *p with the reference's SOR controls (omega 1.5, |dphi| < 1e-4,
+ * 512 iterations; include/physics.hpp:103-104,152, sim_structs.hpp:36,45). */
+HV_API void hv_sor_reference_defaults(hv_sor_params *p);
+
+/* Skyrme coefficients from (t0, t3, sigma, a_sym):
+ * A = 3/4 t0 rho0, B = (sigma+2)/16 t3 rho0^(sigma+1), gamma = sigma+1,
+ * C = a_sym, with rho0 = 0.16 fm^-3 (include/sim_structs.hpp:34). */
+HV_API void hv_skyrme_from_t0t3(double t0, double t3, double sigma, double a_sym, hv_skyrme *out);
+
+/* Seeded synthetic nucleus (replaces initialize_particles,
+ * include/physics.hpp:34-97, which needs GSL).  std::mt19937_64(seed); each
+ * uniform is (draw >> 11) * 2^-53; coordinates are radius*(2u-1) with
+ * rejection to the open ball.  All positions are drawn first (protons first),
+ * then all wavenumbers, in the ball of radius k_fermi (fm^-1).  The _f32
+ * variant rounds the same double draws to float. */
+HV_API hv_status hv_generate_nucleus_f64(uint64_t seed, int protons, int neutrons,
+                                  double radius, double k_fermi,
+                                  double *x, double *y, double *z,
+                                  double *kx, double *ky, double *kz);
+HV_API hv_status hv_generate_nucleus_f32(uint64_t seed, int protons, int neutrons,
+                                  double radius, double k_fermi,
+                                  float *x, float *y, float *z,
+                                  float *kx, float *ky, float *kz);
+
+/* ---- context lifetime ------------------------------------------------- */
+
+/* Allocates the device state of one run: particles (TestParticles<T>,
+ * include/init.hpp:133-157) and the fields of cpu_simulate
+ * (src/hyper_vlasov.cpp:44-51).  Requires n[a] >= 3, d_max[a] > 0,
+ * protons, neutrons >= 0.  device < 0 selects the current device. */
+HV_API hv_status hv_ctx_create(const hv_world *world, int protons, int neutrons,
+                        hv_precision prec, const hv_run_params *params,
+                        int device, hv_ctx **out);
+HV_API hv_status hv_ctx_destroy(hv_ctx *ctx);
+/* Replaces the run parameters (sizes are fixed at creation). */
+HV_API hv_status hv_ctx_set_params(hv_ctx *ctx, const hv_run_params *params);
+HV_API hv_status hv_ctx_get_params(const hv_ctx *ctx, hv_run_params *out);
+/* The context's CUDA stream (a cudaStream_t). */
+HV_API void *hv_ctx_stream(hv_ctx *ctx);
+/* Blocks until all work queued on the context has finished. */
+HV_API hv_status hv_ctx_synchronize(hv_ctx *ctx);
+
+/* ---- host <-> device transfers (caller-owned host memory) ------------- */
+/* Element type of every host pointer is the context precision (double for
+ * HV_F64, float for HV_F32).  Particle counts are those given at creation. */
+
+/* Uploads x,y,z,kx,ky,kz (any may be NULL to keep the device copy). */
+HV_API hv_status hv_upload_particles(hv_ctx *ctx, const void *x, const void *y, const void *z,
+                              const void *kx, const void *ky, const void *kz);
+/* Downloads the particle arrays in the caller's original particle order. */
+HV_API hv_status hv_download_particles(hv_ctx *ctx, void *x, void *y, void *z,
+                                void *kx, void *ky, void *kz);
+HV_API hv_status hv_upload_particle_array(hv_ctx *ctx, int which, const void *host);
+HV_API hv_status hv_download_particle_array(hv_ctx *ctx, int which, void *host);
+HV_API hv_status hv_upload_field(hv_ctx *ctx, int field, const void *host);
+HV_API hv_status hv_download_field(hv_ctx *ctx, int field, void *host);
+/* Device address of a field (valid until hv_ctx_destroy). */
+HV_API hv_status hv_field_device_ptr(hv_ctx *ctx, int field, void **dev_ptr);
+
+/* ---- one entry per reference routine (device-resident state) ---------- */
+
+/* distribute_volumetric_particles_cic (include/tools.hpp:35-96):
+ * particles -> DENSITY_RAW, using params.deposit_mode. */
+HV_API hv_status hv_deposit_cic(hv_ctx *ctx);
+/* compute_volumetric_densities (include/physics.hpp:202-234):
+ * DENSITY_RAW -> DENSITY.  Same node-pair set (|r_i - r_j|^2 <= 16 sigma_r^2,
+ * zero padding) and normalisation 1/(ppn (2 pi sigma_r^2)^1.5). */
+HV_API hv_status hv_smooth_density(hv_ctx *ctx);
+/* compute_volumetric_skyrme_potentials (include/physics.hpp:272-281):
+ * DENSITY -> POTENTIAL. */
+HV_API hv_status hv_skyrme_potential(hv_ctx *ctx);
+/* set_initial_coulomb_boundaries (include/tools.hpp:283-300): writes
+ * phi = 1.44 Z / |r| on the six faces of COULOMB (evaluated in double). */
+HV_API hv_status hv_coulomb_boundary(hv_ctx *ctx);
+/* compute_volumetric_coulomb_potentials_sor (include/physics.hpp:99-157):
+ * red-black SOR on the interior of COULOMB, warm-started from its contents,
+ * source = proton DENSITY.  *iterations (may be NULL) receives the number of
+ * red+black iterations; *metric (may be NULL) the final value of the stopping
+ * quantity.  Returns HV_ERR_NOT_CONVERGED when max_iter was reached. */
+HV_API hv_status hv_coulomb_sor(hv_ctx *ctx, int *iterations, double *metric);
+/* merge_volumetric_potentials (include/tools.hpp:377-384): U_p += phi. */
+HV_API hv_status hv_merge_potentials(hv_ctx *ctx);
+/* compute_volumetric_forces_fdm (include/physics.hpp:159-200):
+ * POTENTIAL -> FORCE_{X,Y,Z}. */
+HV_API hv_status hv_forces_fdm(hv_ctx *ctx);
+/* distribute_forces_to_particles_cic (include/tools.hpp:98-168):
+ * FORCE_{X,Y,Z} -> particle fx,fy,fz (zero outside the grid). */
+HV_API hv_status hv_gather_cic(hv_ctx *ctx);
+/* update_momenta_half (include/physics.hpp:248-258): k += dt/(2 hbar c) f. */
+HV_API hv_status hv_kick_half(hv_ctx *ctx, double dt);
+/* update_positions_full (include/physics.hpp:260-270): x += dt hbar c/mc2 k. */
+HV_API hv_status hv_drift(hv_ctx *ctx, double dt);
+/* nuclear_excitation (include/physics.hpp:236-246): kz += eta N/A (protons),
+ * kz -= eta Z/A (neutrons), Z = params.z, N = params.n. */
+HV_API hv_status hv_excite(hv_ctx *ctx, double eta);
+/* center_of_mass (include/tools.hpp:327-338) and mean_squared_radius
+ * (include/tools.hpp:302-325) of both species, summed in double. */
+HV_API hv_status hv_observe(hv_ctx *ctx, hv_observables *out);
+
+/* ---- whole-step drivers ----------------------------------------------- */
+
+/* The initial field solve of cpu_simulate (src/hyper_vlasov.cpp:53-62):
+ * deposit, smooth, Coulomb boundary, Skyrme, SOR, merge, FDM, gather. */
+HV_API hv_status hv_initial_solve(hv_ctx *ctx, int *sor_iterations);
+
+/* Advances n_steps time steps of the cpu_simulate loop
+ * (src/hyper_vlasov.cpp:63-104): [excite at t >= t_exc, once] -> kick/2 ->
+ * drift -> deposit -> smooth -> Skyrme -> SOR -> merge -> FDM -> gather ->
+ * kick/2.  obs (may be NULL) receives n_steps rows, observed at the start of
+ * each step as the reference records them.  path selects hv_step_path. */
+HV_API hv_status hv_run(hv_ctx *ctx, int n_steps, int path, hv_observables *obs);
+
+/* The whole gpu_simulate slot (src/hyper_vlasov.cpp:120-123) with host
+ * buffers: uploads the particles, runs the initial solve and n_steps steps,
+ * downloads the final particles (in place) and n_steps observable rows.
+ * Element type of the particle pointers follows prec. */
+HV_API hv_status hv_simulate(const hv_world *world, int protons, int neutrons,
+                      hv_precision prec, const hv_run_params *params, int path,
+                      int n_steps, void *x, void *y, void *z,
+                      void *kx, void *ky, void *kz, hv_observables *obs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HV_B200_H */

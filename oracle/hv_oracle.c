@@ -1,0 +1,53 @@
+/*
+ * hv_oracle.c -- CPU restatement of the hyper-vlasov hot path.
+ * TEST INFRASTRUCTURE ONLY (see hv_oracle.h): the checker, never the product.
+ * Build: oracle/Makefile (gcc -std=c11 -O2 -ffp-contract=off -fopenmp).
+ */
+#include "hv_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* std::numbers::pi_v<T> (used via pi<T>, include/sim_structs.hpp:37) */
+#define ORC_PI 3.141592653589793238462643383279502884
+
+#define R double
+#define S d
+#define EXPR(v) exp(v)
+#define POWR(a, b) pow(a, b)
+#define SQRTR(v) sqrt(v)
+#define FABSR(v) fabs(v)
+#include "hv_oracle_impl.h"
+#undef R
+#undef S
+#undef EXPR
+#undef POWR
+#undef SQRTR
+#undef FABSR
+
+#define R float
+#define S f
+#define EXPR(v) expf(v)
+#define POWR(a, b) powf(a, b)
+#define SQRTR(v) sqrtf(v)
+#define FABSR(v) fabsf(v)
+#include "hv_oracle_impl.h"
+#undef R
+#undef S
+#undef EXPR
+#undef POWR
+#undef SQRTR
+#undef FABSR
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+/* OpenMP thread count of the restatement (no effect without OpenMP). */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
