@@ -7,7 +7,8 @@ Tolerances (max|gpu - ref| / max|ref|):
           exact node coordinates and <= 1e-14 otherwise; Skyrme <= 1e-15 (CUDA's
           pow and glibc's may differ in the last bit); atomic deposit <= 1e-14.
   HV_F32  as above where the operation order is the same (float rounding is
-          deterministic); Skyrme <= 2e-7, atomic deposit <= 1e-6.
+          deterministic); Skyrme <= 5e-7 (CUDA's powf and glibc's differ by a
+          few ulp), atomic deposit <= 1e-6.
 """
 from __future__ import annotations
 
@@ -80,7 +81,7 @@ def test_skyrme(hv, golden, fixture, prec, exact_grid):
         s.upload_field(1, g["rho"])
         s.skyrme()
         U = s.download_field(2)
-        assert max_rel(U, g["U"]) <= (1e-15 if prec == "f64" else 2e-7)
+        assert max_rel(U, g["U"]) <= (1e-15 if prec == "f64" else 5e-7)
 
 
 @pytest.mark.parametrize("fixture,prec,exact_grid", FIXTURES)
