@@ -1,0 +1,411 @@
+"""Throughput of the hyper-vlasov hot path on B200, in particle-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one time step of the 208Pb / 2.08M test particle / 128^3 (h = 0.25
+fm, dt = 0.2 fm/c) workload: CIC deposit, smoothing, Skyrme potential,
+red-black SOR Coulomb solve (omega 1.8 to relative residual 1e-6), forces,
+gather, leapfrog and the D(t) observables.  Inputs are synthetic (seeded
+uniform-sphere nucleus), resident on the device before timing.
+
+Our arm (default) prints one JSON line with:
+  value        particle-steps/s of K fused FP32 steps, CUDA events on the
+               context stream, max over ranks
+  e2e          the same metric through hv_simulate with pinned host buffers:
+               upload, initial solve, K steps, download of D(t) and particles
+  roofline     the dominant kernel (SOR) against measured HBM bandwidth, from
+               a per-kernel CUDA-event pass of the same steps
+  kernels      per-kernel device time, share and algorithmic GB/s
+  plain_f64    the plain FP64 drop-in (one kernel per reference routine,
+               host-tested SOR) on the same workload, and the D(t) agreement
+  cpu_baseline the reference's own routines on the host cores (rank 0, N=1)
+
+--impl reference times the reference's CPU step routines (compiled from its
+sources into oracle/_ref; the restated C oracle when that build is absent) on
+the same workload, a bounded number of steps.
+
+With torchrun (N > 1) every rank runs an independent replica of the workload
+(weak scaling; the path does not shard), timed between barriers.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hyper-vlasov_b200"))
+
+METRIC = "particle-steps/s (208Pb, 2M tp)"
+UNIT = "particle-steps/s"
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "sor_traffic.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="208Pb-2.08M-128^3")
+    ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--warm-start", choices=["previous", "extrapolate"], default="previous")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-steps", type=int, default=2, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-warmup", type=int, default=0, help=argparse.SUPPRESS)
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, n in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- helpers
+def dist_setup(gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def step_bytes(w, n_sor, wordsize=4):
+    """Algorithmic bytes of one step, per kernel: 48 B per particle (x, k read
+    and written) and 4 G (24 + 3 n_sor) B of grid traffic (deposit 2 words per
+    node, smoothing 4, Skyrme 4, merge 2, FDM 8, gather 6 minus overlap, SOR 3
+    per iteration)."""
+    G, N = w.G, w.particles
+    s = wordsize / 4.0
+    return {
+        "particle": s * (48 * N + 4 * G * (2 + 6)),
+        "smooth": s * 4 * G * 4,
+        "skyrme": s * 4 * G * 4,
+        "sor": s * 4 * G * 3 * n_sor,
+        "forces": s * 4 * G * 10,
+    }
+
+
+# ---------------------------------------------------------------- CPU arm
+def cpu_sample(args):
+    """Runs inside a child process with the stack and OpenMP settings the
+    reference's deposit needs: the reference's step routines on the host."""
+    import numpy as np
+
+    import hv_b200 as hv
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from hv_oracle import Oracle, Reference, RunSpec, reference_available
+    w = hv.WORKLOADS[args.workload]
+    dt = np.float32 if args.precision == "f32" else np.float64
+    parts = hv.workload_particles(w, dt)
+    A, B, Cc, g = w.skyrme()
+    steps = args.cpu_warmup + args.cpu_steps
+    run = RunSpec(z=w.Z, n=w.N, part_per_nucleon=w.ppn, sigma_r=w.sigma_r, dt=w.dt, t_exc=w.t_exc, eta_exc=w.eta,
+                  A=A, B=B, C=Cc, gamma=g, sor_omega=w.sor_omega, sor_tol=w.sor_tol,
+                  sor_criterion=w.sor_criterion, sor_max_iter=w.sor_max_iter)
+    threads = os.cpu_count() or 1
+    if reference_available("_portable"):
+        r = Reference(dt, "_portable")
+        r.set_threads(threads)
+        _, _, times = r.simulate(w.world_tuple(), run, w.protons, w.neutrons, *parts, steps, smooth_mode=1,
+                                 step_times=True)
+        kind = "reference"
+        what = ("the reference's own routines (include/*.hpp, compiled from source, -O3 -march=x86-64-v3) in "
+                "cpu_simulate order; its SOR is hard-wired to omega 1.5, |dphi| < 1e-4, 512 iterations; the "
+                "O(G^2) smoothing replaced by the identical-pair-set offset table")
+    else:
+        o = Oracle(dt)
+        o.set_threads(threads)
+        _, _, times = o.simulate(w.world_tuple(), run, w.protons, w.neutrons, *parts, steps, step_times=True)
+        kind = "port"
+        what = "the C restatement of the reference (oracle/hv_oracle.c) with the workload's SOR settings"
+    timed = times[1 + args.cpu_warmup:]
+    secs = float(timed.sum())
+    print(json.dumps({"kind": kind, "seconds": secs, "steps": int(len(timed)), "init_seconds": float(times[0]),
+                      "threads": threads, "what": what, "value": w.particles * len(timed) / secs}))
+
+
+def run_cpu_child(args, steps, warmup):
+    env = dict(os.environ)
+    env["OMP_STACKSIZE"] = "64M"  # the deposit reduction keeps a private 2G grid per thread
+    env["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
+    cmd = (f"ulimit -s unlimited; exec {sys.executable} {os.path.abspath(__file__)} --cpu-sample "
+           f"--workload '{args.workload}' --precision {args.precision} --cpu-steps {steps} --cpu-warmup {warmup}")
+    r = subprocess.run(["bash", "-c", cmd], capture_output=True, text=True, env=env, timeout=1800)
+    for line in r.stdout.splitlines()[::-1]:
+        if line.startswith("{"):
+            return json.loads(line)
+    raise RuntimeError("CPU sample failed: " + r.stderr[-2000:])
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import hv_b200 as hv
+    w = hv.WORKLOADS[args.workload]
+    # each step of the reference is a full time step of the workload; bound the
+    # number of timed steps so that the arm ends within a few minutes
+    steps = max(1, min(args.steps, 3))
+    warm = min(args.warmup, 1)
+    s = run_cpu_child(args, steps, warm)
+    line = {
+        "metric": METRIC, "value": s["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": s["steps"],
+        "warmup": warm, "ms_per_step": 1e3 * s["seconds"] / s["steps"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": w.name, "particles": w.particles, "grid": f"{w.n}^3", "h_fm": w.h, "dt_fm_c": w.dt},
+        "cpu_baseline": {"value": s["value"], "unit": UNIT, "cores": s["threads"], "kind": s["kind"],
+                         "sample": f"{s['steps']} time steps of {w.name} after {warm} warm-up step(s) and the "
+                                   f"initial solve ({s['init_seconds']:.1f} s, untimed); {s['what']}"},
+        "e2e": {"value": s["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def our_arm(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import hv_b200 as hv
+    w = hv.WORKLOADS[args.workload]
+    prec = hv.HV_F32 if args.precision == "f32" else hv.HV_F64
+    dt = np.float32 if prec == hv.HV_F32 else np.float64
+    K, W = args.steps, max(3, args.warmup)
+    warm_mode = hv.HV_WARM_EXTRAPOLATE if args.warm_start == "extrapolate" else hv.HV_WARM_PREVIOUS
+    parts = hv.workload_particles(w, dt)
+    torch.cuda.set_device(local)
+
+    sess = hv.Session.from_workload(w, prec, device=local)
+    sess.set_fast_options(sor_warm_start=warm_mode)
+    sess.upload_particles(*parts)
+    sess.run(W, hv.HV_PATH_FUSED)  # includes the initial field solve
+    stream = torch.cuda.ExternalStream(sess.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        obs = sess.run(K, hv.HV_PATH_FUSED)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(world, ms)
+    value = w.particles * K * world / (ms_max / 1e3)
+    sor_its = obs["sor_iterations"].astype(np.int64)
+
+    # per-kernel device times over the same number of steps (direct launches)
+    sess.set_profiling(True)
+    obs_p = sess.run(K, hv.HV_PATH_FUSED)
+    kt = sess.kernel_times()
+    sess.set_profiling(False)
+    its_p = obs_p["sor_iterations"].astype(np.int64)
+    nbytes = step_bytes(w, its_p.mean(), 4 if prec == hv.HV_F32 else 8)
+    tot_ms = sum(v[0] for v in kt.values())
+    kernels = {}
+    for k, (kms, n) in kt.items():
+        if n == 0:
+            continue
+        per = kms / n
+        b = nbytes[k]
+        kernels[k] = {"launches": n, "avg_ms": per, "share": kms / tot_ms if tot_ms else None,
+                      "algorithmic_bytes": b, "gbs": b / (per / 1e3) / 1e9}
+    peak, peak_kind = peaks()
+    sor_b = sum(step_bytes(w, n, 4 if prec == hv.HV_F32 else 8)["sor"] for n in its_p)
+    sor_ms = kt["sor"][0]
+    achieved = sor_b / (sor_ms / 1e3) / 1e9 if sor_ms > 0 else None
+    traffic = None
+    if os.path.exists(PROFILE_TRAFFIC):
+        try:
+            with open(PROFILE_TRAFFIC) as f:
+                traffic = json.load(f).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "traffic": traffic,
+                "kernel": "k_sor_fast (persistent red-black SOR)", "peak_source": peak_kind,
+                "bytes": "12 B per node per red+black iteration (read phi, rho_p; write phi)",
+                "mean_sor_iterations": float(its_p.mean())}
+
+    launches_per_step = 6
+    chunk = sess.fast_options().graph_steps or 8
+    gpu_launches = K * launches_per_step + math.ceil(K / chunk)
+    sess.close()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": w.name, "nucleus": f"208Pb (Z={w.Z}, N={w.N})", "particles": w.particles,
+                   "grid": f"{w.n}^3", "h_fm": w.h, "dt_fm_c": w.dt,
+                   "sor": f"red-black omega {w.sor_omega} to relative residual {w.sor_tol:g}",
+                   "warm_start": args.warm_start, "path": "fused",
+                   "precision": "f32 particles/grids, f64 phi, SOR residual and observable sums",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "working set larger than L2 (particle state 50 MB + 2x128^3 fields ~120 MB)"},
+        "sor_iterations_per_step": float(sor_its.mean()),
+        "roofline": roofline, "kernels": kernels, "gpu_launches": gpu_launches,
+        "clocks": clk.summary(),
+    }
+
+    if not args.no_e2e:
+        pinned = [torch.from_numpy(p.copy()).pin_memory() for p in parts]
+        host = [t.numpy() for t in pinned]
+        barrier(world)
+        t0 = time.perf_counter()
+        obs_e = hv.simulate(w, *host, K, prec, hv.HV_PATH_FUSED)
+        el = time.perf_counter() - t0
+        el_max = max_over_ranks(world, el)
+        es = 4 if prec == hv.HV_F32 else 8
+        line["e2e"] = {"value": w.particles * K * world / el_max, "unit": UNIT,
+                       "h2d_bytes_per_step": 6 * w.particles * es / K,
+                       "d2h_bytes_per_step": (6 * w.particles * es + obs_e.nbytes) / K,
+                       "includes": "context creation, upload, initial solve, K steps, download (hv_simulate)"}
+
+    if not args.no_plain and rank == 0:
+        # the plain FP64 drop-in: per-routine kernels, SOR tested on the host
+        p64 = [p.astype(np.float64) for p in parts]
+        with hv.Session.from_workload(w, hv.HV_F64, device=local) as s64:
+            s64.upload_particles(*p64)
+            s64.initial_solve()
+            kp = 3
+            st = torch.cuda.ExternalStream(s64.stream())
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a0.record(st)
+            ob64 = s64.run(kp, hv.HV_PATH_PLAIN)
+            a1.record(st)
+            a1.synchronize()
+            pms = a0.elapsed_time(a1) / kp
+        with hv.Session.from_workload(w, prec, device=local) as sf:
+            sf.upload_particles(*parts)
+            obf = sf.run(kp, hv.HV_PATH_FUSED)
+        dmax = float(np.max(np.abs(ob64["dipole"])))
+        line["plain_f64"] = {"value": w.particles / (pms / 1e3), "unit": UNIT, "ms_per_step": pms, "steps": kp,
+                             "speedup_of_value": value / world / (w.particles / (pms / 1e3)),
+                             "sor_iterations_per_step": float(ob64["sor_iterations"].mean()),
+                             "dipole_max_rel_diff_fused_f32": float(np.max(np.abs(obf["dipole"] - ob64["dipole"])) /
+                                                                    dmax) if dmax > 0 else None}
+
+    if not args.no_cpu and rank == 0 and world == 1:
+        try:
+            s = run_cpu_child(args, args.cpu_steps, 0)
+            line["cpu_baseline"] = {"value": s["value"], "unit": UNIT, "cores": s["threads"], "kind": s["kind"],
+                                    "sample": f"{s['steps']} time step(s) of {w.name} after the initial solve "
+                                              f"({s['init_seconds']:.1f} s, untimed); {s['what']}"}
+        except Exception as e:  # reported, never fatal for the GPU number
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"failed: {e}"[:300]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.cpu_sample:
+        cpu_sample(args)
+        return
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        reference_arm(args, world, rank)
+        return
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        our_arm(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

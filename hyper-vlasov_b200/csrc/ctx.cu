@@ -372,6 +372,7 @@ hv_status hv_ctx_create(const hv_world *world, int protons, int neutrons, hv_pre
     c->params = *params;
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
+    hv_fast_options_default(&c->fast);
     hv_status st = HV_OK;
     auto fail = [&](hv_status s) {
         hv_ctx_destroy(c);
@@ -419,6 +420,8 @@ hv_status hv_ctx_destroy(hv_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     fused_release(c);
+    for (cudaEvent_t e : c->prof.events) cudaEventDestroy(e);
+    c->prof.events.clear();
     free_state(c->d64);
     free_state(c->d32);
     Scratch &s = c->scratch;
@@ -460,10 +463,8 @@ hv_status hv_ctx_set_params(hv_ctx *c, const hv_run_params *p) {
         }
         HV_CUDA(cudaStreamSynchronize(c->stream));
     }
-    if (c->fused.graph) {
-        cudaGraphExecDestroy(c->fused.graph);
-        c->fused.graph = nullptr;
-    }
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    fused_release(c);  // plans and graphs depend on the parameters
     return HV_OK;
 }
 
@@ -486,6 +487,8 @@ hv_status hv_ctx_synchronize(hv_ctx *c) {
 hv_status hv_upload_particle_array(hv_ctx *c, int which, const void *host) {
     if (!c) return HV_ERR_BAD_ARG;
     HV_CUDA(cudaSetDevice(c->device));
+    if (which <= HV_PART_Z) c->fields_valid = false;
+    fused_invalidate(c);
     HV_TRY(DISPATCH(c, upload_part<double>(c, which, host), upload_part<float>(c, which, host)));
     HV_CUDA(cudaStreamSynchronize(c->stream));
     return HV_OK;
@@ -502,6 +505,8 @@ hv_status hv_upload_particles(hv_ctx *c, const void *x, const void *y, const voi
     if (!c) return HV_ERR_BAD_ARG;
     const void *src[6] = {x, y, z, kx, ky, kz};
     HV_CUDA(cudaSetDevice(c->device));
+    if (x || y || z) c->fields_valid = false;
+    fused_invalidate(c);
     for (int a = 0; a < 6; a++)
         if (src[a]) HV_TRY(DISPATCH(c, upload_part<double>(c, a, src[a]), upload_part<float>(c, a, src[a])));
     HV_CUDA(cudaStreamSynchronize(c->stream));
@@ -524,6 +529,7 @@ hv_status hv_upload_field(hv_ctx *c, int field, const void *host) {
     void *d = DISPATCH(c, (void *)field_ptr(c->d64, field, &n, c->geom.G), (void *)field_ptr(c->d32, field, &n, c->geom.G));
     if (!d) return HV_ERR_BAD_ARG;
     const size_t es = c->prec == HV_F64 ? 8 : 4;
+    fused_invalidate(c);
     HV_CUDA(cudaMemcpyAsync(d, host, es * n, cudaMemcpyHostToDevice, c->stream));
     HV_CUDA(cudaStreamSynchronize(c->stream));
     if (field == HV_FIELD_COULOMB) c->boundary_set = true;  // the caller owns phi now
@@ -554,7 +560,8 @@ hv_status hv_field_device_ptr(hv_ctx *c, int field, void **dev_ptr) {
 // ---- per-routine entry points -------------------------------------------
 #define STAGE_BEGIN(c)                          \
     if (!(c)) return HV_ERR_BAD_ARG;            \
-    HV_CUDA(cudaSetDevice((c)->device));
+    HV_CUDA(cudaSetDevice((c)->device));        \
+    fused_invalidate(c);
 
 #define SYNC_END(c)                                  \
     HV_CUDA(cudaStreamSynchronize((c)->stream));     \
@@ -649,12 +656,66 @@ hv_status hv_excite(hv_ctx *c, double eta) {
 }
 
 hv_status hv_observe(hv_ctx *c, hv_observables *out) {
-    STAGE_BEGIN(c);
+    if (!c) return HV_ERR_BAD_ARG;
+    HV_CUDA(cudaSetDevice(c->device));
     if (!out) return HV_ERR_BAD_ARG;
     std::memset(out, 0, sizeof(*out));
     HV_TRY(DISPATCH(c, launch_observe<double>(c, c->d64.x, c->d64.y, c->d64.z, out),
                     launch_observe<float>(c, c->d32.x, c->d32.y, c->d32.z, out)));
     out->t = c->step_index * c->params.dt;
+    return HV_OK;
+}
+
+void hv_fast_options_default(hv_fast_options *o) {
+    if (!o) return;
+    o->sor_warm_start = HV_WARM_PREVIOUS;
+    o->sor_inner_min = 2;
+    o->sor_inner_max = 64;
+    o->sort_every = 16;
+    o->graph_steps = 8;
+}
+
+hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
+    if (!c || !o) return HV_ERR_BAD_ARG;
+    if (o->sor_warm_start != HV_WARM_PREVIOUS && o->sor_warm_start != HV_WARM_EXTRAPOLATE) return HV_ERR_BAD_ARG;
+    if (o->sor_inner_min < 1 || o->sor_inner_max < o->sor_inner_min || o->sor_inner_max > 4096) return HV_ERR_BAD_ARG;
+    if (o->sort_every < 0 || o->graph_steps < 0 || o->graph_steps > 64) return HV_ERR_BAD_ARG;
+    HV_CUDA(cudaSetDevice(c->device));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->fused.graph) {
+        cudaGraphExecDestroy(c->fused.graph);
+        c->fused.graph = nullptr;
+        c->fused.graph_len = 0;
+    }
+    c->fast = *o;
+    return HV_OK;
+}
+
+hv_status hv_ctx_get_fast_options(const hv_ctx *c, hv_fast_options *o) {
+    if (!c || !o) return HV_ERR_BAD_ARG;
+    *o = c->fast;
+    return HV_OK;
+}
+
+hv_status hv_ctx_set_profiling(hv_ctx *c, int enable) {
+    if (!c) return HV_ERR_BAD_ARG;
+    HV_CUDA(cudaSetDevice(c->device));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    c->prof.on = enable != 0;
+    c->prof.kernel.clear();
+    for (int k = 0; k < HV_K_COUNT; k++) {
+        c->prof.ms[k] = 0.0;
+        c->prof.launches[k] = 0;
+    }
+    return HV_OK;
+}
+
+hv_status hv_ctx_kernel_times(hv_ctx *c, double *total_ms, int *launches, int n) {
+    if (!c || n < 0 || n > HV_K_COUNT) return HV_ERR_BAD_ARG;
+    for (int k = 0; k < n; k++) {
+        if (total_ms) total_ms[k] = c->prof.ms[k];
+        if (launches) launches[k] = c->prof.launches[k];
+    }
     return HV_OK;
 }
 
@@ -665,14 +726,20 @@ hv_status hv_initial_solve(hv_ctx *c, int *sor_iterations) {
     if (sor_iterations) *sor_iterations = its;
     if (st != HV_OK && st != HV_ERR_NOT_CONVERGED) return st;
     HV_CUDA(cudaStreamSynchronize(c->stream));
+    c->fields_valid = true;
     return HV_OK;
 }
 
 hv_status hv_run(hv_ctx *c, int n_steps, int path, hv_observables *obs) {
-    STAGE_BEGIN(c);
+    if (!c) return HV_ERR_BAD_ARG;
+    HV_CUDA(cudaSetDevice(c->device));
     if (n_steps < 0) return HV_ERR_BAD_ARG;
+    if (path != HV_PATH_PLAIN && path != HV_PATH_FUSED) return HV_ERR_BAD_ARG;
+    // a run starts from forces of the current positions: solve for them first
+    // if nothing has (the fused path uses its own kernels for that solve)
     if (path == HV_PATH_FUSED) return fused_run(c, n_steps, obs);
-    if (path != HV_PATH_PLAIN) return HV_ERR_BAD_ARG;
+    if (!c->fields_valid) HV_TRY(hv_initial_solve(c, nullptr));
+    fused_invalidate(c);  // the plain step rewrites the fields
     for (int s = 0; s < n_steps; s++) {
         hv_observables *row = obs ? &obs[s] : nullptr;
         if (row) std::memset(row, 0, sizeof(*row));
@@ -690,7 +757,7 @@ hv_status hv_simulate(const hv_world *world, int protons, int neutrons, hv_preci
     hv_ctx *c = nullptr;
     HV_TRY(hv_ctx_create(world, protons, neutrons, prec, params, -1, &c));
     hv_status st = hv_upload_particles(c, x, y, z, kx, ky, kz);
-    if (st == HV_OK) st = hv_initial_solve(c, nullptr);
+    // hv_run performs the initial field solve on the chosen path
     if (st == HV_OK) st = hv_run(c, n_steps, path, obs);
     if (st == HV_OK) st = hv_download_particles(c, x, y, z, kx, ky, kz);
     hv_ctx_destroy(c);

@@ -80,23 +80,59 @@ struct Scratch {
     size_t cub_tmp_bytes = 0;
 };
 
+// Partition and device buffers of the persistent SOR solver (k_sor_fast.cu).
+struct SorFast {
+    bool ok = false;           // a partition that fits on chip was found
+    int P = 0, R = 0;          // planes and rows owned by one block
+    int bx = 0, by = 0;        // blocks along x (interior planes) and y
+    int nblocks = 0;
+    int threads = 0;
+    size_t smem = 0;
+    int nz2 = 0;               // (nz + 1) / 2: length of one colour half-line
+    void *delta = nullptr;     // SOR correction, colour-split layout
+    void *src = nullptr;       // residual source, colour-split layout
+    double *partials = nullptr;
+    unsigned *phase = nullptr; // per-block publish counters
+    unsigned *bar = nullptr;   // [0] arrivals, [1] generation
+    int *status = nullptr;     // [0] error, [1] iterations, [2] converged, [3] m hint
+    double *metric = nullptr;  // final stopping quantity
+};
+
+// Decomposed smoothing plan (k_smooth_fast.cu).
+struct SmoothFast {
+    bool ok = false;           // tap table is symmetric with contiguous z runs
+    int A = 0, B = 0, W = 0;   // max |a|, |b|, z half-width
+    float *g = nullptr;        // device: gx[A+1], gy[B+1], gz[W+1]
+    int *w = nullptr;          // device: w(|a|,|b|) or -1, (A+1) x (B+1)
+};
+
 // Fast-path (fused) buffers.
 struct Fused {
     bool ready = false;
-    double *phi64 = nullptr;    // Coulomb potential, always double
-    double *phi64_prev = nullptr;
-    float *delta = nullptr;     // SOR correction (float)
-    float *src = nullptr;       // SOR source (float residual)
-    double *delta64 = nullptr;  // SOR correction when T = double
-    double *src64 = nullptr;
-    void *F4 = nullptr;         // interleaved forces, T4 per node
-    double *obs_dev = nullptr;  // per-step observables ring
-    int obs_cap = 0;
-    int *sor_its_dev = nullptr;
-    int *flags = nullptr;       // device status / control words
+    double *phi64 = nullptr;      // Coulomb potential (double for every precision)
+    double *phi64_prev = nullptr; // previous step's phi (extrapolated warm start)
+    void *F4 = nullptr;           // interleaved forces, 4 x T per node
+    double *obs_partials = nullptr;  // per-step observable partials
+    int obs_blocks = 0;
+    int obs_rows = 0;             // capacity in steps
+    int *sor_its = nullptr;       // per-step SOR iterations (device)
+    double *obs_rows_dev = nullptr;  // reduced rows (device)
     cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0;
-    int prev_valid = 0;
+    int graph_len = 0;
+    bool prev_valid = false;      // phi64_prev holds the previous step's phi
+    bool f4_current = false;      // F4 holds the forces of the current positions
+    int m_hint = 8;
+    SorFast sor;
+    SmoothFast smooth;
+};
+
+// Per-kernel CUDA-event timing of fused steps (hv_ctx_set_profiling).
+struct Profile {
+    bool on = false;
+    std::vector<cudaEvent_t> events;  // event pairs (start, stop)
+    std::vector<int> kernel;          // kernel id of each pair in use
+    double ms[HV_K_COUNT] = {0, 0, 0, 0, 0};
+    int launches[HV_K_COUNT] = {0, 0, 0, 0, 0};
 };
 
 }  // namespace hv
@@ -118,7 +154,10 @@ struct hv_ctx {
     int *taps_dev = nullptr;
     hv::Scratch scratch;
     hv::Fused fused;
+    hv::Profile prof;
+    hv_fast_options fast{};
     bool boundary_set = false;
+    bool fields_valid = false;  // forces correspond to the current positions
     bool permuted = false;   // particle slots reordered by the fused path
     bool excited = false;
     int step_index = 0;      // steps taken so far (time = step_index * dt)
@@ -163,6 +202,7 @@ hv_status launch_observe(hv_ctx *c, const T *x, const T *y, const T *z, hv_obser
 hv_status fused_prepare(hv_ctx *c);
 hv_status fused_release(hv_ctx *c);
 hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs);
+void fused_invalidate(hv_ctx *c);
 
 // geometry helpers
 inline Geom make_geom(const hv_world &w) {

@@ -1,10 +1,654 @@
-// Fused fast path (placeholder until the fused kernels land).
+// Fused fast path (HV_PATH_FUSED): one particle kernel per step, the field
+// kernels, the persistent SOR, replayed from a CUDA graph.
+//
+// The reference's step (src/hyper_vlasov.cpp:86-103) is
+//   [observe] [excite once] kick/2(f_n) drift deposit ... gather(f_{n+1}) kick/2(f_{n+1}).
+// The particle kernel of step n does, per particle, everything between two
+// field solves with the same arithmetic sequence:
+//   gather f_n -> [closing kick/2 of step n-1] -> observe x_n -> [excite]
+//   -> opening kick/2 of step n -> drift -> deposit x_{n+1},
+// so x and k are read and written once per step (48 B per particle in
+// float).  The closing half kick of the last step is applied by
+// k_close_kick when hv_run returns, leaving the state the plain path leaves.
+#include <cmath>
+#include <cstring>
+
 #include "hv_internal.h"
 
 namespace hv {
 
-hv_status fused_prepare(hv_ctx *) { return HV_ERR_UNSUPPORTED; }
-hv_status fused_release(hv_ctx *) { return HV_OK; }
-hv_status fused_run(hv_ctx *, int, hv_observables *) { return HV_ERR_UNSUPPORTED; }
+hv_status sor_fast_plan(hv_ctx *c);
+void sor_fast_release(hv_ctx *c);
+template <typename T>
+hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring);
+hv_status smooth_fast_plan(hv_ctx *c);
+void smooth_fast_release(hv_ctx *c);
+hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho);
+
+namespace {
+
+constexpr int kPBlock = 256;
+constexpr int kRing = 64;  // observable rows kept on the device
+
+// control words (Fused::ctl)
+enum { CTL_STEP = 0, CTL_MHINT = 1, CTL_PREV = 2, CTL_EXCITE = 3, CTL_CLOSE = 4, CTL_N = 8 };
+
+template <typename T>
+__device__ __forceinline__ void load_f4(const T *F4, long long node, T &fx, T &fy, T &fz);
+template <>
+__device__ __forceinline__ void load_f4<float>(const float *F4, long long node, float &fx, float &fy, float &fz) {
+    float4 v = __ldg(reinterpret_cast<const float4 *>(F4) + node);
+    fx = v.x;
+    fy = v.y;
+    fz = v.z;
+}
+template <>
+__device__ __forceinline__ void load_f4<double>(const double *F4, long long node, double &fx, double &fy, double &fz) {
+    const double2 *p = reinterpret_cast<const double2 *>(F4) + 2 * node;
+    double2 a = __ldg(p), b = __ldg(p + 1);
+    fx = a.x;
+    fy = a.y;
+    fz = b.x;
+}
+
+// CIC force gather at (px,py,pz) (distribute_forces_to_particles_cic,
+// include/tools.hpp:98-168; corner order and corner drop as there).
+template <typename T>
+__device__ __forceinline__ void gather_at(const Geom &g, const T *F4, long long off, T px, T py, T pz, T &ax, T &ay,
+                                          T &az) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    ax = ay = az = T(0);
+    T cx = (nx / T(2.0)) * (px / T(g.dmx) + T(1.0));
+    T cy = (ny / T(2.0)) * (py / T(g.dmy) + T(1.0));
+    T cz = (nz / T(2.0)) * (pz / T(g.dmz) + T(1.0));
+    if (cx < T(0) || cy < T(0) || cz < T(0) || cx >= nx || cy >= ny || cz >= nz) return;
+    int x0 = (int)cx, y0 = (int)cy, z0 = (int)cz;
+    T dx = cx - x0, dy = cy - y0, dz = cz - z0;
+    T tx = T(1) - dx, ty = T(1) - dy, tz = T(1) - dz;
+    const bool bx = x0 + 1 < nx, by = y0 + 1 < ny, bz = z0 + 1 < nz;
+    const long long sx = (long long)ny * nz, sy = nz;
+    const long long n0 = off + x0 * sx + y0 * sy + z0;
+    T fx, fy, fz, w;
+#define HV_G(COND, DNODE, W)                    \
+    if (COND) {                                 \
+        load_f4<T>(F4, n0 + (DNODE), fx, fy, fz); \
+        w = (W);                                \
+        ax += w * fx;                           \
+        ay += w * fy;                           \
+        az += w * fz;                           \
+    }
+    HV_G(true, 0, tx * ty * tz)
+    HV_G(bx, sx, dx * ty * tz)
+    HV_G(by, sy, tx * dy * tz)
+    HV_G(bx && by, sx + sy, dx * dy * tz)
+    HV_G(bz, 1, tx * ty * dz)
+    HV_G(bx && bz, sx + 1, dx * ty * dz)
+    HV_G(by && bz, sy + 1, tx * dy * dz)
+    HV_G(bx && by && bz, sx + sy + 1, dx * dy * dz)
+#undef HV_G
+}
+
+// CIC deposit of one particle (distribute_volumetric_particles_cic,
+// include/tools.hpp:35-96), atomically.
+template <typename T>
+__device__ __forceinline__ void deposit_at(const Geom &g, T *rho, long long off, T px, T py, T pz) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    T cx = (nx / T(2.0)) * (px / T(g.dmx) + T(1.0));
+    T cy = (ny / T(2.0)) * (py / T(g.dmy) + T(1.0));
+    T cz = (nz / T(2.0)) * (pz / T(g.dmz) + T(1.0));
+    if (cx < T(0) || cy < T(0) || cz < T(0) || cx >= nx || cy >= ny || cz >= nz) return;
+    int x0 = (int)cx, y0 = (int)cy, z0 = (int)cz;
+    T dx = cx - x0, dy = cy - y0, dz = cz - z0;
+    T tx = T(1) - dx, ty = T(1) - dy, tz = T(1) - dz;
+    const bool bx = x0 + 1 < nx, by = y0 + 1 < ny, bz = z0 + 1 < nz;
+    const long long sx = (long long)ny * nz, sy = nz;
+    T *b = rho + off + x0 * sx + y0 * sy + z0;
+    atomicAdd(b, tx * ty * tz);
+    if (bx) atomicAdd(b + sx, dx * ty * tz);
+    if (by) atomicAdd(b + sy, tx * dy * tz);
+    if (bx && by) atomicAdd(b + sx + sy, dx * dy * tz);
+    if (bz) atomicAdd(b + 1, tx * ty * dz);
+    if (bx && bz) atomicAdd(b + sx + 1, dx * ty * dz);
+    if (by && bz) atomicAdd(b + sy + 1, tx * dy * dz);
+    if (bx && by && bz) atomicAdd(b + sx + sy + 1, dx * dy * dz);
+}
+
+template <typename T>
+struct PArgs {
+    Geom g;
+    int protons, total;
+    T *x, *y, *z, *kx, *ky, *kz;
+    const T *F4;
+    T *rho_raw;
+    T h, fd, dp, dn;
+    const int *ctl;
+    double *obs;  // [kRing][blocks][6]
+};
+
+// One step of every particle; observables of x_n into the ring row of step n.
+template <typename T>
+__global__ void __launch_bounds__(kPBlock) k_particle_step(PArgs<T> a) {
+    const int step = a.ctl[CTL_STEP];
+    const bool close = a.ctl[CTL_CLOSE] != 0;
+    const bool excite = a.ctl[CTL_EXCITE] == step;
+    const T dmx = T(a.g.dmx), dmy = T(a.g.dmy), dmz = T(a.g.dmz);
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.total; i += gridDim.x * blockDim.x) {
+        const int s = i < a.protons ? 0 : 1;
+        const long long off = s ? a.g.G : 0;
+        T px = a.x[i], py = a.y[i], pz = a.z[i];
+        T qx = a.kx[i], qy = a.ky[i], qz = a.kz[i];
+        T fx, fy, fz;
+        gather_at<T>(a.g, a.F4, off, px, py, pz, fx, fy, fz);
+        if (close) {  // closing kick/2 of the previous step (physics.hpp:248-258)
+            qx += a.h * fx;
+            qy += a.h * fy;
+            qz += a.h * fz;
+        }
+        // observables of x_n (tools.hpp:302-338)
+        v[s] += (double)pz;
+        if (!(px < -dmx || px > dmx || py < -dmy || py > dmy || pz < -dmz || pz > dmz)) {
+            v[2 + s] += (double)(px * px + py * py + pz * pz);
+            v[4 + s] += 1.0;
+        }
+        if (excite) qz += s ? -a.dn : a.dp;  // physics.hpp:236-246
+        qx += a.h * fx;                      // opening kick/2
+        qy += a.h * fy;
+        qz += a.h * fz;
+        px += a.fd * qx;  // drift (physics.hpp:260-270)
+        py += a.fd * qy;
+        pz += a.fd * qz;
+        a.x[i] = px;
+        a.y[i] = py;
+        a.z[i] = pz;
+        a.kx[i] = qx;
+        a.ky[i] = qy;
+        a.kz[i] = qz;
+        deposit_at<T>(a.g, a.rho_raw, off, px, py, pz);
+    }
+    // deterministic block reduction of the six sums
+    __shared__ double sh[6][kPBlock / 32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int c = 0; c < 6; c++) {
+        double u = v[c];
+        for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+        if (l == 0) sh[c][w] = u;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double u = 0.0;
+        for (int q = 0; q < kPBlock / 32; q++) u += sh[threadIdx.x][q];
+        a.obs[((long long)(step % kRing) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = u;
+    }
+}
+
+// Closing kick/2 with the forces of the final positions; stores f.
+template <typename T>
+__global__ void k_close_kick(Geom g, int protons, int total, const T *__restrict__ x, const T *__restrict__ y,
+                             const T *__restrict__ z, T *kx, T *ky, T *kz, T *fx, T *fy, T *fz, const T *F4, T h) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    T ax, ay, az;
+    gather_at<T>(g, F4, i < protons ? 0 : g.G, x[i], y[i], z[i], ax, ay, az);
+    kx[i] += h * ax;
+    ky[i] += h * ay;
+    kz[i] += h * az;
+    fx[i] = ax;
+    fy[i] = ay;
+    fz[i] = az;
+}
+
+// Skyrme potential (include/physics.hpp:272-281, physics_formulas.hpp:70-77).
+template <typename T>
+__global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__restrict__ rho, T *U) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    const T rp = rho[i], rn = rho[i + G];
+    const T t = (rp + rn) / T(0.16);
+    const T base = A * t + B * pow(t, gamma);
+    const T iso = T(2.0) * C * ((rn - rp) / T(0.16));
+    U[i] = base - iso;
+    U[i + G] = base + iso;
+}
+
+// -grad(U + phi_p) with the reference's one-sided faces
+// (compute_volumetric_forces_fdm, include/physics.hpp:159-200), the Coulomb
+// merge (include/tools.hpp:377-384) folded in, written as (Fx,Fy,Fz,0).
+template <typename T>
+__global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U, const double *__restrict__ phi,
+                            T *F4) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * g.G) return;
+    const bool prot = i < g.G;
+    const long long id = prot ? i : i - g.G;
+    const T *Us = U + (prot ? 0 : g.G);
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long sx = (long long)ny * nz, sy = nz;
+    const int k = (int)(id % nz), j = (int)((id / nz) % ny), ii = (int)(id / sx);
+    auto u = [&](long long q) { return prot ? Us[q] + (T)phi[q] : Us[q]; };
+    T gx, gy, gz;
+    if (ii == 0) gx = (u(id + sx) - u(id)) * idx;
+    else if (ii == nx - 1) gx = (u(id) - u(id - sx)) * idx;
+    else gx = (u(id + sx) - u(id - sx)) * (T(0.5) * idx);
+    if (j == 0) gy = (u(id + sy) - u(id)) * idy;
+    else if (j == ny - 1) gy = (u(id) - u(id - sy)) * idy;
+    else gy = (u(id + sy) - u(id - sy)) * (T(0.5) * idy);
+    if (k == 0) gz = (u(id + 1) - u(id)) * idz;
+    else if (k == nz - 1) gz = (u(id) - u(id - 1)) * idz;
+    else gz = (u(id + 1) - u(id - 1)) * (T(0.5) * idz);
+    T *o = F4 + 4 * i;
+    o[0] = -gx;
+    o[1] = -gy;
+    o[2] = -gz;
+    o[3] = T(0);
+}
+
+template <typename T>
+__global__ void k_pack_f4(long long n, const T *__restrict__ Fx, const T *__restrict__ Fy, const T *__restrict__ Fz,
+                          T *F4) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    F4[4 * i] = Fx[i];
+    F4[4 * i + 1] = Fy[i];
+    F4[4 * i + 2] = Fz[i];
+    F4[4 * i + 3] = T(0);
+}
+
+template <typename T>
+__global__ void k_unpack_f4(long long n, const T *__restrict__ F4, T *Fx, T *Fy, T *Fz) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Fx[i] = F4[4 * i];
+    Fy[i] = F4[4 * i + 1];
+    Fz[i] = F4[4 * i + 2];
+}
+
+// POTENTIAL with the Coulomb term merged and phi in T, as the plain path leaves them.
+template <typename T>
+__global__ void k_merge_out(long long G, const double *__restrict__ phi64, T *U, T *phi) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    const T p = (T)phi64[i];
+    U[i] += p;
+    phi[i] = p;
+}
+
+template <typename T>
+__global__ void k_widen(long long n, const T *__restrict__ in, double *out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)in[i];
+}
+
+__global__ void k_advance(int *ctl) {
+    ctl[CTL_STEP] += 1;
+    ctl[CTL_CLOSE] = 1;
+}
+
+// rows[r] = sums over blocks (fixed order) of the ring row of step s0 + r
+__global__ void k_reduce_rows(const double *__restrict__ obs, int blocks, int s0, int nrows, double *rows) {
+    const int r = blockIdx.x, c = threadIdx.x;
+    if (r >= nrows || c >= 6) return;
+    const long long base = (long long)((s0 + r) % kRing) * blocks * 6;
+    double u = 0.0;
+    for (int b = 0; b < blocks; b++) u += obs[base + (long long)b * 6 + c];
+    rows[r * 8 + c] = u;
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+template <typename T>
+State<T> &st(hv_ctx *c);
+template <>
+State<double> &st<double>(hv_ctx *c) { return c->d64; }
+template <>
+State<float> &st<float>(hv_ctx *c) { return c->d32; }
+
+int *ctl_of(hv_ctx *c) { return c->fused.sor_its + kRing; }
+
+// CUDA-event pair around one kernel launch when profiling is on.
+struct ProfScope {
+    hv_ctx *c;
+    int pair = -1;
+    ProfScope(hv_ctx *cc, int kid) : c(cc) {
+        Profile &p = c->prof;
+        if (!p.on) return;
+        pair = (int)p.kernel.size();
+        while (p.events.size() < 2 * (size_t)pair + 2) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                pair = -1;
+                return;
+            }
+            p.events.push_back(e);
+        }
+        p.kernel.push_back(kid);
+        cudaEventRecord(p.events[2 * pair], c->stream);
+    }
+    ~ProfScope() {
+        if (pair >= 0) cudaEventRecord(c->prof.events[2 * pair + 1], c->stream);
+    }
+};
+
+// Adds the recorded pairs (the stream must be synchronised) to the totals.
+void prof_collect(hv_ctx *c) {
+    Profile &p = c->prof;
+    for (size_t i = 0; i < p.kernel.size(); i++) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.events[2 * i], p.events[2 * i + 1]) == cudaSuccess) {
+            p.ms[p.kernel[i]] += ms;
+            p.launches[p.kernel[i]] += 1;
+        }
+    }
+    p.kernel.clear();
+    cudaGetLastError();
+}
+
+// Enqueues one fused step on the context stream (graph-capturable).
+template <typename T>
+hv_status enqueue_step(hv_ctx *c) {
+    State<T> &s = st<T>(c);
+    Fused &f = c->fused;
+    const Geom &g = c->geom;
+    const hv_run_params &p = c->params;
+    int *ctl = ctl_of(c);
+    HV_CUDA(cudaMemsetAsync(s.rho_raw, 0, sizeof(T) * 2 * g.G, c->stream));
+    PArgs<T> a;
+    a.g = g;
+    a.protons = c->protons;
+    a.total = c->total;
+    a.x = s.x;
+    a.y = s.y;
+    a.z = s.z;
+    a.kx = s.kx;
+    a.ky = s.ky;
+    a.kz = s.kz;
+    a.F4 = reinterpret_cast<const T *>(f.F4);
+    a.rho_raw = s.rho_raw;
+    a.h = T(p.dt) / (T(2.0) * T(kHbarC));
+    a.fd = (T(p.dt) * T(kHbarC)) / T(kMc2);
+    const T zz = T(p.z), nn = T(p.n), e = T(p.eta_exc);
+    a.dp = e * nn / (zz + nn);
+    a.dn = e * zz / (zz + nn);
+    a.ctl = ctl;
+    a.obs = f.obs_partials;
+    if (c->total > 0) {
+        ProfScope ps(c, HV_K_PARTICLE);
+        k_particle_step<T><<<f.obs_blocks, kPBlock, 0, c->stream>>>(a);
+    } else {
+        HV_CUDA(cudaMemsetAsync(f.obs_partials, 0, sizeof(double) * kRing * f.obs_blocks * 6, c->stream));
+    }
+    HV_CUDA(cudaGetLastError());
+    {
+        ProfScope ps(c, HV_K_SMOOTH);
+        if (sizeof(T) == 4 && f.smooth.ok)
+            HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho)));
+        else
+            HV_TRY(launch_smooth<T>(c, s.rho_raw, s.rho));
+    }
+    const hv_skyrme &sk = p.skyrme;
+    {
+        ProfScope ps(c, HV_K_SKYRME);
+        k_skyrme_fast<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C), T(sk.gamma), s.rho,
+                                                                s.U);
+    }
+    HV_CUDA(cudaGetLastError());
+    {
+        ProfScope ps(c, HV_K_SOR);
+        HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, f.sor_its, kRing));
+    }
+    const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
+            idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
+    {
+        ProfScope ps(c, HV_K_FORCES);
+        k_forces_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
+                                                                  reinterpret_cast<T *>(f.F4));
+    }
+    HV_CUDA(cudaGetLastError());
+    k_advance<<<1, 1, 0, c->stream>>>(ctl);
+    HV_CUDA(cudaGetLastError());
+    return HV_OK;
+}
+
+// The initial field solve of cpu_simulate (src/hyper_vlasov.cpp:53-62) on the
+// fused kernels: deposit, smoothing, Coulomb boundary (double monopole,
+// include/tools.hpp:283-300), Skyrme, SOR from phi = 0 inside, forces, and the
+// gather into f.
+template <typename T>
+hv_status initial_typed(hv_ctx *c) {
+    State<T> &s = st<T>(c);
+    Fused &f = c->fused;
+    const Geom &g = c->geom;
+    const hv_run_params &p = c->params;
+    int *ctl = ctl_of(c);
+    HV_TRY(launch_deposit_atomic<T>(c, s.x, s.y, s.z, s.rho_raw));
+    if (sizeof(T) == 4 && f.smooth.ok)
+        HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho)));
+    else
+        HV_TRY(launch_smooth<T>(c, s.rho_raw, s.rho));
+    const hv_skyrme &sk = p.skyrme;
+    k_skyrme_fast<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C), T(sk.gamma), s.rho, s.U);
+    HV_CUDA(cudaGetLastError());
+    if (!c->boundary_set) {
+        HV_CUDA(cudaMemsetAsync(f.phi64, 0, sizeof(double) * g.G, c->stream));
+        HV_TRY(launch_boundary<double>(c, f.phi64));
+        c->boundary_set = true;
+    } else {
+        k_widen<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, s.phi, f.phi64);
+    }
+    int h_ctl[3] = {c->step_index, f.m_hint, 0};
+    HV_CUDA(cudaMemcpyAsync(ctl, h_ctl, sizeof(int) * 3, cudaMemcpyHostToDevice, c->stream));
+    HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, nullptr, kRing));
+    const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
+            idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
+    k_forces_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64, reinterpret_cast<T *>(f.F4));
+    HV_CUDA(cudaGetLastError());
+    int status[3] = {0, 0, 0};
+    HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    if (status[0]) {
+        set_last_error("SOR: a bounded device-side wait timed out");
+        return HV_ERR_TIMEOUT;
+    }
+    // f of the initial positions; the plain buffers get the same fields
+    if (c->total > 0)
+        k_close_kick<T><<<nblk(c->total, 256), 256, 0, c->stream>>>(g, c->protons, c->total, s.x, s.y, s.z, s.kx, s.ky,
+                                                                    s.kz, s.fx, s.fy, s.fz,
+                                                                    reinterpret_cast<const T *>(f.F4), T(0));
+    k_unpack_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(2 * g.G, reinterpret_cast<const T *>(f.F4), s.Fx, s.Fy, s.Fz);
+    k_merge_out<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, f.phi64, s.U, s.phi);
+    HV_CUDA(cudaGetLastError());
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    f.f4_current = true;
+    c->fields_valid = true;
+    return HV_OK;
+}
+
+template <typename T>
+hv_status enqueue_steps(hv_ctx *c, int n) {
+    for (int i = 0; i < n; i++) HV_TRY(enqueue_step<T>(c));
+    return HV_OK;
+}
+
+template <typename T>
+hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
+    State<T> &s = st<T>(c);
+    Fused &f = c->fused;
+    const Geom &g = c->geom;
+    int *ctl = ctl_of(c);
+    // bring the fused state up to date with the plain buffers
+    if (!f.f4_current) {
+        k_pack_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(2 * g.G, s.Fx, s.Fy, s.Fz, reinterpret_cast<T *>(f.F4));
+        k_widen<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, s.phi, f.phi64);
+        HV_CUDA(cudaGetLastError());
+        int zero = 0;
+        HV_CUDA(cudaMemcpyAsync(ctl + CTL_PREV, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        f.f4_current = true;
+    }
+    // excitation step: first n with n dt >= t_exc (hyper_vlasov.cpp:86), in T
+    int exc = -1;
+    if (!c->excited) {
+        for (int n = c->step_index; n < c->step_index + n_steps; n++)
+            if (T(n) * T(c->params.dt) >= T(c->params.t_exc)) {
+                exc = n;
+                break;
+            }
+    }
+    int h_ctl[5] = {c->step_index, f.m_hint, 0, exc, 0};
+    HV_CUDA(cudaMemcpyAsync(ctl + CTL_STEP, &h_ctl[0], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    HV_CUDA(cudaMemcpyAsync(ctl + CTL_EXCITE, &h_ctl[3], sizeof(int) * 2, cudaMemcpyHostToDevice, c->stream));
+
+    const int chunk = c->fast.graph_steps > 0 ? std::min(c->fast.graph_steps, kRing) : std::min(8, kRing);
+    int done = 0;
+    std::vector<double> rows;
+    std::vector<int> its(kRing);
+    while (done < n_steps) {
+        const int k = std::min(chunk, n_steps - done);
+        bool launched = false;
+        if (c->fast.graph_steps > 0 && k == chunk && !c->prof.on) {
+            if (!f.graph || f.graph_len != k) {
+                if (f.graph) {
+                    cudaGraphExecDestroy(f.graph);
+                    f.graph = nullptr;
+                }
+                cudaGraph_t gr = nullptr;
+                if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                    hv_status es = enqueue_steps<T>(c, k);
+                    cudaError_t ce = cudaStreamEndCapture(c->stream, &gr);
+                    if (es == HV_OK && ce == cudaSuccess && gr &&
+                        cudaGraphInstantiate(&f.graph, gr, 0) == cudaSuccess) {
+                        f.graph_len = k;
+                    } else {
+                        f.graph = nullptr;
+                        c->fast.graph_steps = 0;  // capture not possible here: launch directly
+                    }
+                    if (gr) cudaGraphDestroy(gr);
+                    cudaGetLastError();
+                }
+            }
+            if (f.graph) {
+                HV_CUDA(cudaGraphLaunch(f.graph, c->stream));
+                launched = true;
+            }
+        }
+        if (!launched) HV_TRY(enqueue_steps<T>(c, k));
+        // observables of the k steps
+        const int s0 = c->step_index + done;
+        k_reduce_rows<<<k, 32, 0, c->stream>>>(f.obs_partials, f.obs_blocks, s0, k, f.obs_rows_dev);
+        HV_CUDA(cudaGetLastError());
+        rows.resize((size_t)k * 8);
+        HV_CUDA(cudaMemcpyAsync(rows.data(), f.obs_rows_dev, sizeof(double) * 8 * k, cudaMemcpyDeviceToHost, c->stream));
+        HV_CUDA(cudaMemcpyAsync(its.data(), f.sor_its, sizeof(int) * kRing, cudaMemcpyDeviceToHost, c->stream));
+        int status[3] = {0, 0, 0};
+        HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
+        HV_CUDA(cudaStreamSynchronize(c->stream));
+        prof_collect(c);
+        if (status[0]) {
+            set_last_error("SOR: a bounded device-side wait timed out");
+            return HV_ERR_TIMEOUT;
+        }
+        if (obs) {
+            const double zz = c->params.z, nn = c->params.n;
+            for (int r = 0; r < k; r++) {
+                hv_observables &o = obs[done + r];
+                const double *v = &rows[(size_t)r * 8];
+                std::memset(&o, 0, sizeof(o));
+                o.t = (double)(T(s0 + r) * T(c->params.dt));
+                o.zcm_p = v[0] / (double)c->protons;
+                o.zcm_n = v[1] / (double)c->neutrons;
+                o.rms_p = std::sqrt(v[2] / v[4]);
+                o.rms_n = std::sqrt(v[3] / v[5]);
+                o.dipole = (nn * zz) / (nn + zz) * (o.zcm_p - o.zcm_n);
+                int it = its[(s0 + r) % kRing];
+                o.sor_iterations = it < 0 ? -it : it;
+                if (it < 0) o.flags |= HV_OBS_SOR_NOT_CONVERGED;
+            }
+        }
+        done += k;
+    }
+    if (exc >= 0) c->excited = true;
+    c->step_index += n_steps;
+    // closing kick/2 and the plain-path view of the fields
+    State<T> &S = s;
+    if (c->total > 0)
+        k_close_kick<T><<<nblk(c->total, 256), 256, 0, c->stream>>>(g, c->protons, c->total, S.x, S.y, S.z, S.kx, S.ky,
+                                                                    S.kz, S.fx, S.fy, S.fz,
+                                                                    reinterpret_cast<const T *>(f.F4),
+                                                                    T(c->params.dt) / (T(2.0) * T(kHbarC)));
+    k_unpack_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(2 * g.G, reinterpret_cast<const T *>(f.F4), S.Fx, S.Fy, S.Fz);
+    k_merge_out<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, f.phi64, S.U, S.phi);
+    HV_CUDA(cudaGetLastError());
+    int mh = 0;
+    HV_CUDA(cudaMemcpyAsync(&mh, ctl + CTL_MHINT, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    f.m_hint = mh > 0 ? mh : f.m_hint;
+    return HV_OK;
+}
+
+}  // namespace
+
+hv_status fused_prepare(hv_ctx *c) {
+    Fused &f = c->fused;
+    if (f.ready) return HV_OK;
+    const Geom &g = c->geom;
+    const size_t es = c->prec == HV_F64 ? 8 : 4;
+    HV_CUDA(cudaMalloc((void **)&f.phi64, sizeof(double) * g.G));
+    HV_CUDA(cudaMalloc((void **)&f.phi64_prev, sizeof(double) * g.G));
+    HV_CUDA(cudaMemsetAsync(f.phi64, 0, sizeof(double) * g.G, c->stream));
+    HV_CUDA(cudaMemsetAsync(f.phi64_prev, 0, sizeof(double) * g.G, c->stream));
+    HV_CUDA(cudaMalloc(&f.F4, es * 4 * 2 * g.G));
+    f.obs_blocks = 4 * c->sm_count;
+    HV_CUDA(cudaMalloc((void **)&f.obs_partials, sizeof(double) * kRing * f.obs_blocks * 6));
+    HV_CUDA(cudaMalloc((void **)&f.obs_rows_dev, sizeof(double) * kRing * 8));
+    HV_CUDA(cudaMalloc((void **)&f.sor_its, sizeof(int) * (kRing + CTL_N)));
+    HV_CUDA(cudaMemsetAsync(f.sor_its, 0, sizeof(int) * (kRing + CTL_N), c->stream));
+    f.obs_rows = kRing;
+    HV_TRY(sor_fast_plan(c));
+    if (!f.sor.ok) {
+        set_last_error("fused path: the SOR correction of this grid does not fit on chip");
+        return HV_ERR_UNSUPPORTED;
+    }
+    if (c->prec == HV_F32) HV_TRY(smooth_fast_plan(c));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    f.ready = true;
+    return HV_OK;
+}
+
+hv_status fused_release(hv_ctx *c) {
+    Fused &f = c->fused;
+    if (f.graph) cudaGraphExecDestroy(f.graph);
+    void *ptrs[] = {f.phi64, f.phi64_prev, f.F4, f.obs_partials, f.obs_rows_dev, f.sor_its};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    sor_fast_release(c);
+    smooth_fast_release(c);
+    f = Fused();
+    return HV_OK;
+}
+
+hv_status fused_initial_solve(hv_ctx *c) {
+    hv_status st = fused_prepare(c);
+    if (st != HV_OK) {
+        fused_release(c);
+        return st;
+    }
+    return c->prec == HV_F64 ? initial_typed<double>(c) : initial_typed<float>(c);
+}
+
+hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs) {
+    if (!c->fields_valid) HV_TRY(fused_initial_solve(c));
+    if (n_steps == 0) return HV_OK;
+    hv_status st = fused_prepare(c);
+    if (st != HV_OK) {
+        fused_release(c);
+        return st;
+    }
+    return c->prec == HV_F64 ? run_typed<double>(c, n_steps, obs) : run_typed<float>(c, n_steps, obs);
+}
+
+// Marks the fused copies stale after the plain path or an upload changed the state.
+void fused_invalidate(hv_ctx *c) {
+    c->fused.f4_current = false;
+    c->fused.prev_valid = false;
+}
 
 }  // namespace hv

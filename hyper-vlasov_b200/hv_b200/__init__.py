@@ -5,13 +5,14 @@ package is the Python side of its C ABI (include/hv_b200.h).
 """
 from . import _lib
 from ._lib import (HV_DEPOSIT_ATOMIC, HV_DEPOSIT_SORTED, HV_F32, HV_F64, HV_PATH_FUSED, HV_PATH_PLAIN,
-                   HV_SOR_MAX_UPDATE, HV_SOR_REL_RESIDUAL, OBS_DTYPE, HVError, load)
+                   HV_SOR_MAX_UPDATE, HV_SOR_REL_RESIDUAL, HV_WARM_EXTRAPOLATE, HV_WARM_PREVIOUS, OBS_DTYPE,
+                   HVError, load)
 from .api import Session, generate_nucleus, simulate, workload_particles
 from .workloads import CA40_SMALL, PB208_2M, PB208_104K, WORKLOADS, Workload
 
 __all__ = [
     "HV_DEPOSIT_ATOMIC", "HV_DEPOSIT_SORTED", "HV_F32", "HV_F64", "HV_PATH_FUSED", "HV_PATH_PLAIN",
-    "HV_SOR_MAX_UPDATE", "HV_SOR_REL_RESIDUAL", "OBS_DTYPE", "HVError", "load", "Session",
+    "HV_SOR_MAX_UPDATE", "HV_SOR_REL_RESIDUAL", "HV_WARM_EXTRAPOLATE", "HV_WARM_PREVIOUS", "OBS_DTYPE", "HVError", "load", "Session",
     "generate_nucleus", "simulate", "workload_particles", "CA40_SMALL", "PB208_2M", "PB208_104K",
     "WORKLOADS", "Workload", "_lib",
 ]

@@ -63,6 +63,15 @@ class hv_run_params(C.Structure):
     ]
 
 
+class hv_fast_options(C.Structure):
+    _fields_ = [("sor_warm_start", C.c_int), ("sor_inner_min", C.c_int), ("sor_inner_max", C.c_int),
+                ("sort_every", C.c_int), ("graph_steps", C.c_int)]
+
+
+HV_WARM_PREVIOUS = 0
+HV_WARM_EXTRAPOLATE = 1
+
+
 class hv_observables(C.Structure):
     _fields_ = [
         ("t", C.c_double), ("rms_p", C.c_double), ("rms_n", C.c_double),
@@ -117,6 +126,11 @@ SIGNATURES = {
     "hv_drift": (_S, [_P, _D]),
     "hv_excite": (_S, [_P, _D]),
     "hv_observe": (_S, [_P, _P]),
+    "hv_fast_options_default": (None, [_P]),
+    "hv_ctx_set_fast_options": (_S, [_P, _P]),
+    "hv_ctx_get_fast_options": (_S, [_P, _P]),
+    "hv_ctx_set_profiling": (_S, [_P, _I]),
+    "hv_ctx_kernel_times": (_S, [_P, _P, _P, _I]),
     "hv_initial_solve": (_S, [_P, _P]),
     "hv_run": (_S, [_P, _I, _I, _P]),
     "hv_simulate": (_S, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),

@@ -100,6 +100,39 @@ class Session:
         L.check(self.lib.hv_ctx_set_params(self._ctx, C.byref(params)), "hv_ctx_set_params")
         self.params = params
 
+    def fast_options(self) -> L.hv_fast_options:
+        o = L.hv_fast_options()
+        L.check(self.lib.hv_ctx_get_fast_options(self._ctx, C.byref(o)), "hv_ctx_get_fast_options")
+        return o
+
+    def set_fast_options(self, **kw):
+        """Updates fields of hv_fast_options (sor_warm_start, sor_inner_min,
+        sor_inner_max, sort_every, graph_steps)."""
+        o = self.fast_options()
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise KeyError(k)
+            setattr(o, k, int(v))
+        L.check(self.lib.hv_ctx_set_fast_options(self._ctx, C.byref(o)), "hv_ctx_set_fast_options")
+
+    KERNELS = ("particle", "smooth", "skyrme", "sor", "forces")
+
+    def set_profiling(self, enable: bool):
+        """Per-kernel CUDA-event timing of fused steps (direct launches)."""
+        L.check(self.lib.hv_ctx_set_profiling(self._ctx, int(bool(enable))), "hv_ctx_set_profiling")
+
+    def kernel_times(self):
+        """{kernel: (total device ms, launches)} since profiling was enabled."""
+        n = len(self.KERNELS)
+        ms = (C.c_double * n)()
+        ln = (C.c_int * n)()
+        L.check(self.lib.hv_ctx_kernel_times(self._ctx, ms, ln, n), "hv_ctx_kernel_times")
+        return {k: (ms[i], ln[i]) for i, k in enumerate(self.KERNELS)}
+
+    def stream(self):
+        """The context's CUDA stream (cudaStream_t as an integer)."""
+        return self.lib.hv_ctx_stream(self._ctx) or 0
+
     def synchronize(self):
         L.check(self.lib.hv_ctx_synchronize(self._ctx), "hv_ctx_synchronize")
 

@@ -264,6 +264,47 @@ HV_API hv_status hv_excite(hv_ctx *ctx, double eta);
  * (include/tools.hpp:302-325) of both species, summed in double. */
 HV_API hv_status hv_observe(hv_ctx *ctx, hv_observables *out);
 
+/* ---- fused-path options ------------------------------------------------ */
+
+/* SOR starting guess of each step's solve in the fused path. */
+typedef enum hv_warm_start {
+    HV_WARM_PREVIOUS = 0,    /* the previous step's phi, as the reference does  */
+    HV_WARM_EXTRAPOLATE = 1  /* 2 phi(t) - phi(t - dt): same stopping rule, fewer
+                                iterations; the converged phi differs from the
+                                reference's by less than the tolerance          */
+} hv_warm_start;
+
+/* Controls of HV_PATH_FUSED that have no counterpart in the reference. */
+typedef struct hv_fast_options {
+    int sor_warm_start;   /* hv_warm_start                                      */
+    int sor_inner_min;    /* red+black iterations between two FP64 residual     */
+    int sor_inner_max;    /*   checks: adaptive, clamped to [min, max]          */
+    int sort_every;       /* re-sort particle slots by cell every n steps (0 = off) */
+    int graph_steps;      /* steps captured per CUDA graph launch (0 = no graph) */
+} hv_fast_options;
+
+/* Defaults: HV_WARM_PREVIOUS, inner 2..64, sort every 16 steps, 8-step graphs. */
+HV_API void hv_fast_options_default(hv_fast_options *o);
+HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);
+HV_API hv_status hv_ctx_get_fast_options(const hv_ctx *ctx, hv_fast_options *o);
+
+/* Kernels of one fused step, for hv_ctx_kernel_times. */
+typedef enum hv_kernel_id {
+    HV_K_PARTICLE = 0,  /* gather + kicks + drift + deposit + observables      */
+    HV_K_SMOOTH = 1,    /* Gaussian smoothing                                  */
+    HV_K_SKYRME = 2,    /* Skyrme + symmetry potential                         */
+    HV_K_SOR = 3,       /* persistent Coulomb SOR                              */
+    HV_K_FORCES = 4,    /* -grad(U + phi) into the interleaved force field     */
+    HV_K_COUNT = 5
+} hv_kernel_id;
+
+/* Per-kernel CUDA-event timing of fused steps.  While enabled, steps are
+ * launched directly (not from a graph) with an event pair around each kernel
+ * on the context stream; hv_ctx_kernel_times returns the accumulated device
+ * milliseconds and launch counts per hv_kernel_id since the last enable. */
+HV_API hv_status hv_ctx_set_profiling(hv_ctx *ctx, int enable);
+HV_API hv_status hv_ctx_kernel_times(hv_ctx *ctx, double *total_ms, int *launches, int n);
+
 /* ---- whole-step drivers ----------------------------------------------- */
 
 /* The initial field solve of cpu_simulate (src/hyper_vlasov.cpp:53-62):

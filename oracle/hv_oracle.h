@@ -79,7 +79,7 @@ typedef struct orc_obs {
                          const R *y, const R *z, orc_obs *out);                               \
     int orc_simulate_##S(const orc_world *w, const orc_run *run, int protons, int neutrons,    \
                          R *x, R *y, R *z, R *kx, R *ky, R *kz, int steps, orc_obs *obs,      \
-                         R *fields_out);
+                         R *fields_out, double *step_seconds);
 
 ORC_DECLARE(double, d)
 ORC_DECLARE(float, f)

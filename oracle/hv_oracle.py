@@ -205,17 +205,20 @@ class Oracle:
         self._f("orc_observe")(C.byref(make_world(*world)), protons, neutrons, _ptr(x), _ptr(y), _ptr(z), C.byref(o))
         return o
 
-    def simulate(self, world, run: RunSpec, protons, neutrons, x, y, z, kx, ky, kz, steps, want_fields=False):
+    def simulate(self, world, run: RunSpec, protons, neutrons, x, y, z, kx, ky, kz, steps, want_fields=False,
+                 step_times=False):
         """cpu_simulate order; particle arrays are advanced in place.
-        Returns (observables structured array, fields or None)."""
+        Returns (observables structured array, fields or None), plus the
+        seconds of the initial solve and of each step when step_times."""
         self._chk(x, y, z, kx, ky, kz)
         obs = np.zeros(steps, OBS_DTYPE)
         G = int(np.prod(world[0]))
         fields = np.zeros(11 * G, self.dtype) if want_fields else None
+        times = np.zeros(steps + 1, np.float64)
         self._f("orc_simulate")(C.byref(make_world(*world)), C.byref(run.to_c()), protons, neutrons,
                                 _ptr(x), _ptr(y), _ptr(z), _ptr(kx), _ptr(ky), _ptr(kz), steps,
-                                obs.ctypes.data_as(C.c_void_p), _ptr(fields))
-        return obs, fields
+                                obs.ctypes.data_as(C.c_void_p), _ptr(fields), _ptr(times))
+        return (obs, fields, times) if step_times else (obs, fields)
 
 
 def split_fields(fields, G):
@@ -336,21 +339,25 @@ class Reference:
         return f(n, d, protons, neutrons, _ptr(x), _ptr(y), _ptr(z), species)
 
     def simulate(self, world, run: RunSpec, protons, neutrons, x, y, z, kx, ky, kz, steps,
-                 smooth_mode=1, want_fields=False):
+                 smooth_mode=1, want_fields=False, step_times=False):
         """The cpu_simulate loop with the reference's routines (its SOR is
         hard-wired to omega 1.5, |dphi| < 1e-4, 512).  smooth_mode 0 = the
         reference's O(G^2) smoothing, 1 = offset-table restatement.
-        Returns (rows[steps,5] = t, rms_p, rms_n, zcm_p, zcm_n; fields; seconds)."""
+        Returns (rows[steps,5] = t, rms_p, rms_n, zcm_p, zcm_n; fields; seconds).
+        With step_times=True, seconds is an array: [0] the initial field solve,
+        [1 + s] step s."""
         G = int(np.prod(world[0]))
         rows = np.zeros((steps, 5), np.float64)
         fields = np.zeros(11 * G, self.dtype) if want_fields else None
+        times = np.zeros(steps + 1, np.float64)
         n, d = self._w(world)
         f = self._f("simulate")
         f.restype = C.c_double
         f.argtypes = ([C.c_void_p, C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 6 +
                       [C.c_double, C.c_int, C.c_int, C.c_int] + [C.c_double] * 4 +
-                      [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p])
+                      [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                       C.c_void_p])
         secs = f(n, d, protons, neutrons, _ptr(x), _ptr(y), _ptr(z), _ptr(kx), _ptr(ky), _ptr(kz),
                  run.sigma_r, run.part_per_nucleon, run.z, run.n, run.A, run.B, run.C, run.gamma,
-                 run.dt, run.t_exc, run.eta_exc, steps, smooth_mode, _ptr(rows), _ptr(fields))
-        return rows, fields, secs
+                 run.dt, run.t_exc, run.eta_exc, steps, smooth_mode, _ptr(rows), _ptr(fields), _ptr(times))
+        return rows, fields, (times if step_times else secs)

@@ -360,7 +360,9 @@ void FN(orc_observe)(const orc_world *w, int protons, int neutrons, const R *x, 
 /* cpu_simulate (src/hyper_vlasov.cpp:32-104) without VTK/stats I/O; one
  * observable row per step, recorded where the reference records it. */
 int FN(orc_simulate)(const orc_world *w, const orc_run *run, int protons, int neutrons, R *x, R *y,
-                     R *z, R *kx, R *ky, R *kz, int steps, orc_obs *obs, R *fields_out) {
+                     R *z, R *kx, R *ky, R *kz, int steps, orc_obs *obs, R *fields_out,
+                     double *step_seconds) {
+    double t0 = orc_wtime();
     const long G = (long)w->n[0] * w->n[1] * w->n[2];
     const int total = protons + neutrons;
     R *rho = (R *)calloc((size_t)(2 * G), sizeof(R));
@@ -386,7 +388,9 @@ int FN(orc_simulate)(const orc_world *w, const orc_run *run, int protons, int ne
     FN(orc_merge)(w, U, phi);
     FN(orc_fdm)(w, U, Fx, Fy, Fz);
     FN(orc_gather_cic)(w, protons, neutrons, x, y, z, Fx, Fy, Fz, fx, fy, fz);
+    if (step_seconds) step_seconds[0] = orc_wtime() - t0;
     for (int step = 0; step < steps; step++) {
+        double ts = orc_wtime();
         if (obs) {
             FN(orc_observe)(w, protons, neutrons, x, y, z, &obs[step]);
             obs[step].t = (double)(step * dt);
@@ -408,6 +412,7 @@ int FN(orc_simulate)(const orc_world *w, const orc_run *run, int protons, int ne
         FN(orc_fdm)(w, U, Fx, Fy, Fz);
         FN(orc_gather_cic)(w, protons, neutrons, x, y, z, Fx, Fy, Fz, fx, fy, fz);
         FN(orc_kick_half)(total, kx, ky, kz, fx, fy, fz, dt);
+        if (step_seconds) step_seconds[1 + step] = orc_wtime() - ts;
     }
     if (fields_out) { /* layout: rho(2G) U(2G) phi(G) Fx(2G) Fy(2G) Fz(2G) */
         memcpy(fields_out, rho, sizeof(R) * 2 * G);

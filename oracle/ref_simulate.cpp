@@ -29,12 +29,13 @@ template <> struct OrcSmooth<float> {
     static void run(const orc_world *w, double s, int ppn, float *r, float *t) { orc_smooth_f(w, s, ppn, r, t); }
 };
 
-// One row per step: t, rms_p, rms_n, zcm_p, zcm_n (src/hyper_vlasov.cpp:66-70)
+// One row per step: t, rms_p, rms_n, zcm_p, zcm_n (src/hyper_vlasov.cpp:66-70).
+// step_seconds (may be null): [0] the initial field solve, [1 + s] step s.
 template <typename T>
 double simulate(const int *n, const double *dm, int protons, int neutrons, T *x, T *y, T *z, T *kx,
                 T *ky, T *kz, double sigma_r, int ppn, int Z, int N, double A, double B, double C,
                 double gamma, double dt_d, double t_exc, double eta, int steps, int smooth_mode,
-                double *rows, T *fields_out) {
+                double *rows, T *fields_out, double *step_seconds) {
     World<T> world;
     orc_world ow;
     for (int a = 0; a < 3; a++) {
@@ -87,7 +88,10 @@ double simulate(const int *n, const double *dm, int protons, int neutrons, T *x,
     merge_volumetric_potentials(&potentials, coulomb, world);
     compute_volumetric_forces_fdm(&forces, potentials, world);
     distribute_forces_to_particles_cic(&part, forces, world);
+    double t_init = omp_get_wtime() - t0;
+    if (step_seconds) step_seconds[0] = t_init;
     for (int step = 0; step < steps; step++) {
+        double ts = omp_get_wtime();
         if (rows) {
             T x_p = center_of_mass(part, PROTONS);
             T x_n = center_of_mass(part, NEUTRONS);
@@ -113,6 +117,7 @@ double simulate(const int *n, const double *dm, int protons, int neutrons, T *x,
         compute_volumetric_forces_fdm(&forces, potentials, world);
         distribute_forces_to_particles_cic(&part, forces, world);
         update_momenta_half(&part, dt);
+        if (step_seconds) step_seconds[1 + step] = omp_get_wtime() - ts;
     }
     double elapsed = omp_get_wtime() - t0;
     if (fields_out) {  // rho(2G) U(2G) phi(G) Fx(2G) Fy(2G) Fz(2G)
@@ -133,9 +138,11 @@ double simulate(const int *n, const double *dm, int protons, int neutrons, T *x,
                                        T *x, T *y, T *z, T *kx, T *ky, T *kz, double sigma_r,       \
                                        int ppn, int Z, int N, double A, double B, double C,         \
                                        double gamma, double dt, double t_exc, double eta,           \
-                                       int steps, int smooth_mode, double *rows, T *fields_out) {   \
+                                       int steps, int smooth_mode, double *rows, T *fields_out,     \
+                                       double *step_seconds) {                                      \
         return simulate<T>(n, dm, protons, neutrons, x, y, z, kx, ky, kz, sigma_r, ppn, Z, N, A, B, \
-                           C, gamma, dt, t_exc, eta, steps, smooth_mode, rows, fields_out);         \
+                           C, gamma, dt, t_exc, eta, steps, smooth_mode, rows, fields_out,          \
+                           step_seconds);                                                           \
     }
 
 REF_SIM(double, d)

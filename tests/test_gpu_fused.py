@@ -1,0 +1,193 @@
+"""GPU: the fused fast path (HV_PATH_FUSED) against the oracle and the plain path.
+
+Tolerances
+  * D(t): max|D - D_ref| / max|D_ref| <= 1e-3 for the float path against the
+    double oracle (the accuracy target of the float form), <= 1e-6 for the
+    double fused path against the double plain path;
+  * SOR: every step converges to the same stopping rule (relative residual
+    1e-6); the fused solver checks it every few iterations, so it may run up
+    to sor_inner_max iterations more than the plain solver, never fewer;
+  * fields after a fused run: smoothed density and potential of the final
+    positions within 1e-5 (float) of the oracle's, forces within 1e-4.
+"""
+from __future__ import annotations
+
+from dataclasses import replace
+
+import numpy as np
+import pytest
+from conftest import max_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_runspec(w):
+    from hv_oracle import RunSpec
+    A, B, C, gm = w.skyrme()
+    return RunSpec(z=w.Z, n=w.N, part_per_nucleon=w.ppn, sigma_r=w.sigma_r, dt=w.dt, t_exc=w.t_exc,
+                   eta_exc=w.eta, A=A, B=B, C=C, gamma=gm, sor_omega=w.sor_omega, sor_tol=w.sor_tol,
+                   sor_criterion=w.sor_criterion, sor_max_iter=w.sor_max_iter)
+
+
+def _oracle(w, steps, parts64):
+    from hv_oracle import Oracle
+    o = Oracle(np.float64)
+    o.set_threads(4)
+    a = [p.copy() for p in parts64]
+    obs, _ = o.simulate(w.world_tuple(), _oracle_runspec(w), w.protons, w.neutrons, *a, steps)
+    return obs, a
+
+
+def _fused(hv, w, steps, prec, parts, **opts):
+    with hv.Session.from_workload(w, prec) as s:
+        if opts:
+            s.set_fast_options(**opts)
+        s.upload_particles(*parts)
+        s.initial_solve()
+        obs = s.run(steps, hv.HV_PATH_FUSED)
+        out = s.download_particles()
+    return obs, out
+
+
+def test_fused_f32_dipole_within_1e_3_of_double_oracle(hv):
+    w = hv.CA40_SMALL
+    steps = 200
+    p32 = hv.workload_particles(w, np.float32)
+    obs_o, _ = _oracle(w, steps, [p.astype(np.float64) for p in p32])
+    obs, _ = _fused(hv, w, steps, hv.HV_F32, p32)
+    assert np.array_equal(obs["t"], obs_o["t"].astype(np.float32).astype(np.float64)) or \
+        np.max(np.abs(obs["t"] - obs_o["t"])) < 1e-4
+    err = max_rel(obs["dipole"], obs_o["dipole"])
+    assert err <= 1e-3, err
+    assert not np.any(obs["flags"] & 1)
+    assert np.all(obs["sor_iterations"] >= obs_o["sor_iterations"] - 1)
+
+
+def test_fused_f64_matches_plain_f64(hv):
+    w = hv.CA40_SMALL
+    steps = 30
+    p = hv.workload_particles(w, np.float64)
+    obs_f, out_f = _fused(hv, w, steps, hv.HV_F64, p)
+    with hv.Session.from_workload(w, hv.HV_F64) as s:
+        s.upload_particles(*p)
+        s.initial_solve()
+        obs_p = s.run(steps, hv.HV_PATH_PLAIN)
+        out_p = s.download_particles()
+    assert max_rel(obs_f["dipole"], obs_p["dipole"]) < 1e-6
+    assert np.max(np.abs(out_f[2] - out_p[2])) < 1e-6
+    d = obs_f["sor_iterations"] - obs_p["sor_iterations"]
+    assert np.all(d >= -1) and np.all(d <= 64)
+
+
+def test_fused_reference_sor_rule(hv):
+    w = hv.CA40_SMALL.with_reference_sor()
+    steps = 20
+    p = hv.workload_particles(w, np.float64)
+    obs_f, _ = _fused(hv, w, steps, hv.HV_F64, p)
+    obs_o, _ = _oracle(w, steps, p)
+    assert max_rel(obs_f["dipole"], obs_o["dipole"]) < 1e-4
+
+
+def test_extrapolated_warm_start_saves_iterations(hv):
+    w = hv.CA40_SMALL
+    steps = 60
+    p32 = hv.workload_particles(w, np.float32)
+    obs_a, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_inner_min=1, sor_inner_max=8)
+    obs_b, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_EXTRAPOLATE, sor_inner_min=1,
+                      sor_inner_max=8)
+    assert obs_b["sor_iterations"][10:].sum() < obs_a["sor_iterations"][10:].sum()
+    assert max_rel(obs_b["dipole"], obs_a["dipole"]) < 1e-3
+
+
+def test_fused_state_and_fields_match_oracle_on_final_positions(hv):
+    """After a fused run the plain buffers describe the final state: density,
+    potential and forces of the final positions (computed by the oracle from
+    those positions and the GPU's Coulomb potential)."""
+    from hv_oracle import Oracle
+    w = hv.CA40_SMALL
+    p32 = hv.workload_particles(w, np.float32)
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        s.upload_particles(*p32)
+        s.initial_solve()
+        s.run(3, hv.HV_PATH_FUSED)
+        x, y, z, kx, ky, kz = s.download_particles()
+        rho = s.download_field(1)
+        U = s.download_field(2)
+        phi = s.download_field(3)
+        Fx = s.download_field(4)
+        fz = s.download_array("fz")
+    o = Oracle(np.float64)
+    world = w.world_tuple()
+    x64, y64, z64 = (a.astype(np.float64) for a in (x, y, z))
+    rr = o.smooth(world, w.sigma_r, w.ppn, o.deposit(world, w.protons, w.neutrons, x64, y64, z64))
+    assert max_rel(rho, rr) < 1e-5
+    A, B, C, gm = w.skyrme()
+    Uo = o.skyrme(world, A, B, C, gm, rho.astype(np.float64))
+    o.merge(world, Uo, phi.astype(np.float64))
+    assert max_rel(U, Uo) < 2e-6
+    Fo = o.fdm(world, U.astype(np.float64))
+    assert max_rel(Fx, Fo[0]) < 1e-4
+    fo = o.gather(world, w.protons, w.neutrons, x64, y64, z64, *o.fdm(world, U.astype(np.float64)))
+    assert max_rel(fz, fo[2]) < 1e-4
+    # phi solves the Poisson problem to the requested tolerance
+    assert o.rel_residual(world, phi.astype(np.float64), rho.astype(np.float64)) < 1e-4
+
+
+def test_fused_runs_continue_across_calls_and_paths(hv):
+    """Two fused calls equal one longer call; a plain step after a fused run
+    continues from the same state."""
+    w = hv.CA40_SMALL
+    p = hv.workload_particles(w, np.float64)
+    obs1, out1 = _fused(hv, w, 12, hv.HV_F64, p, graph_steps=4)
+    with hv.Session.from_workload(w, hv.HV_F64) as s:
+        s.set_fast_options(graph_steps=4)
+        s.upload_particles(*p)
+        s.initial_solve()
+        a = s.run(5, hv.HV_PATH_FUSED)
+        b = s.run(7, hv.HV_PATH_FUSED)
+        out2 = s.download_particles()
+        c = s.run(2, hv.HV_PATH_PLAIN)
+    d = np.concatenate([a["dipole"], b["dipole"]])
+    assert max_rel(d, obs1["dipole"]) < 1e-9
+    assert np.max(np.abs(out2[2] - out1[2])) < 1e-9
+    assert np.all(np.isfinite(c["dipole"]))
+    assert np.allclose(np.concatenate([a["t"], b["t"], c["t"]]), np.arange(14) * w.dt)
+
+
+def test_graph_and_direct_launch_agree(hv):
+    w = hv.CA40_SMALL
+    p = hv.workload_particles(w, np.float64)
+    og, _ = _fused(hv, w, 16, hv.HV_F64, p, graph_steps=8)
+    od, _ = _fused(hv, w, 16, hv.HV_F64, p, graph_steps=0)
+    assert max_rel(og["dipole"], od["dipole"]) < 1e-12
+
+
+@pytest.mark.parametrize("n", [(20, 16, 24), (33, 17, 9)])
+def test_fused_odd_grids(hv, n):
+    """Non-cubic and odd grids: fused F64 tracks the plain F64 path."""
+    w = replace(hv.CA40_SMALL, name="odd", n=n[0])
+    # anisotropic world through the session directly
+    from hv_b200 import _lib as L
+    world = L.hv_world()
+    for a in range(3):
+        world.n[a] = n[a]
+        world.d_max[a] = 0.5 * n[a] * 1.0
+    params = w.run_params()
+    p = hv.workload_particles(w, np.float64)
+    res = []
+    for path in (hv.HV_PATH_PLAIN, hv.HV_PATH_FUSED):
+        with hv.Session(world, w.protons, w.neutrons, params, hv.HV_F64) as s:
+            s.upload_particles(*p)
+            s.initial_solve()
+            res.append(s.run(8, path))
+    assert max_rel(res[1]["dipole"], res[0]["dipole"]) < 1e-6
+
+
+def test_sor_cap_is_reported_per_step(hv):
+    """A run whose SOR would need more than max_iter iterations reports the
+    non-converged steps through the row flags and keeps going."""
+    w = replace(hv.CA40_SMALL, sor_max_iter=3)
+    p = hv.workload_particles(w, np.float64)
+    obs, _ = _fused(hv, w, 4, hv.HV_F64, p)
+    assert np.all(obs["flags"] & 1)
+    assert np.all(obs["sor_iterations"] <= 3)
