@@ -89,6 +89,7 @@ struct SorFast {
     int threads = 0;
     size_t smem = 0;
     int nz2 = 0;               // (nz + 1) / 2: length of one colour half-line
+    bool src_smem = false;     // the residual source also lives in shared memory
     void *delta = nullptr;     // SOR correction, colour-split layout
     void *src = nullptr;       // residual source, colour-split layout
     double *partials = nullptr;

@@ -10,15 +10,21 @@
 // than phi in float removes the float rounding floor of the residual (a float
 // phi stalls near 1e-4 relative residual on a 64^3 grid).
 //
-// One launch per solve, cooperative so that all blocks are resident.  Block b
-// owns P interior x-planes by R rows (all z) and keeps its delta in shared
-// memory in a colour-split layout: each z-line is stored as its red half and
-// its black half, so a colour sweep reads and writes unit-stride runs.  After
-// each colour sweep a block publishes its updated values to global memory and
-// bumps its phase counter; before the next sweep it waits only for its (up to
-// four) neighbours' counters.  Grid-wide barriers are used only around the
-// double residual.  Every wait is bounded: on timeout the block records an
-// error word and returns, and the host reports HV_ERR_TIMEOUT.
+// One cooperative launch per solve.  Block b owns P interior x-planes by R
+// rows (all z).  Its delta and, when it fits, its source live in shared
+// memory for the whole solve, in a colour-split layout: within a plane all
+// red nodes of a row are contiguous, then all black nodes, so that a colour
+// sweep reads and writes unit-stride runs and the red (or black) half of a
+// plane is one contiguous block in the global mirror ([x][colour][y][z/2]).
+// A colour sweep is:
+//   wait for the (up to four) neighbouring blocks' phase counters,
+//   copy their published boundary half-planes (the colour the sweep reads)
+//     into shared ghost buffers with 16-byte loads,
+//   update the own nodes of the colour from shared memory only,
+//   publish the own boundary half-planes to global memory, bump the phase.
+// Grid-wide barriers are used only around the double residual.  Every wait is
+// bounded: on timeout the block records an error word and returns, and the
+// host reports HV_ERR_TIMEOUT.
 #include <cmath>
 
 #include "hv_internal.h"
@@ -31,18 +37,18 @@ constexpr long long kMaxSpin = 1ll << 23;  // ~0.5 s of polling before giving up
 
 template <typename T, typename S>
 struct SorArgs {
-    int nx, ny, nz, nz2, P, R, bxn, byn, nblocks;
+    int nx, ny, nz, nz2, P, R, bxn, byn, nblocks, src_smem;
     S hx2i, hy2i, hz2i, inv_diag, omega;
     double dhx2i, dhy2i, dhz2i, ddiag, src_c;
     double tol;
     int max_iter, criterion, inner_min, inner_max, extrapolate;
     const T *rho;
     double *phi64, *phi64_prev;
-    S *delta, *src;
+    S *delta, *src;         // global mirrors, [x][colour][y][nz2]
     double *partials;       // [nblocks][4]: rr, bb, max|ddelta|, -
     unsigned *phase;        // [nblocks]
     unsigned *bar;          // [0] arrivals, [1] generation
-    int *status;            // [0] error, [1] iterations, [2] converged
+    int *status;            // [0] error, [1] iterations, [2] converged, [3] cycles
     double *metric;
     int *ctl;               // [0] step counter, [1] m hint, [2] previous-phi valid
     int *its_ring;          // per-step iterations, indexed by step % ring
@@ -81,7 +87,6 @@ __device__ bool grid_barrier(unsigned *bar, int nblocks, int *err) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(32);
             }
         }
         __threadfence();
@@ -109,7 +114,6 @@ __device__ bool wait_neighbours(const SorArgs<T, S> &a, int bx, int by, unsigned
                     ok = 0;
                     break;
                 }
-                __nanosleep(20);
             }
         }
         __threadfence();
@@ -126,7 +130,34 @@ __device__ __forceinline__ void publish(unsigned *phase_slot, unsigned value) {
     }
 }
 
-// Deterministic block sum of two doubles (fixed shuffle tree, fixed warp order).
+// dst[0..n) = src[0..n) through L2 (the source is written by other blocks),
+// 16 bytes at a time when both ends are aligned.
+template <typename S>
+__device__ __forceinline__ void copy_in(S *dst, const S *src, int n) {
+    constexpr int V = 16 / sizeof(S);
+    if ((n % V) == 0 && (((size_t)src | (size_t)dst) & 15) == 0) {
+        const float4 *s4 = reinterpret_cast<const float4 *>(src);
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+        for (int i = threadIdx.x; i < n / V; i += blockDim.x) d4[i] = __ldcg(s4 + i);
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldcg(src + i);
+    }
+}
+
+template <typename S>
+__device__ __forceinline__ void copy_out(S *dst, const S *src, int n) {
+    constexpr int V = 16 / sizeof(S);
+    if ((n % V) == 0 && (((size_t)src | (size_t)dst) & 15) == 0) {
+        const float4 *s4 = reinterpret_cast<const float4 *>(src);
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+        for (int i = threadIdx.x; i < n / V; i += blockDim.x) __stcg(d4 + i, s4[i]);
+    } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) __stcg(dst + i, src[i]);
+    }
+}
+
+// Deterministic block sum of two doubles (fixed shuffle tree, fixed warp order);
+// the result is valid in thread 0.
 __device__ void block_sum2(double &u, double &v) {
     __shared__ double su[kSorThreads / 32], sv[kSorThreads / 32];
     for (int o = 16; o > 0; o >>= 1) {
@@ -170,7 +201,6 @@ __device__ S block_max(S m) {
 template <typename T, typename S>
 __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    S *sd = reinterpret_cast<S *>(smem_raw);
     __shared__ double s_tot[3];
     __shared__ int s_m;
 
@@ -179,19 +209,30 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     const int x0 = 1 + bx * a.P, x1 = min(x0 + a.P, a.nx - 1);
     const int y0 = by * a.R, y1 = min(y0 + a.R, a.ny);
     const int np = x1 - x0, nr = y1 - y0;
-    const int nz = a.nz, ny = a.ny, nz2 = a.nz2, line = 2 * nz2;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, nz2 = a.nz2;
     const long long sxy = (long long)ny * nz;
-    const int own = np * nr * line;
+    const int hp = nr * nz2;   // one colour of one own plane
+    const int own = np * 2 * hp;
+    const bool ysplit = nr < ny;
     int *err = a.status;
+
+    // shared memory: delta | src (optional) | x ghosts [2][hp] | y ghosts [np][2][nz2]
+    S *sd = reinterpret_cast<S *>(smem_raw);
+    S *ss = a.src_smem ? sd + own : nullptr;
+    S *gx = sd + own * (a.src_smem ? 2 : 1);
+    S *gy = gx + 2 * hp;
+    auto SD = [&](int p, int c, int j, int t) -> S & { return sd[((p * 2 + c) * nr + j) * nz2 + t]; };
+    auto gidx = [&](int x, int c, int y) -> long long { return (((long long)x * 2 + c) * ny + y) * nz2; };
+    const bool xlo_ghost = x0 - 1 >= 1, xhi_ghost = x1 <= nx - 2;
+    const bool ylo_ghost = ysplit && y0 - 1 >= 1, yhi_ghost = ysplit && y1 <= ny - 2;
     unsigned my_phase = 0;
 
-    // ---- entry: zero delta, optional extrapolated start ------------------
+    // ---- entry: zero delta (shared and own global mirror) and ghosts ------
     for (int e = tid; e < own; e += nth) sd[e] = S(0);
-    for (int e = tid; e < own; e += nth) {
-        int l = e / line, rem = e - l * line;
-        int j = l % nr, p = l / nr;
-        a.delta[((long long)(x0 + p) * ny + (y0 + j)) * line + rem] = S(0);
-    }
+    for (int e = tid; e < 2 * hp + (ysplit ? np * 2 * nz2 : 0); e += nth) gx[e] = S(0);
+    for (int p = 0; p < np; p++)
+        for (int c = 0; c < 2; c++)
+            for (int e = tid; e < hp; e += nth) a.delta[gidx(x0 + p, c, y0) + e] = S(0);
     const int step = a.ctl[0];
     const bool extrap = a.extrapolate && a.ctl[2];
     if (a.extrapolate) {
@@ -206,17 +247,17 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         }
     }
 
-    int its = 0, m_prev = 0, m = max(a.inner_min, min(a.inner_max, a.ctl[1]));
+    int its = 0, m_prev = 0, cycles = 0, m = max(a.inner_min, min(a.inner_max, a.ctl[1]));
     double rel_prev = -1.0, rel = 0.0, maxd = 0.0;
     bool converged = false;
     S last_max = S(0);
 
     while (true) {
-        // delta of every block is final in global memory after this barrier
         if (its > 0) {
             S bm = block_max<S>(last_max);
             if (tid == 0) a.partials[4 * b + 2] = (double)bm;
         }
+        // delta of every block is final in global memory after this barrier
         if (!grid_barrier(a.bar, a.nblocks, err)) return;
 
         // ---- double residual of phi + delta on own interior nodes -------
@@ -226,25 +267,31 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
             int x = x0 + p, y = y0 + j;
             if (y < 1 || y > ny - 2 || k < 1 || k > nz - 2) continue;
             const long long id = x * sxy + (long long)y * nz + k;
-            auto dl = [&](int xx, int yy, int kk) -> double {
-                // delta at (xx,yy,kk): shared memory when owned, else global
-                int c = (xx + yy + kk) & 1;
-                if (xx >= x0 && xx < x1 && yy >= y0 && yy < y1)
-                    return (double)sd[((xx - x0) * nr + (yy - y0)) * line + c * nz2 + (kk >> 1)];
-                return (double)__ldcg(a.delta + ((long long)xx * ny + yy) * line + c * nz2 + (kk >> 1));
-            };
-            double pc = __ldcg(a.phi64 + id) + dl(x, y, k);
-            double pxm = __ldcg(a.phi64 + id - sxy) + dl(x - 1, y, k);
-            double pxp = __ldcg(a.phi64 + id + sxy) + dl(x + 1, y, k);
-            double pym = __ldcg(a.phi64 + id - nz) + dl(x, y - 1, k);
-            double pyp = __ldcg(a.phi64 + id + nz) + dl(x, y + 1, k);
-            double pzm = __ldcg(a.phi64 + id - 1) + dl(x, y, k - 1);
-            double pzp = __ldcg(a.phi64 + id + 1) + dl(x, y, k + 1);
+            const int kh = k >> 1, c0 = (x + y + k) & 1, c1 = c0 ^ 1;
+            // own values from shared memory, neighbours' from their published mirrors
+            double dc = (double)SD(p, c0, j, kh);
+            double dzm = (double)SD(p, c1, j, (k - 1) >> 1), dzp = (double)SD(p, c1, j, (k + 1) >> 1);
+            double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh)
+                               : (x - 1 == 0 ? 0.0 : (double)__ldcg(a.delta + gidx(x - 1, c1, y) + kh));
+            double dxp = p + 1 < np ? (double)SD(p + 1, c1, j, kh)
+                                    : (x + 1 == nx - 1 ? 0.0 : (double)__ldcg(a.delta + gidx(x + 1, c1, y) + kh));
+            double dym = j > 0 ? (double)SD(p, c1, j - 1, kh)
+                               : (y - 1 == 0 ? 0.0 : (double)__ldcg(a.delta + gidx(x, c1, y - 1) + kh));
+            double dyp = j + 1 < nr ? (double)SD(p, c1, j + 1, kh)
+                                    : (y + 1 == ny - 1 ? 0.0 : (double)__ldcg(a.delta + gidx(x, c1, y + 1) + kh));
+            double pc = __ldcg(a.phi64 + id) + dc;
+            double pxm = __ldcg(a.phi64 + id - sxy) + dxm;
+            double pxp = __ldcg(a.phi64 + id + sxy) + dxp;
+            double pym = __ldcg(a.phi64 + id - nz) + dym;
+            double pyp = __ldcg(a.phi64 + id + nz) + dyp;
+            double pzm = __ldcg(a.phi64 + id - 1) + dzm;
+            double pzp = __ldcg(a.phi64 + id + 1) + dzp;
             double bv = a.src_c * (double)__ldg(a.rho + id);
             double r = bv + (pxp + pxm) * a.dhx2i + (pyp + pym) * a.dhy2i + (pzp + pzm) * a.dhz2i - a.ddiag * pc;
             rr += r * r;
             bb += bv * bv;
-            a.src[((long long)x * ny + y) * line + ((x + y + k) & 1) * nz2 + (k >> 1)] = (S)r;
+            if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)r;
+            else a.src[gidx(x, c0, y) + kh] = (S)r;
         }
         block_sum2(rr, bb);
         if (tid == 0) {
@@ -275,6 +322,7 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         __syncthreads();
         rel = s_tot[1] > 0.0 ? sqrt(s_tot[0] / s_tot[1]) : sqrt(s_tot[0]);
         maxd = s_tot[2];
+        cycles++;
 
         // ---- fold: phi += delta, delta = 0 -------------------------------
         for (int e = tid; e < np * nr * nz; e += nth) {
@@ -282,16 +330,13 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
             int x = x0 + p, y = y0 + j;
             if (y < 1 || y > ny - 2 || k < 1 || k > nz - 2) continue;
             const long long id = x * sxy + (long long)y * nz + k;
-            S d = sd[(p * nr + j) * line + ((x + y + k) & 1) * nz2 + (k >> 1)];
-            a.phi64[id] += (double)d;
+            a.phi64[id] += (double)SD(p, (x + y + k) & 1, j, k >> 1);
         }
         __syncthreads();
-        for (int e = tid; e < own; e += nth) {
-            sd[e] = S(0);
-            int l = e / line, rem = e - l * line;
-            int j = l % nr, p = l / nr;
-            a.delta[((long long)(x0 + p) * ny + (y0 + j)) * line + rem] = S(0);
-        }
+        for (int e = tid; e < own; e += nth) sd[e] = S(0);
+        for (int p = 0; p < np; p++)
+            for (int c = 0; c < 2; c++)
+                for (int e = tid; e < hp; e += nth) a.delta[gidx(x0 + p, c, y0) + e] = S(0);
 
         if (a.criterion == HV_SOR_REL_RESIDUAL) converged = rel <= a.tol;
         else converged = its > 0 && maxd < a.tol;
@@ -303,7 +348,7 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
             if (a.criterion == HV_SOR_REL_RESIDUAL && rel_prev > 0.0 && rel < rel_prev && m_prev > 0) {
                 double q = pow(rel / rel_prev, 1.0 / m_prev);
                 double pred = log(a.tol / rel) / log(q);
-                mm = (int)ceil(pred);
+                mm = pred < 1e6 ? (int)ceil(pred) : a.inner_max;
             }
             mm = max(a.inner_min, min(a.inner_max, mm));
             mm = min(mm, a.max_iter - its);
@@ -318,40 +363,47 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         last_max = S(0);
         for (int it = 0; it < m; it++) {
             for (int c = 0; c < 2; c++) {
-                if (!wait_neighbours(a, bx, by, my_phase)) return;
                 const int cp = c ^ 1;
+                if (!wait_neighbours(a, bx, by, my_phase)) return;
+                // neighbours' boundary values of the colour this sweep reads
+                if (xlo_ghost) copy_in(gx, a.delta + gidx(x0 - 1, cp, y0), hp);
+                if (xhi_ghost) copy_in(gx + hp, a.delta + gidx(x1, cp, y0), hp);
+                if (ylo_ghost)
+                    for (int p = 0; p < np; p++) copy_in(gy + (p * 2) * nz2, a.delta + gidx(x0 + p, cp, y0 - 1), nz2);
+                if (yhi_ghost)
+                    for (int p = 0; p < np; p++) copy_in(gy + (p * 2 + 1) * nz2, a.delta + gidx(x0 + p, cp, y1), nz2);
+                __syncthreads();
                 const bool track = (it == m - 1);
-                for (int e = tid; e < np * nr * nz2; e += nth) {
+                for (int e = tid; e < np * hp; e += nth) {
                     const int t = e % nz2, l = e / nz2, j = l % nr, p = l / nr;
                     const int x = x0 + p, y = y0 + j;
                     if (y < 1 || y > ny - 2) continue;
                     const int k = ((c - x - y) & 1) + 2 * t;
                     if (k < 1 || k > nz - 2) continue;
-                    const int base = (p * nr + j) * line;
-                    const int kk = k >> 1;
-                    const S self = sd[base + c * nz2 + t];
-                    const S zm = sd[base + cp * nz2 + ((k - 1) >> 1)];
-                    const S zp = sd[base + cp * nz2 + ((k + 1) >> 1)];
-                    S ym, yp, xm, xp;
-                    if (y - 1 == 0) ym = S(0);
-                    else if (j > 0) ym = sd[base - line + cp * nz2 + kk];
-                    else ym = __ldcg(a.delta + ((long long)x * ny + y - 1) * line + cp * nz2 + kk);
-                    if (y + 1 == ny - 1) yp = S(0);
-                    else if (j + 1 < nr) yp = sd[base + line + cp * nz2 + kk];
-                    else yp = __ldcg(a.delta + ((long long)x * ny + y + 1) * line + cp * nz2 + kk);
-                    if (x - 1 == 0) xm = S(0);
-                    else if (p > 0) xm = sd[base - nr * line + cp * nz2 + kk];
-                    else xm = __ldcg(a.delta + ((long long)(x - 1) * ny + y) * line + cp * nz2 + kk);
-                    if (x + 1 == a.nx - 1) xp = S(0);
-                    else if (p + 1 < np) xp = sd[base + nr * line + cp * nz2 + kk];
-                    else xp = __ldcg(a.delta + ((long long)(x + 1) * ny + y) * line + cp * nz2 + kk);
-                    const long long gi = ((long long)x * ny + y) * line + c * nz2 + t;
-                    const S s = a.src[gi];
+                    const int kh = k >> 1;
+                    S *row = &SD(p, c, j, 0);
+                    const S *orow = &SD(p, cp, j, 0);
+                    const S self = row[t];
+                    const S zm = orow[(k - 1) >> 1], zp = orow[(k + 1) >> 1];
+                    const S ym = (y - 1 == 0) ? S(0) : (j > 0 ? SD(p, cp, j - 1, kh) : gy[(p * 2) * nz2 + kh]);
+                    const S yp = (y + 1 == ny - 1) ? S(0)
+                                                   : (j + 1 < nr ? SD(p, cp, j + 1, kh) : gy[(p * 2 + 1) * nz2 + kh]);
+                    const S xm = p > 0 ? SD(p - 1, cp, j, kh) : gx[j * nz2 + kh];
+                    const S xp = p + 1 < np ? SD(p + 1, cp, j, kh) : gx[hp + j * nz2 + kh];
+                    const S s = ss ? ss[((p * 2 + c) * nr + j) * nz2 + t] : __ldcg(a.src + gidx(x, c, y) + t);
                     const S star = ((xm + xp) * a.hx2i + (ym + yp) * a.hy2i + (zm + zp) * a.hz2i + s) * a.inv_diag;
                     const S nv = self + a.omega * (star - self);
-                    sd[base + c * nz2 + t] = nv;
-                    a.delta[gi] = nv;
+                    row[t] = nv;
                     if (track) last_max = fmax(last_max, fabs(nv - self));
+                }
+                __syncthreads();
+                // publish the own boundary half-planes (all of them when P = 1)
+                for (int p = 0; p < np; p++) {
+                    if (p == 0 || p == np - 1) copy_out(a.delta + gidx(x0 + p, c, y0), &SD(p, c, 0, 0), hp);
+                    else if (ysplit) {
+                        copy_out(a.delta + gidx(x0 + p, c, y0), &SD(p, c, 0, 0), nz2);
+                        copy_out(a.delta + gidx(x0 + p, c, y1 - 1), &SD(p, c, nr - 1, 0), nz2);
+                    }
                 }
                 publish(a.phase + b, ++my_phase);
             }
@@ -362,6 +414,7 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     if (b == 0 && tid == 0) {
         a.status[1] = its;
         a.status[2] = converged ? 1 : 0;
+        a.status[3] = cycles;
         a.metric[0] = a.criterion == HV_SOR_REL_RESIDUAL ? rel : maxd;
         a.ctl[1] = max(m, a.inner_min);
         if (a.extrapolate) a.ctl[2] = 1;
@@ -380,27 +433,32 @@ static hv_status plan_for(hv_ctx *c) {
     const size_t static_smem = 2048;
     const size_t limit = prop.sharedMemPerBlockOptin > static_smem ? prop.sharedMemPerBlockOptin - static_smem : 0;
     const int nz2 = (g.nz + 1) / 2;
-    const size_t line = 2 * (size_t)nz2 * sizeof(S);
     const int interior = g.nx - 2;
     f.ok = false;
-    for (int R = g.ny; R >= 1 && !f.ok; R = (R + 1) / 2 == R ? 0 : (R + 1) / 2) {
-        for (int P = 1; P <= interior; P++) {
-            const size_t smem = (size_t)P * R * line;
-            if (smem > limit) break;
-            const int bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
-            if ((long long)bxn * byn > prop.multiProcessorCount) continue;
-            f.P = P;
-            f.R = R;
-            f.bx = bxn;
-            f.by = byn;
-            f.nblocks = bxn * byn;
-            f.smem = smem;
-            f.ok = true;
-            break;
+    // smallest blocks first (most parallel), y split only when a plane does not fit
+    for (int pass = 0; pass < 2 && !f.ok; pass++) {
+        const bool with_src = pass == 0;
+        for (int R = g.ny; R >= 1 && !f.ok; R = (R == 1) ? 0 : (R + 1) / 2) {
+            for (int P = 1; P <= interior; P++) {
+                const size_t own = (size_t)P * 2 * R * nz2;
+                const size_t ghosts = 2 * (size_t)R * nz2 + (R < g.ny ? (size_t)P * 2 * nz2 : 0);
+                const size_t smem = sizeof(S) * (own * (with_src ? 2 : 1) + ghosts);
+                if (smem > limit) break;
+                const int bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
+                if ((long long)bxn * byn > prop.multiProcessorCount) continue;
+                f.P = P;
+                f.R = R;
+                f.bx = bxn;
+                f.by = byn;
+                f.nblocks = bxn * byn;
+                f.smem = smem;
+                f.src_smem = with_src;
+                f.ok = true;
+                break;
+            }
         }
-        if (R == 1) break;
     }
-    if (!f.ok) return HV_OK;  // the fused path falls back to the plain SOR
+    if (!f.ok) return HV_OK;  // the fused path reports HV_ERR_UNSUPPORTED
     f.nz2 = nz2;
     f.threads = kSorThreads;
     auto kern = c->prec == HV_F64 ? (const void *)k_sor_fast<double, double> : (const void *)k_sor_fast<float, float>;
@@ -411,7 +469,7 @@ static hv_status plan_for(hv_ctx *c) {
         f.ok = false;
         return HV_OK;
     }
-    const size_t n = (size_t)g.nx * g.ny * 2 * nz2;
+    const size_t n = (size_t)g.nx * 2 * g.ny * nz2;
     HV_CUDA(cudaMalloc(&f.delta, n * sizeof(S)));
     HV_CUDA(cudaMalloc(&f.src, n * sizeof(S)));
     HV_CUDA(cudaMemsetAsync(f.delta, 0, n * sizeof(S), c->stream));
@@ -445,7 +503,7 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     const Geom &g = c->geom;
     const hv_sor_params &sp = c->params.sor;
     HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
-    HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 3, c->stream));
+    HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, c->stream));
     SorArgs<T, S> a;
     a.nx = g.nx;
     a.ny = g.ny;
@@ -456,6 +514,7 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.bxn = f.bx;
     a.byn = f.by;
     a.nblocks = f.nblocks;
+    a.src_smem = f.src_smem ? 1 : 0;
     const double dx = 2.0 * g.dmx / g.nx, dy = 2.0 * g.dmy / g.ny, dz = 2.0 * g.dmz / g.nz;
     a.dhx2i = 1.0 / (dx * dx);
     a.dhy2i = 1.0 / (dy * dy);
