@@ -125,4 +125,8 @@ PB208_104K = Workload("208Pb-104k-64^3", Z=82, N=126, ppn=500, n=64, h=0.5, dt=0
 # 208Pb, 10,000 per nucleon (2.08M particles), 128^3, h = 0.25 fm, dt = 0.2, 1000 steps
 PB208_2M = Workload("208Pb-2.08M-128^3", Z=82, N=126, ppn=10000, n=128, h=0.25, dt=0.2, steps=1000)
 
-WORKLOADS = {w.name: w for w in (CA40_SMALL, PB208_104K, PB208_2M)}
+# the 128^3 grid of PB208_2M with 100 test particles per nucleon: the same field
+# kernels with a small particle set, for profiling captures that must stay small
+PB208_20K_128 = Workload("208Pb-20.8k-128^3", Z=82, N=126, ppn=100, n=128, h=0.25, dt=0.2, steps=1000)
+
+WORKLOADS = {w.name: w for w in (CA40_SMALL, PB208_104K, PB208_2M, PB208_20K_128)}
