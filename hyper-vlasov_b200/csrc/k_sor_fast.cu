@@ -226,6 +226,16 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     const bool xlo_ghost = x0 - 1 >= 1, xhi_ghost = x1 <= nx - 2;
     const bool ylo_ghost = ysplit && y0 - 1 >= 1, yhi_ghost = ysplit && y1 <= ny - 2;
     unsigned my_phase = 0;
+    // colour sweeps: thread -> half-line position t_own, rows r_start, +rows_step
+    const int rows_step = max(1, nth / nz2);
+    const int r_start = tid / nz2;
+    const int t_own = r_start < rows_step ? tid % nz2 : nz2;  // nz2 = idle thread
+    const int j_start = r_start % nr, p_start = r_start / nr, dj = rows_step % nr, dp = rows_step / nr;
+    // residual and fold: thread -> z position k_own, rows rz_start, +zrows_step
+    const int zrows_step = max(1, nth / nz);
+    const int rz_start = tid / nz;
+    const int k_own = rz_start < zrows_step ? tid % nz : nz;
+    const int jz_start = rz_start % nr, pz_start = rz_start / nr, djz = zrows_step % nr, dpz = zrows_step / nr;
 
     // ---- entry: zero delta (shared and own global mirror) and ghosts ------
     for (int e = tid; e < own; e += nth) sd[e] = S(0);
@@ -262,10 +272,15 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
 
         // ---- double residual of phi + delta on own interior nodes -------
         double rr = 0.0, bb = 0.0;
-        for (int e = tid; e < np * nr * nz; e += nth) {
-            int k = e % nz, l = e / nz, j = l % nr, p = l / nr;
-            int x = x0 + p, y = y0 + j;
-            if (y < 1 || y > ny - 2 || k < 1 || k > nz - 2) continue;
+        const int k = k_own;
+        for (int l = rz_start, j = jz_start, p = pz_start; k >= 1 && k <= nz - 2 && l < np * nr;
+             l += zrows_step, j += djz, p += dpz) {
+            if (j >= nr) {
+                j -= nr;
+                p++;
+            }
+            const int x = x0 + p, y = y0 + j;
+            if (y < 1 || y > ny - 2) continue;
             const long long id = x * sxy + (long long)y * nz + k;
             const int kh = k >> 1, c0 = (x + y + k) & 1, c1 = c0 ^ 1;
             // own values from shared memory, neighbours' from their published mirrors
@@ -325,10 +340,14 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         cycles++;
 
         // ---- fold: phi += delta, delta = 0 -------------------------------
-        for (int e = tid; e < np * nr * nz; e += nth) {
-            int k = e % nz, l = e / nz, j = l % nr, p = l / nr;
-            int x = x0 + p, y = y0 + j;
-            if (y < 1 || y > ny - 2 || k < 1 || k > nz - 2) continue;
+        for (int l = rz_start, j = jz_start, p = pz_start; k >= 1 && k <= nz - 2 && l < np * nr;
+             l += zrows_step, j += djz, p += dpz) {
+            if (j >= nr) {
+                j -= nr;
+                p++;
+            }
+            const int x = x0 + p, y = y0 + j;
+            if (y < 1 || y > ny - 2) continue;
             const long long id = x * sxy + (long long)y * nz + k;
             a.phi64[id] += (double)SD(p, (x + y + k) & 1, j, k >> 1);
         }
@@ -374,27 +393,37 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
                     for (int p = 0; p < np; p++) copy_in(gy + (p * 2 + 1) * nz2, a.delta + gidx(x0 + p, cp, y1), nz2);
                 __syncthreads();
                 const bool track = (it == m - 1);
-                for (int e = tid; e < np * hp; e += nth) {
-                    const int t = e % nz2, l = e / nz2, j = l % nr, p = l / nr;
-                    const int x = x0 + p, y = y0 + j;
-                    if (y < 1 || y > ny - 2) continue;
-                    const int k = ((c - x - y) & 1) + 2 * t;
-                    if (k < 1 || k > nz - 2) continue;
-                    const int kh = k >> 1;
-                    S *row = &SD(p, c, j, 0);
-                    const S *orow = &SD(p, cp, j, 0);
-                    const S self = row[t];
-                    const S zm = orow[(k - 1) >> 1], zp = orow[(k + 1) >> 1];
-                    const S ym = (y - 1 == 0) ? S(0) : (j > 0 ? SD(p, cp, j - 1, kh) : gy[(p * 2) * nz2 + kh]);
-                    const S yp = (y + 1 == ny - 1) ? S(0)
-                                                   : (j + 1 < nr ? SD(p, cp, j + 1, kh) : gy[(p * 2 + 1) * nz2 + kh]);
-                    const S xm = p > 0 ? SD(p - 1, cp, j, kh) : gx[j * nz2 + kh];
-                    const S xp = p + 1 < np ? SD(p + 1, cp, j, kh) : gx[hp + j * nz2 + kh];
-                    const S s = ss ? ss[((p * 2 + c) * nr + j) * nz2 + t] : __ldcg(a.src + gidx(x, c, y) + t);
-                    const S star = ((xm + xp) * a.hx2i + (ym + yp) * a.hy2i + (zm + zp) * a.hz2i + s) * a.inv_diag;
-                    const S nv = self + a.omega * (star - self);
-                    row[t] = nv;
-                    if (track) last_max = fmax(last_max, fabs(nv - self));
+                // thread -> fixed half-line position t, rows walked without
+                // divisions; rows, half-lines and ghosts on the Dirichlet
+                // boundary hold zeros, so neighbours need no boundary tests
+                if (t_own < nz2) {
+                    int j = j_start, p = p_start;
+                    for (int l = r_start; l < np * nr; l += rows_step) {
+                        const int x = x0 + p, y = y0 + j;
+                        const int kc = (c - x - y) & 1, k = kc + 2 * t_own;
+                        if (y >= 1 && y <= ny - 2 && k >= 1 && k <= nz - 2) {
+                            S *row = sd + ((p * 2 + c) * nr + j) * nz2;
+                            const S *orow = sd + ((p * 2 + cp) * nr + j) * nz2;
+                            const S *ymr = j > 0 ? orow - nz2 : gy + (p * 2) * nz2;
+                            const S *ypr = j + 1 < nr ? orow + nz2 : gy + (p * 2 + 1) * nz2;
+                            const S *xmr = p > 0 ? orow - 2 * hp : gx + j * nz2;
+                            const S *xpr = p + 1 < np ? orow + 2 * hp : gx + hp + j * nz2;
+                            const S s = ss ? ss[(row - sd) + t_own] : __ldcg(a.src + gidx(x, c, y) + t_own);
+                            const S self = row[t_own];
+                            const S zs = orow[t_own + kc - 1] + orow[t_own + kc];
+                            const S star = ((xmr[t_own] + xpr[t_own]) * a.hx2i + (ymr[t_own] + ypr[t_own]) * a.hy2i +
+                                            zs * a.hz2i + s) * a.inv_diag;
+                            const S nv = self + a.omega * (star - self);
+                            row[t_own] = nv;
+                            if (track) last_max = fmax(last_max, fabs(nv - self));
+                        }
+                        j += dj;
+                        p += dp;
+                        if (j >= nr) {
+                            j -= nr;
+                            p++;
+                        }
+                    }
                 }
                 __syncthreads();
                 // publish the own boundary half-planes (all of them when P = 1)
