@@ -37,7 +37,7 @@ constexpr long long kMaxSpin = 1ll << 23;  // ~0.5 s of polling before giving up
 
 template <typename T, typename S>
 struct SorArgs {
-    int nx, ny, nz, nz2, P, R, bxn, byn, nblocks, src_smem;
+    int nx, ny, nz, nz2, P, R, bxn, byn, nblocks, src_smem, vec4;
     S hx2i, hy2i, hz2i, inv_diag, omega;
     double dhx2i, dhy2i, dhz2i, ddiag, src_c;
     double tol;
@@ -116,18 +116,18 @@ __device__ bool wait_neighbours(const SorArgs<T, S> &a, int bx, int by, unsigned
                 }
             }
         }
-        __threadfence();
     }
+    // the acquire above plus the block barrier order the neighbours' published
+    // values before this block's subsequent loads
     __syncthreads();
     return ok;
 }
 
+// Publishes `value` after every thread's prior stores: the block barrier
+// orders them before thread 0's release store at gpu scope.
 __device__ __forceinline__ void publish(unsigned *phase_slot, unsigned value) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        st_release(phase_slot, value);
-    }
+    if (threadIdx.x == 0) st_release(phase_slot, value);
 }
 
 // dst[0..n) = src[0..n) through L2 (the source is written by other blocks),
@@ -198,6 +198,85 @@ __device__ S block_max(S m) {
     return m;
 }
 
+// One SOR update of a node: the reference's phi* and relaxation
+// (include/physics.hpp:114-125) on the correction.
+template <typename S, typename T>
+__device__ __forceinline__ S sor_update(const SorArgs<T, S> &a, S self, S xs, S ys, S zs, S s, bool valid) {
+    const S star = (xs * a.hx2i + ys * a.hy2i + zs * a.hz2i + s) * a.inv_diag;
+    return valid ? self + a.omega * (star - self) : self;
+}
+
+// Colour sweep over own rows, four consecutive same-colour nodes per thread
+// (float correction, nz/2 a multiple of 4, source in shared memory).  Lane i
+// of quad q is the node k = kc + 2 (4 q + i); its z neighbours are the other
+// colour's entries 4 q + i + kc - 1 and 4 q + i + kc of the same row.
+template <typename S, typename T>
+__device__ __forceinline__ void sweep_quads(const SorArgs<T, S> &a, int c, int x0, int y0, int np, int nr, int hp,
+                                            S *sd, const S *ss, const S *gx, const S *gy, int q_own, int r_start,
+                                            int rows_step, int j_start, int p_start, int dj, int dp, bool track,
+                                            S &last_max) {
+    const int nz2 = a.nz2, nq = nz2 / 4, ny = a.ny, nz = a.nz, cp = c ^ 1;
+    if (q_own >= nq) return;
+    int j = j_start, p = p_start;
+    for (int l = r_start; l < np * nr; l += rows_step) {
+        const int x = x0 + p, y = y0 + j;
+        if (y >= 1 && y <= ny - 2) {
+            const int kc = (c - x - y) & 1;
+            const int roff = ((p * 2 + c) * nr + j) * nz2;
+            S *row = sd + roff;
+            const S *orow = sd + ((p * 2 + cp) * nr + j) * nz2;
+            const S *ymr = j > 0 ? orow - nz2 : gy + (p * 2) * nz2;
+            const S *ypr = j + 1 < nr ? orow + nz2 : gy + (p * 2 + 1) * nz2;
+            const S *xmr = p > 0 ? orow - 2 * hp : gx + j * nz2;
+            const S *xpr = p + 1 < np ? orow + 2 * hp : gx + hp + j * nz2;
+            const float4 self = reinterpret_cast<const float4 *>(row)[q_own];
+            const float4 o = reinterpret_cast<const float4 *>(orow)[q_own];
+            const float4 s = reinterpret_cast<const float4 *>(ss + roff)[q_own];
+            const float4 xm = reinterpret_cast<const float4 *>(xmr)[q_own];
+            const float4 xp = reinterpret_cast<const float4 *>(xpr)[q_own];
+            const float4 ym = reinterpret_cast<const float4 *>(ymr)[q_own];
+            const float4 yp = reinterpret_cast<const float4 *>(ypr)[q_own];
+            float z0, z1, z2, z3;  // zm + zp per lane
+            if (kc == 0) {
+                const float left = q_own > 0 ? orow[4 * q_own - 1] : 0.0f;
+                z0 = left + o.x;
+                z1 = o.x + o.y;
+                z2 = o.y + o.z;
+                z3 = o.z + o.w;
+            } else {
+                const float right = q_own + 1 < nq ? orow[4 * q_own + 4] : 0.0f;
+                z0 = o.x + o.y;
+                z1 = o.y + o.z;
+                z2 = o.z + o.w;
+                z3 = o.w + right;
+            }
+            const int kb = kc + 8 * q_own;  // k of lane 0; lanes step by 2
+            float4 nv;
+            nv.x = sor_update<S, T>(a, self.x, xm.x + xp.x, ym.x + yp.x, z0, s.x, kb >= 1 && kb <= nz - 2);
+            nv.y = sor_update<S, T>(a, self.y, xm.y + xp.y, ym.y + yp.y, z1, s.y, kb + 2 >= 1 && kb + 2 <= nz - 2);
+            nv.z = sor_update<S, T>(a, self.z, xm.z + xp.z, ym.z + yp.z, z2, s.z, kb + 4 <= nz - 2);
+            nv.w = sor_update<S, T>(a, self.w, xm.w + xp.w, ym.w + yp.w, z3, s.w, kb + 6 <= nz - 2);
+            reinterpret_cast<float4 *>(row)[q_own] = nv;
+            if (track)
+                last_max = fmax(last_max, fmax(fmax(fabs(nv.x - self.x), fabs(nv.y - self.y)),
+                                               fmax(fabs(nv.z - self.z), fabs(nv.w - self.w))));
+        }
+        j += dj;
+        p += dp;
+        if (j >= nr) {
+            j -= nr;
+            p++;
+        }
+    }
+}
+
+// double corrections never take the quad path
+template <>
+__device__ __forceinline__ void sweep_quads<double, double>(const SorArgs<double, double> &, int, int, int, int, int,
+                                                            int, double *, const double *, const double *,
+                                                            const double *, int, int, int, int, int, int, int, bool,
+                                                            double &) {}
+
 template <typename T, typename S>
 __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -236,6 +315,12 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     const int rz_start = tid / nz;
     const int k_own = rz_start < zrows_step ? tid % nz : nz;
     const int jz_start = rz_start % nr, pz_start = rz_start / nr, djz = zrows_step % nr, dpz = zrows_step / nr;
+    // float4 colour sweeps: thread -> quad q_own (4 same-colour nodes) per row
+    const int nq = nz2 / 4;
+    const int rows_step4 = max(1, nq > 0 ? nth / nq : 1);
+    const int r4_start = nq > 0 ? tid / nq : 0;
+    const int q_own = (nq > 0 && r4_start < rows_step4) ? tid % nq : nq;
+    const int j4_start = r4_start % nr, p4_start = r4_start / nr, dj4 = rows_step4 % nr, dp4 = rows_step4 / nr;
 
     // ---- entry: zero delta (shared and own global mirror) and ghosts ------
     for (int e = tid; e < own; e += nth) sd[e] = S(0);
@@ -396,7 +481,10 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
                 // thread -> fixed half-line position t, rows walked without
                 // divisions; rows, half-lines and ghosts on the Dirichlet
                 // boundary hold zeros, so neighbours need no boundary tests
-                if (t_own < nz2) {
+                if (a.vec4) {
+                    sweep_quads<S>(a, c, x0, y0, np, nr, hp, sd, ss, gx, gy, q_own, r4_start, rows_step4, j4_start,
+                                   p4_start, dj4, dp4, track, last_max);
+                } else if (t_own < nz2) {
                     int j = j_start, p = p_start;
                     for (int l = r_start; l < np * nr; l += rows_step) {
                         const int x = x0 + p, y = y0 + j;
@@ -544,6 +632,7 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.byn = f.by;
     a.nblocks = f.nblocks;
     a.src_smem = f.src_smem ? 1 : 0;
+    a.vec4 = (sizeof(S) == 4 && f.nz2 % 4 == 0 && f.src_smem) ? 1 : 0;
     const double dx = 2.0 * g.dmx / g.nx, dy = 2.0 * g.dmy / g.ny, dz = 2.0 * g.dmz / g.nz;
     a.dhx2i = 1.0 / (dx * dx);
     a.dhy2i = 1.0 / (dy * dy);
