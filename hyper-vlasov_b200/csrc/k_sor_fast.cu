@@ -13,18 +13,19 @@
 // One cooperative launch per solve.  Block b owns P interior x-planes by R
 // rows (all z).  Its delta and, when it fits, its source live in shared
 // memory for the whole solve, in a colour-split layout: within a plane all
-// red nodes of a row are contiguous, then all black nodes, so that a colour
-// sweep reads and writes unit-stride runs and the red (or black) half of a
-// plane is one contiguous block in the global mirror ([x][colour][y][z/2]).
-// A colour sweep is:
+// red nodes of a row are contiguous, then all black nodes, so a colour sweep
+// reads and writes unit-stride runs; the global mirror of delta has the same
+// layout ([x][colour][y][z/2]).  A colour sweep is:
 //   wait for the (up to four) neighbouring blocks' phase counters,
-//   copy their published boundary half-planes (the colour the sweep reads)
-//     into shared ghost buffers with 16-byte loads,
-//   update the own nodes of the colour from shared memory only,
-//   publish the own boundary half-planes to global memory, bump the phase.
-// Grid-wide barriers are used only around the double residual.  Every wait is
-// bounded: on timeout the block records an error word and returns, and the
-// host reports HV_ERR_TIMEOUT.
+//   update the own nodes of the colour -- own neighbours from shared memory,
+//     the neighbouring blocks' from their global mirror rows -- writing each
+//     result to shared memory and to the own mirror row,
+//   bump the own phase counter.
+// The mirror rows of the Dirichlet planes and rows are never written and
+// stay zero, so no neighbour load needs a boundary test.  Grid-wide barriers
+// are used only around the double residual.  Every wait is bounded: on
+// timeout the block records an error word and returns, and the host reports
+// HV_ERR_TIMEOUT.
 #include <cmath>
 
 #include "hv_internal.h"
@@ -33,7 +34,7 @@ namespace hv {
 namespace {
 
 constexpr int kSorThreads = 1024;
-constexpr long long kMaxSpin = 1ll << 23;  // ~0.5 s of polling before giving up
+constexpr long long kMaxSpin = 1ll << 24;  // polls before a wait gives up (~1 s)
 
 template <typename T, typename S>
 struct SorArgs {
@@ -55,14 +56,15 @@ struct SorArgs {
     int ring;
 };
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
     unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 __device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 
 // Grid barrier for co-resident blocks; false when a wait timed out or another
@@ -72,16 +74,15 @@ __device__ bool grid_barrier(unsigned *bar, int nblocks, int *err) {
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        unsigned gen = ld_acquire(bar + 1);
-        __threadfence();
+        unsigned gen = ld_relaxed(bar + 1);
+        fence_acq_rel();
         unsigned arrived = atomicAdd(bar, 1u) + 1u;
         if (arrived == (unsigned)nblocks) {
             atomicExch(bar, 0u);
-            __threadfence();
             st_release(bar + 1, gen + 1u);
         } else {
             long long spin = 0;
-            while (ld_acquire(bar + 1) == gen) {
+            while (ld_relaxed(bar + 1) == gen) {
                 if (++spin > kMaxSpin || ld_volatile(err)) {
                     atomicExch(err, 1);
                     ok = 0;
@@ -89,36 +90,42 @@ __device__ bool grid_barrier(unsigned *bar, int nblocks, int *err) {
                 }
             }
         }
-        __threadfence();
+        fence_acq_rel();
     }
     __syncthreads();
     return ok;
 }
 
-// Waits until every neighbouring block has published `target` phases.
+// Waits until every neighbouring block has published `target` phases: lane q
+// of warp 0 polls neighbour q with relaxed loads, then one acquire fence; the
+// block barrier extends the ordering to every thread.
 template <typename T, typename S>
 __device__ bool wait_neighbours(const SorArgs<T, S> &a, int bx, int by, unsigned target) {
     __shared__ int ok;
-    if (threadIdx.x == 0) {
-        ok = 1;
-        int nbs[4], n = 0;
-        if (bx > 0) nbs[n++] = by * a.bxn + bx - 1;
-        if (bx + 1 < a.bxn) nbs[n++] = by * a.bxn + bx + 1;
-        if (by > 0) nbs[n++] = (by - 1) * a.bxn + bx;
-        if (by + 1 < a.byn) nbs[n++] = (by + 1) * a.bxn + bx;
-        for (int q = 0; q < n && ok; q++) {
+    if (threadIdx.x < 32) {
+        const int q = threadIdx.x;
+        int nb = -1;
+        if (q == 0 && bx > 0) nb = by * a.bxn + bx - 1;
+        if (q == 1 && bx + 1 < a.bxn) nb = by * a.bxn + bx + 1;
+        if (q == 2 && by > 0) nb = (by - 1) * a.bxn + bx;
+        if (q == 3 && by + 1 < a.byn) nb = (by + 1) * a.bxn + bx;
+        int good = 1;
+        if (nb >= 0) {
             long long spin = 0;
-            while (ld_acquire(a.phase + nbs[q]) < target) {
+            while (ld_relaxed(a.phase + nb) < target) {
                 if (++spin > kMaxSpin || ld_volatile(a.status)) {
                     atomicExch(a.status, 1);
-                    ok = 0;
+                    good = 0;
                     break;
                 }
             }
         }
+        good = __all_sync(0xffffffffu, good);
+        if (q == 0) {
+            fence_acq_rel();
+            ok = good;
+        }
     }
-    // the acquire above plus the block barrier order the neighbours' published
-    // values before this block's subsequent loads
     __syncthreads();
     return ok;
 }
@@ -128,32 +135,6 @@ __device__ bool wait_neighbours(const SorArgs<T, S> &a, int bx, int by, unsigned
 __device__ __forceinline__ void publish(unsigned *phase_slot, unsigned value) {
     __syncthreads();
     if (threadIdx.x == 0) st_release(phase_slot, value);
-}
-
-// dst[0..n) = src[0..n) through L2 (the source is written by other blocks),
-// 16 bytes at a time when both ends are aligned.
-template <typename S>
-__device__ __forceinline__ void copy_in(S *dst, const S *src, int n) {
-    constexpr int V = 16 / sizeof(S);
-    if ((n % V) == 0 && (((size_t)src | (size_t)dst) & 15) == 0) {
-        const float4 *s4 = reinterpret_cast<const float4 *>(src);
-        float4 *d4 = reinterpret_cast<float4 *>(dst);
-        for (int i = threadIdx.x; i < n / V; i += blockDim.x) d4[i] = __ldcg(s4 + i);
-    } else {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldcg(src + i);
-    }
-}
-
-template <typename S>
-__device__ __forceinline__ void copy_out(S *dst, const S *src, int n) {
-    constexpr int V = 16 / sizeof(S);
-    if ((n % V) == 0 && (((size_t)src | (size_t)dst) & 15) == 0) {
-        const float4 *s4 = reinterpret_cast<const float4 *>(src);
-        float4 *d4 = reinterpret_cast<float4 *>(dst);
-        for (int i = threadIdx.x; i < n / V; i += blockDim.x) __stcg(d4 + i, s4[i]);
-    } else {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) __stcg(dst + i, src[i]);
-    }
 }
 
 // Deterministic block sum of two doubles (fixed shuffle tree, fixed warp order);
@@ -199,43 +180,62 @@ __device__ S block_max(S m) {
 }
 
 // One SOR update of a node: the reference's phi* and relaxation
-// (include/physics.hpp:114-125) on the correction.
+// (include/physics.hpp:114-125) applied to the correction.
 template <typename S, typename T>
 __device__ __forceinline__ S sor_update(const SorArgs<T, S> &a, S self, S xs, S ys, S zs, S s, bool valid) {
     const S star = (xs * a.hx2i + ys * a.hy2i + zs * a.hz2i + s) * a.inv_diag;
     return valid ? self + a.omega * (star - self) : self;
 }
 
-// Colour sweep over own rows, four consecutive same-colour nodes per thread
-// (float correction, nz/2 a multiple of 4, source in shared memory).  Lane i
-// of quad q is the node k = kc + 2 (4 q + i); its z neighbours are the other
-// colour's entries 4 q + i + kc - 1 and 4 q + i + kc of the same row.
+// Geometry of one block, shared by the sweeps.
+struct Block {
+    int x0, y0, np, nr, nz2, hp, ny;
+    __device__ long long mirror(int x, int c, int y) const { return (((long long)x * 2 + c) * ny + y) * nz2; }
+};
+
+// Neighbour row pointers of own row (p, j), other colour cp.
+template <typename S>
+__device__ __forceinline__ void neighbour_rows(const Block &B, S *sd, const S *mirror, int p, int j, int cp,
+                                               const S *&xm, const S *&xp, const S *&ym, const S *&yp) {
+    const S *orow = sd + ((p * 2 + cp) * B.nr + j) * B.nz2;
+    const int x = B.x0 + p, y = B.y0 + j;
+    xm = p > 0 ? orow - 2 * B.hp : mirror + B.mirror(x - 1, cp, y);
+    xp = p + 1 < B.np ? orow + 2 * B.hp : mirror + B.mirror(x + 1, cp, y);
+    ym = j > 0 ? orow - B.nz2 : mirror + B.mirror(x, cp, y - 1);
+    yp = j + 1 < B.nr ? orow + B.nz2 : mirror + B.mirror(x, cp, y + 1);
+}
+
+template <typename S>
+__device__ __forceinline__ float4 load4(const S *p, int q, bool global) {
+    const float4 *v = reinterpret_cast<const float4 *>(p) + q;
+    return global ? __ldcg(v) : *v;
+}
+
+// Colour sweep, four consecutive same-colour nodes per thread (float
+// correction, nz/2 a multiple of 4, source in shared memory).  Lane i of quad
+// q is the node k = kc + 2 (4 q + i); its z neighbours are the other colour's
+// entries 4 q + i + kc - 1 and 4 q + i + kc of the same row.
 template <typename S, typename T>
-__device__ __forceinline__ void sweep_quads(const SorArgs<T, S> &a, int c, int x0, int y0, int np, int nr, int hp,
-                                            S *sd, const S *ss, const S *gx, const S *gy, int q_own, int r_start,
-                                            int rows_step, int j_start, int p_start, int dj, int dp, bool track,
-                                            S &last_max) {
+__device__ __forceinline__ void sweep_quads(const SorArgs<T, S> &a, const Block &B, int c, S *sd, const S *ss,
+                                            int q_own, int r_start, int rows_step, int j_start, int p_start, int dj,
+                                            int dp, bool track, S &last_max) {
     const int nz2 = a.nz2, nq = nz2 / 4, ny = a.ny, nz = a.nz, cp = c ^ 1;
     if (q_own >= nq) return;
     int j = j_start, p = p_start;
-    for (int l = r_start; l < np * nr; l += rows_step) {
-        const int x = x0 + p, y = y0 + j;
+    for (int l = r_start; l < B.np * B.nr; l += rows_step) {
+        const int x = B.x0 + p, y = B.y0 + j;
         if (y >= 1 && y <= ny - 2) {
             const int kc = (c - x - y) & 1;
-            const int roff = ((p * 2 + c) * nr + j) * nz2;
+            const int roff = ((p * 2 + c) * B.nr + j) * nz2;
             S *row = sd + roff;
-            const S *orow = sd + ((p * 2 + cp) * nr + j) * nz2;
-            const S *ymr = j > 0 ? orow - nz2 : gy + (p * 2) * nz2;
-            const S *ypr = j + 1 < nr ? orow + nz2 : gy + (p * 2 + 1) * nz2;
-            const S *xmr = p > 0 ? orow - 2 * hp : gx + j * nz2;
-            const S *xpr = p + 1 < np ? orow + 2 * hp : gx + hp + j * nz2;
+            const S *orow = sd + ((p * 2 + cp) * B.nr + j) * nz2;
+            const S *xmr, *xpr, *ymr, *ypr;
+            neighbour_rows(B, sd, a.delta, p, j, cp, xmr, xpr, ymr, ypr);
+            const float4 xm = load4(xmr, q_own, p == 0), xp = load4(xpr, q_own, p + 1 == B.np);
+            const float4 ym = load4(ymr, q_own, j == 0), yp = load4(ypr, q_own, j + 1 == B.nr);
             const float4 self = reinterpret_cast<const float4 *>(row)[q_own];
             const float4 o = reinterpret_cast<const float4 *>(orow)[q_own];
             const float4 s = reinterpret_cast<const float4 *>(ss + roff)[q_own];
-            const float4 xm = reinterpret_cast<const float4 *>(xmr)[q_own];
-            const float4 xp = reinterpret_cast<const float4 *>(xpr)[q_own];
-            const float4 ym = reinterpret_cast<const float4 *>(ymr)[q_own];
-            const float4 yp = reinterpret_cast<const float4 *>(ypr)[q_own];
             float z0, z1, z2, z3;  // zm + zp per lane
             if (kc == 0) {
                 const float left = q_own > 0 ? orow[4 * q_own - 1] : 0.0f;
@@ -253,18 +253,19 @@ __device__ __forceinline__ void sweep_quads(const SorArgs<T, S> &a, int c, int x
             const int kb = kc + 8 * q_own;  // k of lane 0; lanes step by 2
             float4 nv;
             nv.x = sor_update<S, T>(a, self.x, xm.x + xp.x, ym.x + yp.x, z0, s.x, kb >= 1 && kb <= nz - 2);
-            nv.y = sor_update<S, T>(a, self.y, xm.y + xp.y, ym.y + yp.y, z1, s.y, kb + 2 >= 1 && kb + 2 <= nz - 2);
+            nv.y = sor_update<S, T>(a, self.y, xm.y + xp.y, ym.y + yp.y, z1, s.y, kb + 2 <= nz - 2);
             nv.z = sor_update<S, T>(a, self.z, xm.z + xp.z, ym.z + yp.z, z2, s.z, kb + 4 <= nz - 2);
             nv.w = sor_update<S, T>(a, self.w, xm.w + xp.w, ym.w + yp.w, z3, s.w, kb + 6 <= nz - 2);
             reinterpret_cast<float4 *>(row)[q_own] = nv;
+            __stcg(reinterpret_cast<float4 *>(a.delta + B.mirror(x, c, y)) + q_own, nv);
             if (track)
                 last_max = fmax(last_max, fmax(fmax(fabs(nv.x - self.x), fabs(nv.y - self.y)),
                                                fmax(fabs(nv.z - self.z), fabs(nv.w - self.w))));
         }
         j += dj;
         p += dp;
-        if (j >= nr) {
-            j -= nr;
+        if (j >= B.nr) {
+            j -= B.nr;
             p++;
         }
     }
@@ -272,10 +273,47 @@ __device__ __forceinline__ void sweep_quads(const SorArgs<T, S> &a, int c, int x
 
 // double corrections never take the quad path
 template <>
-__device__ __forceinline__ void sweep_quads<double, double>(const SorArgs<double, double> &, int, int, int, int, int,
-                                                            int, double *, const double *, const double *,
-                                                            const double *, int, int, int, int, int, int, int, bool,
-                                                            double &) {}
+__device__ __forceinline__ void sweep_quads<double, double>(const SorArgs<double, double> &, const Block &, int,
+                                                            double *, const double *, int, int, int, int, int, int,
+                                                            int, bool, double &) {}
+
+// Colour sweep, one node per thread per row (any size and type).
+template <typename S, typename T>
+__device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block &B, int c, S *sd, const S *ss,
+                                             int t_own, int r_start, int rows_step, int j_start, int p_start, int dj,
+                                             int dp, bool track, S &last_max) {
+    const int nz2 = a.nz2, ny = a.ny, nz = a.nz, cp = c ^ 1;
+    if (t_own >= nz2) return;
+    int j = j_start, p = p_start;
+    for (int l = r_start; l < B.np * B.nr; l += rows_step) {
+        const int x = B.x0 + p, y = B.y0 + j;
+        const int kc = (c - x - y) & 1, k = kc + 2 * t_own;
+        if (y >= 1 && y <= ny - 2 && k >= 1 && k <= nz - 2) {
+            const int roff = ((p * 2 + c) * B.nr + j) * nz2;
+            S *row = sd + roff;
+            const S *orow = sd + ((p * 2 + cp) * B.nr + j) * nz2;
+            const S *xmr, *xpr, *ymr, *ypr;
+            neighbour_rows(B, sd, a.delta, p, j, cp, xmr, xpr, ymr, ypr);
+            const S xm = p == 0 ? __ldcg(xmr + t_own) : xmr[t_own];
+            const S xp = p + 1 == B.np ? __ldcg(xpr + t_own) : xpr[t_own];
+            const S ym = j == 0 ? __ldcg(ymr + t_own) : ymr[t_own];
+            const S yp = j + 1 == B.nr ? __ldcg(ypr + t_own) : ypr[t_own];
+            const S s = ss ? ss[roff + t_own] : __ldcg(a.src + B.mirror(x, c, y) + t_own);
+            const S self = row[t_own];
+            const S zs = orow[t_own + kc - 1] + orow[t_own + kc];
+            const S nv = sor_update<S, T>(a, self, xm + xp, ym + yp, zs, s, true);
+            row[t_own] = nv;
+            __stcg(a.delta + B.mirror(x, c, y) + t_own, nv);
+            if (track) last_max = fmax(last_max, fabs(nv - self));
+        }
+        j += dj;
+        p += dp;
+        if (j >= B.nr) {
+            j -= B.nr;
+            p++;
+        }
+    }
+}
 
 template <typename T, typename S>
 __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
@@ -288,46 +326,40 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     const int x0 = 1 + bx * a.P, x1 = min(x0 + a.P, a.nx - 1);
     const int y0 = by * a.R, y1 = min(y0 + a.R, a.ny);
     const int np = x1 - x0, nr = y1 - y0;
-    const int nx = a.nx, ny = a.ny, nz = a.nz, nz2 = a.nz2;
+    const int ny = a.ny, nz = a.nz, nz2 = a.nz2;
     const long long sxy = (long long)ny * nz;
     const int hp = nr * nz2;   // one colour of one own plane
     const int own = np * 2 * hp;
-    const bool ysplit = nr < ny;
     int *err = a.status;
+    const Block B{x0, y0, np, nr, nz2, hp, ny};
 
-    // shared memory: delta | src (optional) | x ghosts [2][hp] | y ghosts [np][2][nz2]
+    // shared memory: delta | src (when it fits)
     S *sd = reinterpret_cast<S *>(smem_raw);
     S *ss = a.src_smem ? sd + own : nullptr;
-    S *gx = sd + own * (a.src_smem ? 2 : 1);
-    S *gy = gx + 2 * hp;
     auto SD = [&](int p, int c, int j, int t) -> S & { return sd[((p * 2 + c) * nr + j) * nz2 + t]; };
-    auto gidx = [&](int x, int c, int y) -> long long { return (((long long)x * 2 + c) * ny + y) * nz2; };
-    const bool xlo_ghost = x0 - 1 >= 1, xhi_ghost = x1 <= nx - 2;
-    const bool ylo_ghost = ysplit && y0 - 1 >= 1, yhi_ghost = ysplit && y1 <= ny - 2;
     unsigned my_phase = 0;
     // colour sweeps: thread -> half-line position t_own, rows r_start, +rows_step
     const int rows_step = max(1, nth / nz2);
     const int r_start = tid / nz2;
     const int t_own = r_start < rows_step ? tid % nz2 : nz2;  // nz2 = idle thread
     const int j_start = r_start % nr, p_start = r_start / nr, dj = rows_step % nr, dp = rows_step / nr;
-    // residual and fold: thread -> z position k_own, rows rz_start, +zrows_step
-    const int zrows_step = max(1, nth / nz);
-    const int rz_start = tid / nz;
-    const int k_own = rz_start < zrows_step ? tid % nz : nz;
-    const int jz_start = rz_start % nr, pz_start = rz_start / nr, djz = zrows_step % nr, dpz = zrows_step / nr;
     // float4 colour sweeps: thread -> quad q_own (4 same-colour nodes) per row
     const int nq = nz2 / 4;
     const int rows_step4 = max(1, nq > 0 ? nth / nq : 1);
     const int r4_start = nq > 0 ? tid / nq : 0;
     const int q_own = (nq > 0 && r4_start < rows_step4) ? tid % nq : nq;
     const int j4_start = r4_start % nr, p4_start = r4_start / nr, dj4 = rows_step4 % nr, dp4 = rows_step4 / nr;
+    // residual and fold: thread -> z position k_own, rows rz_start, +zrows_step
+    const int zrows_step = max(1, nth / nz);
+    const int rz_start = tid / nz;
+    const int k_own = rz_start < zrows_step ? tid % nz : nz;
+    const int jz_start = rz_start % nr, pz_start = rz_start / nr, djz = zrows_step % nr, dpz = zrows_step / nr;
 
-    // ---- entry: zero delta (shared and own global mirror) and ghosts ------
+    // ---- entry: zero delta (shared and own global mirror) -----------------
     for (int e = tid; e < own; e += nth) sd[e] = S(0);
-    for (int e = tid; e < 2 * hp + (ysplit ? np * 2 * nz2 : 0); e += nth) gx[e] = S(0);
     for (int p = 0; p < np; p++)
         for (int c = 0; c < 2; c++)
-            for (int e = tid; e < hp; e += nth) a.delta[gidx(x0 + p, c, y0) + e] = S(0);
+            for (int e = tid; e < hp; e += nth) a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
     const int step = a.ctl[0];
     const bool extrap = a.extrapolate && a.ctl[2];
     if (a.extrapolate) {
@@ -368,17 +400,16 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
             if (y < 1 || y > ny - 2) continue;
             const long long id = x * sxy + (long long)y * nz + k;
             const int kh = k >> 1, c0 = (x + y + k) & 1, c1 = c0 ^ 1;
-            // own values from shared memory, neighbours' from their published mirrors
+            // own values from shared memory, other blocks' from their mirrors
+            // (zero on the Dirichlet planes and rows)
             double dc = (double)SD(p, c0, j, kh);
             double dzm = (double)SD(p, c1, j, (k - 1) >> 1), dzp = (double)SD(p, c1, j, (k + 1) >> 1);
-            double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh)
-                               : (x - 1 == 0 ? 0.0 : (double)__ldcg(a.delta + gidx(x - 1, c1, y) + kh));
-            double dxp = p + 1 < np ? (double)SD(p + 1, c1, j, kh)
-                                    : (x + 1 == nx - 1 ? 0.0 : (double)__ldcg(a.delta + gidx(x + 1, c1, y) + kh));
-            double dym = j > 0 ? (double)SD(p, c1, j - 1, kh)
-                               : (y - 1 == 0 ? 0.0 : (double)__ldcg(a.delta + gidx(x, c1, y - 1) + kh));
-            double dyp = j + 1 < nr ? (double)SD(p, c1, j + 1, kh)
-                                    : (y + 1 == ny - 1 ? 0.0 : (double)__ldcg(a.delta + gidx(x, c1, y + 1) + kh));
+            double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh) : (double)__ldcg(a.delta + B.mirror(x - 1, c1, y) + kh);
+            double dxp =
+                p + 1 < np ? (double)SD(p + 1, c1, j, kh) : (double)__ldcg(a.delta + B.mirror(x + 1, c1, y) + kh);
+            double dym = j > 0 ? (double)SD(p, c1, j - 1, kh) : (double)__ldcg(a.delta + B.mirror(x, c1, y - 1) + kh);
+            double dyp =
+                j + 1 < nr ? (double)SD(p, c1, j + 1, kh) : (double)__ldcg(a.delta + B.mirror(x, c1, y + 1) + kh);
             double pc = __ldcg(a.phi64 + id) + dc;
             double pxm = __ldcg(a.phi64 + id - sxy) + dxm;
             double pxp = __ldcg(a.phi64 + id + sxy) + dxp;
@@ -391,7 +422,7 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
             rr += r * r;
             bb += bv * bv;
             if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)r;
-            else a.src[gidx(x, c0, y) + kh] = (S)r;
+            else a.src[B.mirror(x, c0, y) + kh] = (S)r;
         }
         block_sum2(rr, bb);
         if (tid == 0) {
@@ -440,7 +471,7 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         for (int e = tid; e < own; e += nth) sd[e] = S(0);
         for (int p = 0; p < np; p++)
             for (int c = 0; c < 2; c++)
-                for (int e = tid; e < hp; e += nth) a.delta[gidx(x0 + p, c, y0) + e] = S(0);
+                for (int e = tid; e < hp; e += nth) a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
 
         if (a.criterion == HV_SOR_REL_RESIDUAL) converged = rel <= a.tol;
         else converged = its > 0 && maxd < a.tol;
@@ -467,61 +498,14 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         last_max = S(0);
         for (int it = 0; it < m; it++) {
             for (int c = 0; c < 2; c++) {
-                const int cp = c ^ 1;
                 if (!wait_neighbours(a, bx, by, my_phase)) return;
-                // neighbours' boundary values of the colour this sweep reads
-                if (xlo_ghost) copy_in(gx, a.delta + gidx(x0 - 1, cp, y0), hp);
-                if (xhi_ghost) copy_in(gx + hp, a.delta + gidx(x1, cp, y0), hp);
-                if (ylo_ghost)
-                    for (int p = 0; p < np; p++) copy_in(gy + (p * 2) * nz2, a.delta + gidx(x0 + p, cp, y0 - 1), nz2);
-                if (yhi_ghost)
-                    for (int p = 0; p < np; p++) copy_in(gy + (p * 2 + 1) * nz2, a.delta + gidx(x0 + p, cp, y1), nz2);
-                __syncthreads();
                 const bool track = (it == m - 1);
-                // thread -> fixed half-line position t, rows walked without
-                // divisions; rows, half-lines and ghosts on the Dirichlet
-                // boundary hold zeros, so neighbours need no boundary tests
-                if (a.vec4) {
-                    sweep_quads<S>(a, c, x0, y0, np, nr, hp, sd, ss, gx, gy, q_own, r4_start, rows_step4, j4_start,
-                                   p4_start, dj4, dp4, track, last_max);
-                } else if (t_own < nz2) {
-                    int j = j_start, p = p_start;
-                    for (int l = r_start; l < np * nr; l += rows_step) {
-                        const int x = x0 + p, y = y0 + j;
-                        const int kc = (c - x - y) & 1, k = kc + 2 * t_own;
-                        if (y >= 1 && y <= ny - 2 && k >= 1 && k <= nz - 2) {
-                            S *row = sd + ((p * 2 + c) * nr + j) * nz2;
-                            const S *orow = sd + ((p * 2 + cp) * nr + j) * nz2;
-                            const S *ymr = j > 0 ? orow - nz2 : gy + (p * 2) * nz2;
-                            const S *ypr = j + 1 < nr ? orow + nz2 : gy + (p * 2 + 1) * nz2;
-                            const S *xmr = p > 0 ? orow - 2 * hp : gx + j * nz2;
-                            const S *xpr = p + 1 < np ? orow + 2 * hp : gx + hp + j * nz2;
-                            const S s = ss ? ss[(row - sd) + t_own] : __ldcg(a.src + gidx(x, c, y) + t_own);
-                            const S self = row[t_own];
-                            const S zs = orow[t_own + kc - 1] + orow[t_own + kc];
-                            const S star = ((xmr[t_own] + xpr[t_own]) * a.hx2i + (ymr[t_own] + ypr[t_own]) * a.hy2i +
-                                            zs * a.hz2i + s) * a.inv_diag;
-                            const S nv = self + a.omega * (star - self);
-                            row[t_own] = nv;
-                            if (track) last_max = fmax(last_max, fabs(nv - self));
-                        }
-                        j += dj;
-                        p += dp;
-                        if (j >= nr) {
-                            j -= nr;
-                            p++;
-                        }
-                    }
-                }
-                __syncthreads();
-                // publish the own boundary half-planes (all of them when P = 1)
-                for (int p = 0; p < np; p++) {
-                    if (p == 0 || p == np - 1) copy_out(a.delta + gidx(x0 + p, c, y0), &SD(p, c, 0, 0), hp);
-                    else if (ysplit) {
-                        copy_out(a.delta + gidx(x0 + p, c, y0), &SD(p, c, 0, 0), nz2);
-                        copy_out(a.delta + gidx(x0 + p, c, y1 - 1), &SD(p, c, nr - 1, 0), nz2);
-                    }
-                }
+                if (a.vec4)
+                    sweep_quads<S>(a, B, c, sd, ss, q_own, r4_start, rows_step4, j4_start, p4_start, dj4, dp4, track,
+                                   last_max);
+                else
+                    sweep_scalar<S>(a, B, c, sd, ss, t_own, r_start, rows_step, j_start, p_start, dj, dp, track,
+                                    last_max);
                 publish(a.phase + b, ++my_phase);
             }
         }
@@ -552,14 +536,14 @@ static hv_status plan_for(hv_ctx *c) {
     const int nz2 = (g.nz + 1) / 2;
     const int interior = g.nx - 2;
     f.ok = false;
-    // smallest blocks first (most parallel), y split only when a plane does not fit
+    // smallest blocks first (most parallel), the source in shared memory when
+    // it fits, a y split only when a plane does not fit
     for (int pass = 0; pass < 2 && !f.ok; pass++) {
         const bool with_src = pass == 0;
         for (int R = g.ny; R >= 1 && !f.ok; R = (R == 1) ? 0 : (R + 1) / 2) {
             for (int P = 1; P <= interior; P++) {
                 const size_t own = (size_t)P * 2 * R * nz2;
-                const size_t ghosts = 2 * (size_t)R * nz2 + (R < g.ny ? (size_t)P * 2 * nz2 : 0);
-                const size_t smem = sizeof(S) * (own * (with_src ? 2 : 1) + ghosts);
+                const size_t smem = sizeof(S) * own * (with_src ? 2 : 1);
                 if (smem > limit) break;
                 const int bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
                 if ((long long)bxn * byn > prop.multiProcessorCount) continue;
@@ -586,6 +570,7 @@ static hv_status plan_for(hv_ctx *c) {
         f.ok = false;
         return HV_OK;
     }
+    // mirrors cover every plane and row, so the Dirichlet ones stay zero
     const size_t n = (size_t)g.nx * 2 * g.ny * nz2;
     HV_CUDA(cudaMalloc(&f.delta, n * sizeof(S)));
     HV_CUDA(cudaMalloc(&f.src, n * sizeof(S)));
