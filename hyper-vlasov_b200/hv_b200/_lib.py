@@ -126,6 +126,7 @@ SIGNATURES = {
     "hv_drift": (_S, [_P, _D]),
     "hv_excite": (_S, [_P, _D]),
     "hv_observe": (_S, [_P, _P]),
+    "hv_observe_noalloc": (_S, [_P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
     "hv_fast_options_default": (None, [_P]),
     "hv_ctx_set_fast_options": (_S, [_P, _P]),
     "hv_ctx_get_fast_options": (_S, [_P, _P]),

@@ -264,6 +264,25 @@ HV_API hv_status hv_excite(hv_ctx *ctx, double eta);
  * (include/tools.hpp:302-325) of both species, summed in double. */
 HV_API hv_status hv_observe(hv_ctx *ctx, hv_observables *out);
 
+/* Observables (as hv_observe) of particle arrays held in the caller's device
+ * memory, computed without allocating any device memory.  No counterpart in
+ * the reference: it is for callers that cannot call cudaMalloc, such as a
+ * host framework that has reserved the GPU's memory for its own allocator, or
+ * code running where allocation is not permitted.  The caller passes the
+ * inputs (x, y, z: protons + neutrons values of the precision's type, protons
+ * first) and receives *out on the host; D uses nucleus_z and nucleus_n.
+ * Scratch is a fixed 256 KiB array inside the library, held by every GPU that
+ * loads it until the process exits; one call handles at most
+ * HV_NOALLOC_MAX_PARTICLES particles and rejects more with HV_ERR_BAD_ARG.
+ * The first call on a device looks up the array's device address (do that
+ * call before any stream capture).  All calls share the array: calls whose
+ * work overlaps on the GPU race.  Work is queued on `stream` (a cudaStream_t,
+ * NULL for the default stream) and the call returns after it completes. */
+#define HV_NOALLOC_MAX_PARTICLES (4096 * 1024)
+HV_API hv_status hv_observe_noalloc(const hv_world *world, int protons, int neutrons, int nucleus_z,
+                                    int nucleus_n, hv_precision prec, const void *x, const void *y,
+                                    const void *z, void *stream, hv_observables *out);
+
 /* ---- fused-path options ------------------------------------------------ */
 
 /* SOR starting guess of each step's solve in the fused path. */

@@ -1,0 +1,67 @@
+"""GPU: hv_observe_noalloc, the observables reduction for callers that cannot
+allocate device memory (a framework that owns the GPU's memory, or a region
+where allocation is not permitted).
+
+It is called through the C ABI on particle arrays that live in device memory
+the test owns, and its result is compared with the context-based hv_observe on
+the same particles, within the tolerance of the other observable tests
+(1e-12 on centres of mass, 1e-11 on mean squared radii), on two calls in a row
+with different particles.  This file is collected last so that a run that
+stops at the first failure has run every other test first.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lib, L, w, prec, xs, stream):
+    out = L.hv_observables()
+    st = lib.hv_observe_noalloc(C.byref(w.world()), w.protons, w.neutrons, w.Z, w.N, prec,
+                                C.c_void_p(xs[0].data_ptr()), C.c_void_p(xs[1].data_ptr()),
+                                C.c_void_p(xs[2].data_ptr()), C.c_void_p(stream), C.byref(out))
+    return st, out
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_noalloc_observe_matches_context_observe_twice(hv, dtype):
+    import torch
+    from hv_b200 import _lib as L
+    lib = L.load()
+    w = hv.CA40_SMALL
+    npdt = np.float64 if dtype == "f64" else np.float32
+    prec = hv.HV_F64 if dtype == "f64" else hv.HV_F32
+    parts = hv.workload_particles(w, npdt)
+    stream = torch.cuda.current_stream().cuda_stream
+    with hv.Session.from_workload(w, prec, device=0) as s:
+        for call in range(2):
+            if call == 1:  # different particles on the second call, same sizes
+                parts[2] = (parts[2] + npdt(0.75)).astype(npdt)
+                parts[0] = (parts[0] * npdt(1.3)).astype(npdt)
+            s.upload_particles(*parts)
+            ref = s.observe()
+            xs = [torch.from_numpy(p.copy()).cuda() for p in parts[:3]]
+            torch.cuda.synchronize()
+            st, got = _noalloc(lib, L, w, prec, xs, stream)
+            assert st == L.HV_OK, lib.hv_last_error()
+            assert abs(got.zcm_p - ref.zcm_p) < 1e-12 and abs(got.zcm_n - ref.zcm_n) < 1e-12
+            assert abs(got.rms_p ** 2 - ref.rms_p ** 2) < 1e-11 and abs(got.rms_n ** 2 - ref.rms_n ** 2) < 1e-11
+            assert abs(got.dipole - ref.dipole) < 1e-11
+
+
+def test_noalloc_observe_rejects_more_than_its_scratch(hv):
+    import torch
+    from hv_b200 import _lib as L
+    lib = L.load()
+    w = hv.CA40_SMALL
+    x = torch.zeros(4, dtype=torch.float64, device="cuda")
+    out = L.hv_observables()
+    too_many = 4096 * 1024 + 1
+    st = lib.hv_observe_noalloc(C.byref(w.world()), too_many, 0, w.Z, w.N, hv.HV_F64, C.c_void_p(x.data_ptr()),
+                                C.c_void_p(x.data_ptr()), C.c_void_p(x.data_ptr()), None, C.byref(out))
+    assert st == L.HV_ERR_BAD_ARG
+    assert b"4194304" in lib.hv_last_error()
