@@ -132,6 +132,7 @@ SIGNATURES = {
     "hv_ctx_get_fast_options": (_S, [_P, _P]),
     "hv_ctx_set_profiling": (_S, [_P, _I]),
     "hv_ctx_kernel_times": (_S, [_P, _P, _P, _I]),
+    "hv_write_vtk": (_S, [_P, C.c_char_p]),
     "hv_initial_solve": (_S, [_P, _P]),
     "hv_run": (_S, [_P, _I, _I, _P]),
     "hv_simulate": (_S, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),

@@ -220,6 +220,11 @@ class Session:
         L.check(self.lib.hv_observe(self._ctx, C.byref(o)), "hv_observe")
         return o
 
+    def write_vtk(self, path):
+        """One VTK frame of the current forces, density and potential in the
+        reference's format (include/init.hpp:159-254)."""
+        L.check(self.lib.hv_write_vtk(self._ctx, str(path).encode()), "hv_write_vtk")
+
     def initial_solve(self):
         it = C.c_int(0)
         L.check(self.lib.hv_initial_solve(self._ctx, C.byref(it)), "hv_initial_solve")

@@ -324,6 +324,15 @@ typedef enum hv_kernel_id {
 HV_API hv_status hv_ctx_set_profiling(hv_ctx *ctx, int enable);
 HV_API hv_status hv_ctx_kernel_times(hv_ctx *ctx, double *total_ms, int *launches, int n);
 
+/* ---- output ------------------------------------------------------------ */
+
+/* Writes the context's forces, density and potential as one VTK frame in the
+ * reference's format (output_vtk_header_start, output_vector_field,
+ * output_scalar_field: include/init.hpp:159-254; the frame of
+ * src/hyper_vlasov.cpp:72-84): ASCII STRUCTURED_POINTS header, big-endian
+ * float32 blocks with x varying fastest. */
+HV_API hv_status hv_write_vtk(hv_ctx *ctx, const char *path);
+
 /* ---- whole-step drivers ----------------------------------------------- */
 
 /* The initial field solve of cpu_simulate (src/hyper_vlasov.cpp:53-62):

@@ -338,6 +338,13 @@ class Reference:
         n, d = self._w(world)
         return f(n, d, protons, neutrons, _ptr(x), _ptr(y), _ptr(z), species)
 
+    def write_vtk(self, path, world, Fx, Fy, Fz, rho, U):
+        """The reference's VTK frame writer (include/init.hpp:159-254)."""
+        n, d = self._w(world)
+        f = self._f("write_vtk")
+        f.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p] + [C.c_void_p] * 5
+        return f(str(path).encode(), n, d, _ptr(Fx), _ptr(Fy), _ptr(Fz), _ptr(rho), _ptr(U))
+
     def simulate(self, world, run: RunSpec, protons, neutrons, x, y, z, kx, ky, kz, steps,
                  smooth_mode=1, want_fields=False, step_times=False):
         """The cpu_simulate loop with the reference's routines (its SOR is

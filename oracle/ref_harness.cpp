@@ -141,3 +141,23 @@ REF_API(float, f)
 // particle-order summation of the deposit's array reduction, tools.hpp:45).
 extern "C" void ref_set_threads(int n) { omp_set_num_threads(n); }
 extern "C" int ref_get_threads(void) { return omp_get_max_threads(); }
+
+// The reference's VTK frame writer (include/init.hpp:159-254) in the order of
+// src/hyper_vlasov.cpp:79-82: header, forces, density, potentials.
+#define REF_VTK(T, S)                                                                                \
+    extern "C" int ref_write_vtk_##S(const char *path, const int *n, const double *dm, T *Fx, T *Fy, \
+                                     T *Fz, T *rho, T *U) {                                          \
+        World<T> w = mk_world<T>(n, dm);                                                             \
+        FILE *out = std::fopen(path, "wb");                                                          \
+        if (!out) return 1;                                                                          \
+        VectorField<T> f{Fx, Fy, Fz};                                                                \
+        ScalarField<T> d{rho}, u{U};                                                                 \
+        output_vtk_header_start(out, w);                                                             \
+        output_vector_field(out, f, w, "forces");                                                    \
+        output_scalar_field(out, d, w, "density");                                                   \
+        output_scalar_field(out, u, w, "potentials");                                                \
+        std::fclose(out);                                                                            \
+        return 0;                                                                                    \
+    }
+REF_VTK(double, d)
+REF_VTK(float, f)
