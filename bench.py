@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--workload", default="208Pb-2.08M-128^3")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--warm-start", choices=["previous", "extrapolate"], default="previous")
+    ap.add_argument("--sor-exchange", choices=["auto", "flags"], default="auto")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -258,7 +259,8 @@ def our_arm(args, world, rank, local):
     torch.cuda.set_device(local)
 
     sess = hv.Session.from_workload(w, prec, device=local)
-    sess.set_fast_options(sor_warm_start=warm_mode)
+    sess.set_fast_options(sor_warm_start=warm_mode, sor_exchange=hv.HV_SOR_EXCHANGE_FLAGS
+                          if args.sor_exchange == "flags" else hv.HV_SOR_EXCHANGE_AUTO)
     sess.upload_particles(*parts)
     sess.run(W, hv.HV_PATH_FUSED)  # includes the initial field solve
     stream = torch.cuda.ExternalStream(sess.stream())
@@ -322,7 +324,7 @@ def our_arm(args, world, rank, local):
         "config": {"workload": w.name, "nucleus": f"208Pb (Z={w.Z}, N={w.N})", "particles": w.particles,
                    "grid": f"{w.n}^3", "h_fm": w.h, "dt_fm_c": w.dt,
                    "sor": f"red-black omega {w.sor_omega} to relative residual {w.sor_tol:g}",
-                   "warm_start": args.warm_start, "path": "fused",
+                   "warm_start": args.warm_start, "sor_exchange": args.sor_exchange, "path": "fused",
                    "precision": "f32 particles/grids, f64 phi, SOR residual and observable sums",
                    "parallelism": f"replicas x{world}",
                    "l2": "working set larger than L2 (particle state 50 MB + 2x128^3 fields ~120 MB)"},

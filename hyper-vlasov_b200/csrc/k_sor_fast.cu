@@ -26,6 +26,18 @@
 // are used only around the double residual.  Every wait is bounded: on
 // timeout the block records an error word and returns, and the host reports
 // HV_ERR_TIMEOUT.
+//
+// Tagged exchange (float corrections): instead of phase counters, every
+// mirror entry is a 64-bit word holding the float value and the number of
+// the half-sweep that wrote it.  A block reads a neighbour's row by polling
+// the words themselves until they carry the half-sweep it needs, so a row can
+// be consumed as soon as it is written, without a block-wide release and a
+// separate flag.  One mirror copy is enough: a block overwrites its entry of
+// half-sweep s with that of s + 2 only after reading the neighbour's entry of
+// s + 1 at the same position, which the neighbour computed from the entry of
+// s.  Tags restart at 1 in every solve (the mirror rows are cleared on entry);
+// the first red sweep of each cycle reads no mirror, its neighbours' black
+// corrections being zero.
 #include <cmath>
 
 #include "hv_internal.h"
@@ -35,10 +47,19 @@ namespace {
 
 constexpr int kSorThreads = 1024;
 constexpr long long kMaxSpin = 1ll << 24;  // polls before a wait gives up (~1 s)
+constexpr long long kMaxPoll = 1ll << 22;  // polls of one tagged mirror entry
+#ifndef HV_SOR_POLL_NS
+#define HV_SOR_POLL_NS 64
+#endif
+constexpr unsigned kPollSleepNs = HV_SOR_POLL_NS;  // back-off after a poll that missed
+
+using u64 = unsigned long long;
 
 template <typename T, typename S>
 struct SorArgs {
     int nx, ny, nz, nz2, P, R, bxn, byn, nblocks, src_smem, vec4;
+    int nq_shift;           // log2(nz2 / 4) when a power of two, else -1
+    u64 *tmirror;           // tagged mirror [x][colour][y][nz2]: value bits | half-sweep << 32
     S hx2i, hy2i, hz2i, inv_diag, omega;
     double dhx2i, dhy2i, dhz2i, ddiag, src_c;
     double tol;
@@ -277,6 +298,266 @@ __device__ __forceinline__ void sweep_quads<double, double>(const SorArgs<double
                                                             double *, const double *, int, int, int, int, int, int,
                                                             int, bool, double &) {}
 
+__device__ __forceinline__ u64 tag_word(float v, unsigned tag) {
+    return (u64)__float_as_uint(v) | ((u64)tag << 32);
+}
+
+// Four consecutive tagged entries (one quad), written with two 16-byte
+// relaxed stores; each 64-bit word is single-copy atomic.
+__device__ __forceinline__ void st_tagged4(u64 *p, float4 v, unsigned tag) {
+    asm volatile("st.relaxed.gpu.global.v2.b64 [%0], {%1, %2};" ::"l"(p), "l"(tag_word(v.x, tag)),
+                 "l"(tag_word(v.y, tag))
+                 : "memory");
+    asm volatile("st.relaxed.gpu.global.v2.b64 [%0], {%1, %2};" ::"l"(p + 2), "l"(tag_word(v.z, tag)),
+                 "l"(tag_word(v.w, tag))
+                 : "memory");
+}
+
+// Two ghost quads of one work item (the two neighbours along one axis),
+// polled together: both sources are loaded, then all tags are checked, and
+// only a miss repeats the loads, so a row whose ghosts are already written
+// costs one L2 round trip.  A null source is not read (its value is zero).
+// Bounded: after kMaxPoll polls, or when another block has reported an error,
+// it records the error, sets `failed` and returns what it read; a thread that
+// has failed once reads each further source once without waiting.
+__device__ __forceinline__ void poll_pair(const u64 *g0, const u64 *g1, unsigned tag, int *status, bool &failed,
+                                          float4 &v0, float4 &v1) {
+    u64 w[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    const u64 *g[2] = {g0, g1};
+    long long n = 0;
+    while (true) {
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            if (!g[i]) continue;
+            asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];"
+                         : "=l"(w[i][0]), "=l"(w[i][1])
+                         : "l"(g[i])
+                         : "memory");
+            asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];"
+                         : "=l"(w[i][2]), "=l"(w[i][3])
+                         : "l"(g[i] + 2)
+                         : "memory");
+        }
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+            if (g[i])
+                ok = ok && (unsigned)(w[i][0] >> 32) == tag && (unsigned)(w[i][1] >> 32) == tag &&
+                     (unsigned)(w[i][2] >> 32) == tag && (unsigned)(w[i][3] >> 32) == tag;
+        if (ok || failed) break;
+        if ((++n & 63) == 0 && (n > kMaxPoll || ld_volatile(status))) {
+            failed = true;
+            atomicExch(status, 1);
+            break;
+        }
+        // a waiting warp yields its issue slots to the warps that compute
+        if (kPollSleepNs) __nanosleep(kPollSleepNs);
+    }
+    v0 = make_float4(__uint_as_float((unsigned)w[0][0]), __uint_as_float((unsigned)w[0][1]),
+                     __uint_as_float((unsigned)w[0][2]), __uint_as_float((unsigned)w[0][3]));
+    v1 = make_float4(__uint_as_float((unsigned)w[1][0]), __uint_as_float((unsigned)w[1][1]),
+                     __uint_as_float((unsigned)w[1][2]), __uint_as_float((unsigned)w[1][3]));
+}
+
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+
+// Colour sweep with the tagged exchange (float corrections, nz/2 a multiple
+// of 4, source in shared memory).  Work item w is quad w % nq (four
+// consecutive same-colour nodes) of row order[w / nq] (p << 16 | j); the order lists the
+// block's face rows -- those that read or feed another block -- before its
+// inner rows, so the rows the neighbours wait for are written first and the
+// ghosts this block needs have the inner rows' time to arrive.  Rows of other
+// blocks are polled for half-sweep `tag_in` (0: they are zero, the first red
+// sweep of a cycle); Dirichlet planes and rows are zero.  Face rows are
+// written to the mirror with `tag_out`.
+template <typename T>
+__device__ __forceinline__ void sweep_quads_tagged(const SorArgs<T, float> &a, const Block &B, int c, float *sd,
+                                                   const float *ss, const unsigned *order, bool track,
+                                                   float &last_max, unsigned tag_out, unsigned tag_in, bool &failed) {
+    const int nz2 = a.nz2, nq = nz2 / 4, nx = a.nx, ny = a.ny, nz = a.nz, cp = c ^ 1;
+    const int items = B.np * B.nr * nq;
+    const long long cstride = (long long)ny * nz2;  // one colour of one plane in the mirror
+    for (int w = threadIdx.x; w < items; w += blockDim.x) {
+        const int r = a.nq_shift >= 0 ? w >> a.nq_shift : w / nq, q = w - r * nq;
+        const unsigned e = order[r];
+        const int p = (int)(e >> 16), j = (int)(e & 0xffffu);
+        const int x = B.x0 + p, y = B.y0 + j;
+        if (y < 1 || y > ny - 2) continue;
+        const int kc = (c - x - y) & 1;
+        const int roff = ((p * 2 + c) * B.nr + j) * nz2;
+        float *row = sd + roff;
+        const float *orow = sd + ((p * 2 + cp) * B.nr + j) * nz2;
+        // ghost sources: xm, xp, ym, yp rows of other blocks (null: own or zero)
+        const bool gx0 = p == 0 && x - 1 >= 1, gx1 = p + 1 == B.np && x + 1 <= nx - 2;
+        const bool gy0 = j == 0 && y - 1 >= 1, gy1 = j + 1 == B.nr && y + 1 <= ny - 2;
+        // mirror entry of quad q in row (x, y), other colour
+        const u64 *gq = a.tmirror + ((2ll * x + cp) * cstride + (long long)y * nz2 + 4 * q);
+        float4 m4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), p4 = m4;
+        if (tag_in && (gx0 || gx1))
+            poll_pair(gx0 ? gq - 2 * cstride : nullptr, gx1 ? gq + 2 * cstride : nullptr, tag_in, a.status, failed,
+                      m4, p4);
+        if (p > 0) m4 = reinterpret_cast<const float4 *>(orow - 2 * B.hp)[q];
+        if (p + 1 < B.np) p4 = reinterpret_cast<const float4 *>(orow + 2 * B.hp)[q];
+        const float4 xs = add4(m4, p4);
+        m4 = p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (tag_in && (gy0 || gy1))
+            poll_pair(gy0 ? gq - nz2 : nullptr, gy1 ? gq + nz2 : nullptr, tag_in, a.status, failed, m4, p4);
+        if (j > 0) m4 = reinterpret_cast<const float4 *>(orow - nz2)[q];
+        if (j + 1 < B.nr) p4 = reinterpret_cast<const float4 *>(orow + nz2)[q];
+        const float4 ys = add4(m4, p4);
+        const float4 self = reinterpret_cast<const float4 *>(row)[q];
+        const float4 o = reinterpret_cast<const float4 *>(orow)[q];
+        const float4 s = reinterpret_cast<const float4 *>(ss + roff)[q];
+        float z0, z1, z2, z3;  // zm + zp per lane
+        if (kc == 0) {
+            const float left = q > 0 ? orow[4 * q - 1] : 0.0f;
+            z0 = left + o.x;
+            z1 = o.x + o.y;
+            z2 = o.y + o.z;
+            z3 = o.z + o.w;
+        } else {
+            const float right = q + 1 < nq ? orow[4 * q + 4] : 0.0f;
+            z0 = o.x + o.y;
+            z1 = o.y + o.z;
+            z2 = o.z + o.w;
+            z3 = o.w + right;
+        }
+        const int kb = kc + 8 * q;
+        float4 nv;
+        nv.x = sor_update<float, T>(a, self.x, xs.x, ys.x, z0, s.x, kb >= 1 && kb <= nz - 2);
+        nv.y = sor_update<float, T>(a, self.y, xs.y, ys.y, z1, s.y, kb + 2 <= nz - 2);
+        nv.z = sor_update<float, T>(a, self.z, xs.z, ys.z, z2, s.z, kb + 4 <= nz - 2);
+        nv.w = sor_update<float, T>(a, self.w, xs.w, ys.w, z3, s.w, kb + 6 <= nz - 2);
+        reinterpret_cast<float4 *>(row)[q] = nv;
+        if (gx0 || gx1 || gy0 || gy1) st_tagged4(const_cast<u64 *>(gq) + (c - cp) * cstride, nv, tag_out);
+        if (track)
+            last_max = fmax(last_max, fmax(fmax(fabs(nv.x - self.x), fabs(nv.y - self.y)),
+                                           fmax(fabs(nv.z - self.z), fabs(nv.w - self.w))));
+    }
+}
+
+// One work item of a tagged sweep (a quad of one row), decoded once per solve.
+struct Item {
+    int roff;        // shared-memory offset of the quad in colour 0 of its row
+    unsigned flags;  // kItem* bits below
+    const u64 *gq;   // tagged mirror entry of the quad in colour 0 of its row
+};
+enum : unsigned {
+    kItemActive = 1u,   // an interior row of this block
+    kOwnXm = 2u,        // neighbour rows held in this block's shared memory
+    kOwnXp = 4u,
+    kOwnYm = 8u,
+    kOwnYp = 16u,
+    kGhostXm = 32u,     // neighbour rows of another block (tagged mirror)
+    kGhostXp = 64u,
+    kGhostYm = 128u,
+    kGhostYp = 256u,
+    kKc0 = 512u,        // parity of the first node of colour 0 in the row
+    kFirstQuad = 1024u,
+    kLastQuad = 2048u,
+};
+constexpr int kLaneShift = 12;  // bits 12..15: lanes inside the z range for kc = 0; 16..19 for kc = 1
+constexpr unsigned kGhostAny = kGhostXm | kGhostXp | kGhostYm | kGhostYp;
+
+template <typename T>
+__device__ Item make_item(const SorArgs<T, float> &a, const Block &B, const unsigned *order, int w) {
+    Item it{0, 0u, a.tmirror};
+    const int nq = a.nz2 / 4;
+    if (w >= B.np * B.nr * nq) return it;
+    const int r = w / nq, q = w - r * nq;
+    const unsigned e = order[r];
+    const int p = (int)(e >> 16), j = (int)(e & 0xffffu), x = B.x0 + p, y = B.y0 + j;
+    if (y < 1 || y > a.ny - 2) return it;
+    unsigned f = kItemActive;
+    if (p > 0) f |= kOwnXm;
+    if (p + 1 < B.np) f |= kOwnXp;
+    if (j > 0) f |= kOwnYm;
+    if (j + 1 < B.nr) f |= kOwnYp;
+    if (p == 0 && x - 1 >= 1) f |= kGhostXm;
+    if (p + 1 == B.np && x + 1 <= a.nx - 2) f |= kGhostXp;
+    if (j == 0 && y - 1 >= 1) f |= kGhostYm;
+    if (j + 1 == B.nr && y + 1 <= a.ny - 2) f |= kGhostYp;
+    if ((-x - y) & 1) f |= kKc0;
+    if (q == 0) f |= kFirstQuad;
+    if (q + 1 == nq) f |= kLastQuad;
+    for (int kc = 0; kc < 2; kc++)
+        for (int i = 0; i < 4; i++) {
+            const int k = kc + 8 * q + 2 * i;
+            if (k >= 1 && k <= a.nz - 2) f |= 1u << (kLaneShift + 4 * kc + i);
+        }
+    it.flags = f;
+    it.roff = (p * 2 * B.nr + j) * a.nz2 + 4 * q;
+    it.gq = a.tmirror + ((2ll * x) * a.ny * a.nz2 + (long long)y * a.nz2 + 4 * q);
+    return it;
+}
+
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+// Colour sweep of one decoded work item with the tagged exchange; the same
+// update and neighbour sums as sweep_quads_tagged.
+template <typename T>
+__device__ __forceinline__ void sweep_item(const SorArgs<T, float> &a, const Item &it, int c, int hp,
+                                           long long cstride, float *sd, const float *ss, unsigned tag_in,
+                                           unsigned tag_out, bool track, float &last_max, bool &failed) {
+    const unsigned f = it.flags;
+    if (!(f & kItemActive)) return;
+    const int cp = c ^ 1, kc = ((f & kKc0) ? 1 : 0) ^ c, nz2 = a.nz2;
+    float *rowq = sd + it.roff + c * hp;
+    const float *orq = sd + it.roff + cp * hp;
+    const u64 *g = it.gq + cp * cstride;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 m4 = zero4, p4 = zero4;
+    if (tag_in && (f & (kGhostXm | kGhostXp)))
+        poll_pair((f & kGhostXm) ? g - 2 * cstride : nullptr, (f & kGhostXp) ? g + 2 * cstride : nullptr, tag_in,
+                  a.status, failed, m4, p4);
+    if (f & kOwnXm) m4 = lds4(orq - 2 * hp);
+    if (f & kOwnXp) p4 = lds4(orq + 2 * hp);
+    const float4 xs = add4(m4, p4);
+    m4 = p4 = zero4;
+    if (tag_in && (f & (kGhostYm | kGhostYp)))
+        poll_pair((f & kGhostYm) ? g - nz2 : nullptr, (f & kGhostYp) ? g + nz2 : nullptr, tag_in, a.status, failed,
+                  m4, p4);
+    if (f & kOwnYm) m4 = lds4(orq - nz2);
+    if (f & kOwnYp) p4 = lds4(orq + nz2);
+    const float4 ys = add4(m4, p4);
+    const float4 self = lds4(rowq), o = lds4(orq), s = lds4(ss + it.roff + c * hp);
+    float z0, z1, z2, z3;  // zm + zp per lane
+    if (kc == 0) {
+        const float left = (f & kFirstQuad) ? 0.0f : orq[-1];
+        z0 = left + o.x;
+        z1 = o.x + o.y;
+        z2 = o.y + o.z;
+        z3 = o.z + o.w;
+    } else {
+        const float right = (f & kLastQuad) ? 0.0f : orq[4];
+        z0 = o.x + o.y;
+        z1 = o.y + o.z;
+        z2 = o.z + o.w;
+        z3 = o.w + right;
+    }
+    const unsigned lanes = f >> (kLaneShift + 4 * kc);
+    float4 nv;
+    nv.x = sor_update<float, T>(a, self.x, xs.x, ys.x, z0, s.x, lanes & 1u);
+    nv.y = sor_update<float, T>(a, self.y, xs.y, ys.y, z1, s.y, lanes & 2u);
+    nv.z = sor_update<float, T>(a, self.z, xs.z, ys.z, z2, s.z, lanes & 4u);
+    nv.w = sor_update<float, T>(a, self.w, xs.w, ys.w, z3, s.w, lanes & 8u);
+    *reinterpret_cast<float4 *>(rowq) = nv;
+    if (f & kGhostAny) st_tagged4(const_cast<u64 *>(it.gq) + c * cstride, nv, tag_out);
+    if (track)
+        last_max = fmax(last_max, fmax(fmax(fabs(nv.x - self.x), fabs(nv.y - self.y)),
+                                       fmax(fabs(nv.z - self.z), fabs(nv.w - self.w))));
+}
+
+// Correction of a neighbouring block's node from its mirror entry (either
+// layout); called after a grid barrier, when every entry is final.
+template <bool kTag, typename T, typename S>
+__device__ __forceinline__ double mirror_value(const SorArgs<T, S> &a, long long idx) {
+    if constexpr (kTag) return (double)__uint_as_float((unsigned)__ldcg(a.tmirror + idx));
+    else return (double)__ldcg(a.delta + idx);
+}
+
 // Colour sweep, one node per thread per row (any size and type).
 template <typename S, typename T>
 __device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block &B, int c, S *sd, const S *ss,
@@ -315,7 +596,9 @@ __device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block
     }
 }
 
-template <typename T, typename S>
+// kTag: tagged exchange (float corrections in quads); kItems: 1 or 2 work
+// items per thread decoded once per solve, 0 decoded in every sweep.
+template <typename T, typename S, bool kTag, int kItems>
 __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double s_tot[3];
@@ -336,6 +619,8 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     // shared memory: delta | src (when it fits)
     S *sd = reinterpret_cast<S *>(smem_raw);
     S *ss = a.src_smem ? sd + own : nullptr;
+    // tagged sweeps: the block's rows, face rows first
+    unsigned *order = reinterpret_cast<unsigned *>(sd + (size_t)own * (a.src_smem ? 2 : 1));
     auto SD = [&](int p, int c, int j, int t) -> S & { return sd[((p * 2 + c) * nr + j) * nz2 + t]; };
     unsigned my_phase = 0;
     // colour sweeps: thread -> half-line position t_own, rows r_start, +rows_step
@@ -355,11 +640,33 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     const int k_own = rz_start < zrows_step ? tid % nz : nz;
     const int jz_start = rz_start % nr, pz_start = rz_start / nr, djz = zrows_step % nr, dpz = zrows_step / nr;
 
+    if constexpr (kTag) {
+        if (tid == 0) {
+            int n = 0;
+            for (int pass = 0; pass < 2; pass++)
+                for (int l = 0; l < np * nr; l++) {
+                    const int p = l / nr, j = l - p * nr, x = x0 + p, y = y0 + j;
+                    const bool face = (p == 0 && x - 1 >= 1) || (p + 1 == np && x + 1 <= a.nx - 2) ||
+                                      (j == 0 && y - 1 >= 1) || (j + 1 == nr && y + 1 <= ny - 2);
+                    if (face == (pass == 0)) order[n++] = (unsigned)p << 16 | (unsigned)j;
+                }
+        }
+    }
+    [[maybe_unused]] Item items[kItems > 0 ? kItems : 1];
+    if constexpr (kTag && kItems > 0) {
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kItems; k++) items[k] = make_item<T>(a, B, order, tid + k * nth);
+    }
+
     // ---- entry: zero delta (shared and own global mirror) -----------------
     for (int e = tid; e < own; e += nth) sd[e] = S(0);
     for (int p = 0; p < np; p++)
         for (int c = 0; c < 2; c++)
-            for (int e = tid; e < hp; e += nth) a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
+            for (int e = tid; e < hp; e += nth) {
+                if constexpr (kTag) a.tmirror[B.mirror(x0 + p, c, y0) + e] = 0ull;
+                else a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
+            }
     const int step = a.ctl[0];
     const bool extrap = a.extrapolate && a.ctl[2];
     if (a.extrapolate) {
@@ -404,12 +711,12 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
             // (zero on the Dirichlet planes and rows)
             double dc = (double)SD(p, c0, j, kh);
             double dzm = (double)SD(p, c1, j, (k - 1) >> 1), dzp = (double)SD(p, c1, j, (k + 1) >> 1);
-            double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh) : (double)__ldcg(a.delta + B.mirror(x - 1, c1, y) + kh);
+            double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh) : mirror_value<kTag>(a, B.mirror(x - 1, c1, y) + kh);
             double dxp =
-                p + 1 < np ? (double)SD(p + 1, c1, j, kh) : (double)__ldcg(a.delta + B.mirror(x + 1, c1, y) + kh);
-            double dym = j > 0 ? (double)SD(p, c1, j - 1, kh) : (double)__ldcg(a.delta + B.mirror(x, c1, y - 1) + kh);
+                p + 1 < np ? (double)SD(p + 1, c1, j, kh) : mirror_value<kTag>(a, B.mirror(x + 1, c1, y) + kh);
+            double dym = j > 0 ? (double)SD(p, c1, j - 1, kh) : mirror_value<kTag>(a, B.mirror(x, c1, y - 1) + kh);
             double dyp =
-                j + 1 < nr ? (double)SD(p, c1, j + 1, kh) : (double)__ldcg(a.delta + B.mirror(x, c1, y + 1) + kh);
+                j + 1 < nr ? (double)SD(p, c1, j + 1, kh) : mirror_value<kTag>(a, B.mirror(x, c1, y + 1) + kh);
             double pc = __ldcg(a.phi64 + id) + dc;
             double pxm = __ldcg(a.phi64 + id - sxy) + dxm;
             double pxp = __ldcg(a.phi64 + id + sxy) + dxp;
@@ -469,9 +776,10 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         }
         __syncthreads();
         for (int e = tid; e < own; e += nth) sd[e] = S(0);
-        for (int p = 0; p < np; p++)
-            for (int c = 0; c < 2; c++)
-                for (int e = tid; e < hp; e += nth) a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
+        if constexpr (!kTag)
+            for (int p = 0; p < np; p++)
+                for (int c = 0; c < 2; c++)
+                    for (int e = tid; e < hp; e += nth) a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
 
         if (a.criterion == HV_SOR_REL_RESIDUAL) converged = rel <= a.tol;
         else converged = its > 0 && maxd < a.tol;
@@ -492,10 +800,35 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
         __syncthreads();
         m_prev = m = s_m;
         rel_prev = rel;
-        publish(a.phase + b, ++my_phase);
-
-        // ---- m red+black iterations on delta ------------------------------
         last_max = S(0);
+
+        // ---- m red+black iterations on delta, tagged exchange -------------
+        if constexpr (kTag) {
+            bool failed = false;
+            for (int it = 0; it < m; it++) {
+                const unsigned t = (unsigned)(its + it);
+                for (int c = 0; c < 2; c++) {
+                    // red(t) is half-sweep 2t+1, black(t) 2t+2; red reads black(t-1)
+                    const unsigned tag_in = c == 0 ? (it == 0 ? 0u : 2u * t) : 2u * t + 1u;
+                    const unsigned tag_out = 2u * t + 1u + (unsigned)c;
+                    if constexpr (kItems > 0) {
+#pragma unroll
+                        for (int k = 0; k < kItems; k++)
+                            sweep_item<T>(a, items[k], c, hp, (long long)ny * nz2, sd, ss, tag_in, tag_out,
+                                          it == m - 1, last_max, failed);
+                    } else {
+                        sweep_quads_tagged<T>(a, B, c, sd, ss, order, it == m - 1, last_max, tag_out, tag_in,
+                                              failed);
+                    }
+                    if (__syncthreads_or(failed)) return;
+                }
+            }
+            its += m;
+            continue;
+        }
+
+        // ---- m red+black iterations on delta, phase counters --------------
+        publish(a.phase + b, ++my_phase);
         for (int it = 0; it < m; it++) {
             for (int c = 0; c < 2; c++) {
                 if (!wait_neighbours(a, bx, by, my_phase)) return;
@@ -536,8 +869,40 @@ static hv_status plan_for(hv_ctx *c) {
     const int nz2 = (g.nz + 1) / 2;
     const int interior = g.nx - 2;
     f.ok = false;
-    // smallest blocks first (most parallel), the source in shared memory when
-    // it fits, a y split only when a plane does not fit
+    if (sizeof(S) == 4 && nz2 % 4 == 0) {
+        // float corrections in quads: blocks of P planes x R rows with the
+        // source in shared memory, chosen for the fewest quads per thread, then
+        // the smallest total face (blocks x (P + R): the rows exchanged per
+        // sweep), then the fewest blocks
+        const long long nq = nz2 / 4;
+        long long best[3] = {0, 0, 0};
+        for (int P = 1; P <= interior; P++)
+            for (int R = 1; R <= g.ny; R++) {
+                const size_t own = (size_t)P * 2 * R * nz2;
+                const size_t smem = sizeof(S) * own * 2 + ((size_t)P * R * 4 + 15) / 16 * 16;
+                if (smem > limit) break;
+                const long long bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
+                if (bxn * byn > prop.multiProcessorCount) continue;
+                const long long key[3] = {((long long)P * R * nq + kSorThreads - 1) / kSorThreads,
+                                          bxn * byn * (P + R), bxn * byn};
+                if (f.ok && !(key[0] < best[0] || (key[0] == best[0] && (key[1] < best[1] ||
+                                                   (key[1] == best[1] && key[2] < best[2])))))
+                    continue;
+                best[0] = key[0];
+                best[1] = key[1];
+                best[2] = key[2];
+                f.P = P;
+                f.R = R;
+                f.bx = (int)bxn;
+                f.by = (int)byn;
+                f.nblocks = (int)(bxn * byn);
+                f.smem = smem;
+                f.src_smem = true;
+                f.ok = true;
+            }
+    }
+    // otherwise smallest blocks first (most parallel), the source in shared
+    // memory when it fits, a y split only when a plane does not fit
     for (int pass = 0; pass < 2 && !f.ok; pass++) {
         const bool with_src = pass == 0;
         for (int R = g.ny; R >= 1 && !f.ok; R = (R == 1) ? 0 : (R + 1) / 2) {
@@ -562,19 +927,28 @@ static hv_status plan_for(hv_ctx *c) {
     if (!f.ok) return HV_OK;  // the fused path reports HV_ERR_UNSUPPORTED
     f.nz2 = nz2;
     f.threads = kSorThreads;
-    auto kern = c->prec == HV_F64 ? (const void *)k_sor_fast<double, double> : (const void *)k_sor_fast<float, float>;
-    HV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
-    int per_sm = 0;
-    HV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, f.threads, f.smem));
-    if (per_sm < 1 || (long long)per_sm * prop.multiProcessorCount < f.nblocks) {
-        f.ok = false;
-        return HV_OK;
+    const void *kerns[4] = {(const void *)k_sor_fast<S, S, false, 0>, nullptr, nullptr, nullptr};
+    if constexpr (sizeof(S) == 4) {
+        kerns[1] = (const void *)k_sor_fast<S, S, true, 0>;
+        kerns[2] = (const void *)k_sor_fast<S, S, true, 1>;
+        kerns[3] = (const void *)k_sor_fast<S, S, true, 2>;
     }
-    // mirrors cover every plane and row, so the Dirichlet ones stay zero
+    for (const void *kern : kerns) {
+        if (!kern) continue;
+        HV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
+        int per_sm = 0;
+        HV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, f.threads, f.smem));
+        if (per_sm < 1 || (long long)per_sm * prop.multiProcessorCount < f.nblocks) {
+            f.ok = false;
+            return HV_OK;
+        }
+    }
+    // mirrors cover every plane and row, so the Dirichlet ones stay zero; 8
+    // bytes per entry, which also holds the tagged words of a float solve
     const size_t n = (size_t)g.nx * 2 * g.ny * nz2;
-    HV_CUDA(cudaMalloc(&f.delta, n * sizeof(S)));
+    HV_CUDA(cudaMalloc(&f.delta, n * 8));
     HV_CUDA(cudaMalloc(&f.src, n * sizeof(S)));
-    HV_CUDA(cudaMemsetAsync(f.delta, 0, n * sizeof(S), c->stream));
+    HV_CUDA(cudaMemsetAsync(f.delta, 0, n * 8, c->stream));
     HV_CUDA(cudaMemsetAsync(f.src, 0, n * sizeof(S), c->stream));
     HV_CUDA(cudaMalloc((void **)&f.partials, sizeof(double) * 4 * f.nblocks));
     HV_CUDA(cudaMemsetAsync(f.partials, 0, sizeof(double) * 4 * f.nblocks, c->stream));
@@ -618,6 +992,9 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.nblocks = f.nblocks;
     a.src_smem = f.src_smem ? 1 : 0;
     a.vec4 = (sizeof(S) == 4 && f.nz2 % 4 == 0 && f.src_smem) ? 1 : 0;
+    a.nq_shift = -1;
+    for (int sh = 0; sh < 30; sh++)
+        if ((f.nz2 / 4) == (1 << sh)) a.nq_shift = sh;
     const double dx = 2.0 * g.dmx / g.nx, dy = 2.0 * g.dmy / g.ny, dz = 2.0 * g.dmz / g.nz;
     a.dhx2i = 1.0 / (dx * dx);
     a.dhy2i = 1.0 / (dy * dy);
@@ -639,6 +1016,7 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.phi64 = c->fused.phi64;
     a.phi64_prev = c->fused.phi64_prev;
     a.delta = reinterpret_cast<S *>(f.delta);
+    a.tmirror = reinterpret_cast<u64 *>(f.delta);
     a.src = reinterpret_cast<S *>(f.src);
     a.partials = f.partials;
     a.phase = f.phase;
@@ -649,8 +1027,15 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.its_ring = its_ring;
     a.ring = ring;
     void *args[] = {&a};
-    HV_CUDA(cudaLaunchCooperativeKernel((const void *)k_sor_fast<T, S>, dim3(f.nblocks), dim3(f.threads), args,
-                                        f.smem, c->stream));
+    const void *kern = (const void *)k_sor_fast<T, S, false, 0>;
+    if constexpr (sizeof(S) == 4)
+        if (a.vec4 && c->fast.sor_exchange == HV_SOR_EXCHANGE_AUTO) {
+            const long long per_thread = ((long long)f.P * f.R * (f.nz2 / 4) + f.threads - 1) / f.threads;
+            kern = per_thread == 1   ? (const void *)k_sor_fast<T, S, true, 1>
+                   : per_thread == 2 ? (const void *)k_sor_fast<T, S, true, 2>
+                                     : (const void *)k_sor_fast<T, S, true, 0>;
+        }
+    HV_CUDA(cudaLaunchCooperativeKernel(kern, dim3(f.nblocks), dim3(f.threads), args, f.smem, c->stream));
     return HV_OK;
 }
 

@@ -65,11 +65,13 @@ class hv_run_params(C.Structure):
 
 class hv_fast_options(C.Structure):
     _fields_ = [("sor_warm_start", C.c_int), ("sor_inner_min", C.c_int), ("sor_inner_max", C.c_int),
-                ("sort_every", C.c_int), ("graph_steps", C.c_int)]
+                ("sort_every", C.c_int), ("graph_steps", C.c_int), ("sor_exchange", C.c_int)]
 
 
 HV_WARM_PREVIOUS = 0
 HV_WARM_EXTRAPOLATE = 1
+HV_SOR_EXCHANGE_AUTO = 0
+HV_SOR_EXCHANGE_FLAGS = 1
 
 
 class hv_observables(C.Structure):

@@ -293,6 +293,13 @@ typedef enum hv_warm_start {
                                 reference's by less than the tolerance          */
 } hv_warm_start;
 
+/* How the blocks of the fused SOR exchange boundary corrections. */
+typedef enum hv_sor_exchange {
+    HV_SOR_EXCHANGE_AUTO = 0,   /* tagged mirror words where supported (float,
+                                   z extent a multiple of 8), else counters    */
+    HV_SOR_EXCHANGE_FLAGS = 1   /* per-block phase counters after each sweep   */
+} hv_sor_exchange;
+
 /* Controls of HV_PATH_FUSED that have no counterpart in the reference. */
 typedef struct hv_fast_options {
     int sor_warm_start;   /* hv_warm_start                                      */
@@ -300,9 +307,11 @@ typedef struct hv_fast_options {
     int sor_inner_max;    /*   checks: adaptive, clamped to [min, max]          */
     int sort_every;       /* re-sort particle slots by cell every n steps (0 = off) */
     int graph_steps;      /* steps captured per CUDA graph launch (0 = no graph) */
+    int sor_exchange;     /* hv_sor_exchange                                    */
 } hv_fast_options;
 
-/* Defaults: HV_WARM_PREVIOUS, inner 2..64, sort every 16 steps, 8-step graphs. */
+/* Defaults: HV_WARM_PREVIOUS, inner 2..64, sort every 16 steps, 8-step graphs,
+ * HV_SOR_EXCHANGE_AUTO. */
 HV_API void hv_fast_options_default(hv_fast_options *o);
 HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);
 HV_API hv_status hv_ctx_get_fast_options(const hv_ctx *ctx, hv_fast_options *o);
