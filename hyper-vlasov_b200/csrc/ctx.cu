@@ -670,7 +670,7 @@ void hv_fast_options_default(hv_fast_options *o) {
     if (!o) return;
     o->sor_warm_start = HV_WARM_PREVIOUS;
     o->sor_inner_min = 2;
-    o->sor_inner_max = 64;
+    o->sor_inner_max = 256;
     o->sort_every = 16;
     o->graph_steps = 8;
     o->sor_exchange = HV_SOR_EXCHANGE_AUTO;

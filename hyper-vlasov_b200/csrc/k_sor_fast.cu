@@ -38,6 +38,7 @@
 // s.  Tags restart at 1 in every solve (the mirror rows are cleared on entry);
 // the first red sweep of each cycle reads no mirror, its neighbours' black
 // corrections being zero.
+#include <algorithm>
 #include <cmath>
 
 #include "hv_internal.h"
@@ -438,116 +439,206 @@ __device__ __forceinline__ void sweep_quads_tagged(const SorArgs<T, float> &a, c
     }
 }
 
-// One work item of a tagged sweep (a quad of one row), decoded once per solve.
-struct Item {
-    int roff;        // shared-memory offset of the quad in colour 0 of its row
-    unsigned flags;  // kItem* bits below
-    const u64 *gq;   // tagged mirror entry of the quad in colour 0 of its row
-};
-enum : unsigned {
-    kItemActive = 1u,   // an interior row of this block
-    kOwnXm = 2u,        // neighbour rows held in this block's shared memory
-    kOwnXp = 4u,
-    kOwnYm = 8u,
-    kOwnYp = 16u,
-    kGhostXm = 32u,     // neighbour rows of another block (tagged mirror)
-    kGhostXp = 64u,
-    kGhostYm = 128u,
-    kGhostYp = 256u,
-    kKc0 = 512u,        // parity of the first node of colour 0 in the row
-    kFirstQuad = 1024u,
-    kLastQuad = 2048u,
-};
-constexpr int kLaneShift = 12;  // bits 12..15: lanes inside the z range for kc = 0; 16..19 for kc = 1
-constexpr unsigned kGhostAny = kGhostXm | kGhostXp | kGhostYm | kGhostYp;
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
-template <typename T>
-__device__ Item make_item(const SorArgs<T, float> &a, const Block &B, const unsigned *order, int w) {
-    Item it{0, 0u, a.tmirror};
-    const int nq = a.nz2 / 4;
-    if (w >= B.np * B.nr * nq) return it;
-    const int r = w / nq, q = w - r * nq;
-    const unsigned e = order[r];
-    const int p = (int)(e >> 16), j = (int)(e & 0xffffu), x = B.x0 + p, y = B.y0 + j;
-    if (y < 1 || y > a.ny - 2) return it;
-    unsigned f = kItemActive;
-    if (p > 0) f |= kOwnXm;
-    if (p + 1 < B.np) f |= kOwnXp;
-    if (j > 0) f |= kOwnYm;
-    if (j + 1 < B.nr) f |= kOwnYp;
-    if (p == 0 && x - 1 >= 1) f |= kGhostXm;
-    if (p + 1 == B.np && x + 1 <= a.nx - 2) f |= kGhostXp;
-    if (j == 0 && y - 1 >= 1) f |= kGhostYm;
-    if (j + 1 == B.nr && y + 1 <= a.ny - 2) f |= kGhostYp;
-    if ((-x - y) & 1) f |= kKc0;
-    if (q == 0) f |= kFirstQuad;
-    if (q + 1 == nq) f |= kLastQuad;
+// ---- staged tagged sweep -------------------------------------------------
+// A sweep first updates the block's perimeter rows, from shared memory and a
+// shared-memory buffer of ghost rows (the neighbouring blocks' rows across the
+// block's faces), writing those that a neighbouring block reads to the
+// mirror.  After a block barrier, threads [0, kGhostThreads) poll the
+// neighbours' perimeter rows just written for this sweep into the ghost
+// buffer, for the next sweep, while the other threads update the inner rows
+// (off the block's perimeter), which read only this block's shared memory.
+// The fetch's L2 round trip is thus spent under the inner rows' updates.
+constexpr int kGhostThreads = 256;
+
+// Shared-memory tables behind delta | src, sized by the plan's P x R block.
+struct Staged {
+    unsigned *order;  // [P R] rows, face rows first (generic tagged sweep)
+    unsigned *ftab;   // [P R] perimeter rows: p << 16 | j
+    unsigned *fgi;    // [P R][2] ghost-buffer rows: xm | xp << 16, ym | yp << 16 (0xffff: none)
+    unsigned *gsrc;   // [2 (P + R)] mirror index of each ghost row (colour 0)
+    float *gbuf;      // [2 (P + R)][nz2] ghost values of the current sweep
+    __host__ __device__ static size_t bytes(int P, int R, int nz2) {
+        const size_t pr = (size_t)P * R, g = 2 * ((size_t)P + R);
+        return 16 * ((pr * 4 + 15) / 16 + (pr * 4 + 15) / 16 + (pr * 8 + 15) / 16 + (g * 4 + 15) / 16) +
+               g * nz2 * 4;
+    }
+    __device__ Staged(void *base, int P, int R) {
+        const size_t pr = (size_t)P * R, g = 2 * ((size_t)P + R);
+        unsigned char *p = reinterpret_cast<unsigned char *>(base);
+        order = reinterpret_cast<unsigned *>(p);
+        p += 16 * ((pr * 4 + 15) / 16);
+        ftab = reinterpret_cast<unsigned *>(p);
+        p += 16 * ((pr * 4 + 15) / 16);
+        fgi = reinterpret_cast<unsigned *>(p);
+        p += 16 * ((pr * 8 + 15) / 16);
+        gsrc = reinterpret_cast<unsigned *>(p);
+        p += 16 * ((g * 4 + 15) / 16);
+        gbuf = reinterpret_cast<float *>(p);
+    }
+};
+
+enum : unsigned {
+    kQActive = 1u,     // an interior row of the grid
+    kQOwnXm = 2u,      // neighbour rows in this block's shared memory
+    kQOwnXp = 4u,
+    kQOwnYm = 8u,
+    kQOwnYp = 16u,
+    kQGhXm = 32u,      // neighbour rows of another block (ghost buffer)
+    kQGhXp = 64u,
+    kQGhYm = 128u,
+    kQGhYp = 256u,
+    kQKc0 = 512u,      // parity of the row's first colour-0 node
+    kQFirst = 1024u,   // first / last quad of the row
+    kQLast = 2048u,
+};
+constexpr int kQLanes = 12;  // bits 12..15: lanes inside the z range for kc = 0; 16..19 for kc = 1
+constexpr int kQShift = 24;  // bits 24..31: the quad index q
+constexpr unsigned kQGhAny = kQGhXm | kQGhXp | kQGhYm | kQGhYp;
+
+struct Quad {        // a quad of an inner row
+    int roff;        // shared-memory offset of the quad in colour 0 of its row
+    unsigned flags;
+};
+struct FaceQuad {    // a quad of a perimeter row
+    int roff;
+    unsigned flags;
+    unsigned gq;     // mirror index of the quad in colour 0 of its row
+    unsigned gx, gy; // ghost-buffer rows xm | xp << 16, ym | yp << 16
+};
+struct GhostQuad {   // a quad of a ghost row
+    unsigned src;    // mirror index (colour 0)
+    int dst;         // ghost-buffer offset; < 0: none
+};
+
+// Flags shared by inner and perimeter quads: parity, z-range lanes, row ends.
+__device__ __forceinline__ unsigned quad_flags(int x, int y, int q, int nq, int nz) {
+    unsigned f = kQActive | (unsigned)q << kQShift;
+    if ((-x - y) & 1) f |= kQKc0;
+    if (q == 0) f |= kQFirst;
+    if (q + 1 == nq) f |= kQLast;
     for (int kc = 0; kc < 2; kc++)
         for (int i = 0; i < 4; i++) {
             const int k = kc + 8 * q + 2 * i;
-            if (k >= 1 && k <= a.nz - 2) f |= 1u << (kLaneShift + 4 * kc + i);
+            if (k >= 1 && k <= nz - 2) f |= 1u << (kQLanes + 4 * kc + i);
         }
-    it.flags = f;
-    it.roff = (p * 2 * B.nr + j) * a.nz2 + 4 * q;
-    it.gq = a.tmirror + ((2ll * x) * a.ny * a.nz2 + (long long)y * a.nz2 + 4 * q);
-    return it;
+    return f;
 }
 
-__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
-
-// Colour sweep of one decoded work item with the tagged exchange; the same
-// update and neighbour sums as sweep_quads_tagged.
+// The SOR update of a quad from its neighbour sums (lanes outside the z range
+// keep their value), written to shared memory; returns the new quad.
 template <typename T>
-__device__ __forceinline__ void sweep_item(const SorArgs<T, float> &a, const Item &it, int c, int hp,
-                                           long long cstride, float *sd, const float *ss, unsigned tag_in,
-                                           unsigned tag_out, bool track, float &last_max, bool &failed) {
-    const unsigned f = it.flags;
-    if (!(f & kItemActive)) return;
-    const int cp = c ^ 1, kc = ((f & kKc0) ? 1 : 0) ^ c, nz2 = a.nz2;
-    float *rowq = sd + it.roff + c * hp;
-    const float *orq = sd + it.roff + cp * hp;
-    const u64 *g = it.gq + cp * cstride;
-    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 m4 = zero4, p4 = zero4;
-    if (tag_in && (f & (kGhostXm | kGhostXp)))
-        poll_pair((f & kGhostXm) ? g - 2 * cstride : nullptr, (f & kGhostXp) ? g + 2 * cstride : nullptr, tag_in,
-                  a.status, failed, m4, p4);
-    if (f & kOwnXm) m4 = lds4(orq - 2 * hp);
-    if (f & kOwnXp) p4 = lds4(orq + 2 * hp);
-    const float4 xs = add4(m4, p4);
-    m4 = p4 = zero4;
-    if (tag_in && (f & (kGhostYm | kGhostYp)))
-        poll_pair((f & kGhostYm) ? g - nz2 : nullptr, (f & kGhostYp) ? g + nz2 : nullptr, tag_in, a.status, failed,
-                  m4, p4);
-    if (f & kOwnYm) m4 = lds4(orq - nz2);
-    if (f & kOwnYp) p4 = lds4(orq + nz2);
-    const float4 ys = add4(m4, p4);
-    const float4 self = lds4(rowq), o = lds4(orq), s = lds4(ss + it.roff + c * hp);
+__device__ __forceinline__ float4 update_quad(const SorArgs<T, float> &a, unsigned f, int c, float *rowq,
+                                              const float *orq, const float *srq, float4 xs, float4 ys, bool track,
+                                              float &last_max) {
+    const int kc = ((f & kQKc0) ? 1 : 0) ^ c;
+    const float4 self = lds4(rowq), o = lds4(orq), s = lds4(srq);
     float z0, z1, z2, z3;  // zm + zp per lane
     if (kc == 0) {
-        const float left = (f & kFirstQuad) ? 0.0f : orq[-1];
+        const float left = (f & kQFirst) ? 0.0f : orq[-1];
         z0 = left + o.x;
         z1 = o.x + o.y;
         z2 = o.y + o.z;
         z3 = o.z + o.w;
     } else {
-        const float right = (f & kLastQuad) ? 0.0f : orq[4];
+        const float right = (f & kQLast) ? 0.0f : orq[4];
         z0 = o.x + o.y;
         z1 = o.y + o.z;
         z2 = o.z + o.w;
         z3 = o.w + right;
     }
-    const unsigned lanes = f >> (kLaneShift + 4 * kc);
+    const unsigned lanes = f >> (kQLanes + 4 * kc);
     float4 nv;
     nv.x = sor_update<float, T>(a, self.x, xs.x, ys.x, z0, s.x, lanes & 1u);
     nv.y = sor_update<float, T>(a, self.y, xs.y, ys.y, z1, s.y, lanes & 2u);
     nv.z = sor_update<float, T>(a, self.z, xs.z, ys.z, z2, s.z, lanes & 4u);
     nv.w = sor_update<float, T>(a, self.w, xs.w, ys.w, z3, s.w, lanes & 8u);
     *reinterpret_cast<float4 *>(rowq) = nv;
-    if (f & kGhostAny) st_tagged4(const_cast<u64 *>(it.gq) + c * cstride, nv, tag_out);
     if (track)
         last_max = fmax(last_max, fmax(fmax(fabs(nv.x - self.x), fabs(nv.y - self.y)),
                                        fmax(fabs(nv.z - self.z), fabs(nv.w - self.w))));
+    return nv;
+}
+
+template <typename T>
+__device__ __forceinline__ void sweep_inner(const SorArgs<T, float> &a, const Quad &it, int c, int hp, float *sd,
+                                            const float *ss, bool track, float &last_max) {
+    if (!(it.flags & kQActive)) return;
+    const int nz2 = a.nz2;
+    float *rowq = sd + it.roff + c * hp;
+    const float *orq = sd + it.roff + (c ^ 1) * hp;
+    const float4 xs = add4(lds4(orq - 2 * hp), lds4(orq + 2 * hp));
+    const float4 ys = add4(lds4(orq - nz2), lds4(orq + nz2));
+    update_quad<T>(a, it.flags, c, rowq, orq, ss + it.roff + c * hp, xs, ys, track, last_max);
+}
+
+template <typename T>
+__device__ __forceinline__ void sweep_face(const SorArgs<T, float> &a, const FaceQuad &it, int c, int hp,
+                                           long long cstride, float *sd, const float *ss, const float *gbuf,
+                                           unsigned tag_out, bool track, float &last_max) {
+    const unsigned f = it.flags;
+    if (!(f & kQActive)) return;
+    const int nz2 = a.nz2, q4 = 4 * (int)(f >> kQShift);
+    float *rowq = sd + it.roff + c * hp;
+    const float *orq = sd + it.roff + (c ^ 1) * hp;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 xm = (f & kQOwnXm) ? lds4(orq - 2 * hp) : (f & kQGhXm) ? lds4(gbuf + (it.gx & 0xffffu) * nz2 + q4) : zero4;
+    const float4 xp = (f & kQOwnXp) ? lds4(orq + 2 * hp) : (f & kQGhXp) ? lds4(gbuf + (it.gx >> 16) * nz2 + q4) : zero4;
+    const float4 ym = (f & kQOwnYm) ? lds4(orq - nz2) : (f & kQGhYm) ? lds4(gbuf + (it.gy & 0xffffu) * nz2 + q4) : zero4;
+    const float4 yp = (f & kQOwnYp) ? lds4(orq + nz2) : (f & kQGhYp) ? lds4(gbuf + (it.gy >> 16) * nz2 + q4) : zero4;
+    const float4 nv =
+        update_quad<T>(a, f, c, rowq, orq, ss + it.roff + c * hp, add4(xm, xp), add4(ym, yp), track, last_max);
+    if (f & kQGhAny) st_tagged4(a.tmirror + it.gq + c * cstride, nv, tag_out);
+}
+
+// Polls the thread's ghost quads (colour offset coff) until all carry `tag`
+// and copies them to the ghost buffer; tag 0 stores zeros (the first red
+// sweep of a cycle).  All loads are issued before any tag is checked, and only
+// a miss repeats them.  Bounded like poll_pair.
+template <int kG>
+__device__ __forceinline__ void fetch_ghosts(const u64 *tm, const GhostQuad (&g)[kG], long long coff, unsigned tag,
+                                             float *gbuf, int *status, bool &failed) {
+    u64 w[kG][4];
+#pragma unroll
+    for (int i = 0; i < kG; i++) w[i][0] = w[i][1] = w[i][2] = w[i][3] = 0;
+    if (tag) {
+        long long n = 0;
+        while (true) {
+#pragma unroll
+            for (int i = 0; i < kG; i++) {
+                if (g[i].dst < 0) continue;
+                const u64 *p = tm + g[i].src + coff;
+                asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];"
+                             : "=l"(w[i][0]), "=l"(w[i][1])
+                             : "l"(p)
+                             : "memory");
+                asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];"
+                             : "=l"(w[i][2]), "=l"(w[i][3])
+                             : "l"(p + 2)
+                             : "memory");
+            }
+            bool ok = true;
+#pragma unroll
+            for (int i = 0; i < kG; i++)
+                if (g[i].dst >= 0)
+                    ok = ok && (unsigned)(w[i][0] >> 32) == tag && (unsigned)(w[i][1] >> 32) == tag &&
+                         (unsigned)(w[i][2] >> 32) == tag && (unsigned)(w[i][3] >> 32) == tag;
+            if (ok || failed) break;
+            if ((++n & 63) == 0 && (n > kMaxPoll || ld_volatile(status))) {
+                failed = true;
+                atomicExch(status, 1);
+                break;
+            }
+            if (kPollSleepNs) __nanosleep(kPollSleepNs);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kG; i++)
+        if (g[i].dst >= 0)
+            *reinterpret_cast<float4 *>(gbuf + g[i].dst) =
+                make_float4(__uint_as_float((unsigned)w[i][0]), __uint_as_float((unsigned)w[i][1]),
+                            __uint_as_float((unsigned)w[i][2]), __uint_as_float((unsigned)w[i][3]));
 }
 
 // Correction of a neighbouring block's node from its mirror entry (either
@@ -596,9 +687,11 @@ __device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block
     }
 }
 
-// kTag: tagged exchange (float corrections in quads); kItems: 1 or 2 work
-// items per thread decoded once per solve, 0 decoded in every sweep.
-template <typename T, typename S, bool kTag, int kItems>
+// kTag: tagged exchange (float corrections in quads).  kInner, kFace,
+// kGhost > 0: staged sweep with at most that many inner quads per compute
+// thread, perimeter quads per thread and ghost quads per fetch thread, decoded
+// once per solve; kInner = 0: the generic tagged sweep.
+template <typename T, typename S, bool kTag, int kInner, int kFace, int kGhost>
 __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double s_tot[3];
@@ -619,8 +712,9 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     // shared memory: delta | src (when it fits)
     S *sd = reinterpret_cast<S *>(smem_raw);
     S *ss = a.src_smem ? sd + own : nullptr;
-    // tagged sweeps: the block's rows, face rows first
-    unsigned *order = reinterpret_cast<unsigned *>(sd + (size_t)own * (a.src_smem ? 2 : 1));
+    // tagged sweeps: row tables and the ghost buffer
+    const Staged st(sd + (size_t)a.P * 2 * a.R * nz2 * (a.src_smem ? 2 : 1), a.P, a.R);
+    unsigned *order = st.order;
     auto SD = [&](int p, int c, int j, int t) -> S & { return sd[((p * 2 + c) * nr + j) * nz2 + t]; };
     unsigned my_phase = 0;
     // colour sweeps: thread -> half-line position t_own, rows r_start, +rows_step
@@ -652,11 +746,86 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
                 }
         }
     }
-    [[maybe_unused]] Item items[kItems > 0 ? kItems : 1];
-    if constexpr (kTag && kItems > 0) {
+    constexpr bool kStaged = kTag && kInner > 0;
+    [[maybe_unused]] Quad inner[kStaged ? kInner : 1];
+    [[maybe_unused]] FaceQuad face[kStaged ? kFace : 1];
+    [[maybe_unused]] GhostQuad ghost[kStaged ? kGhost : 1];
+    if constexpr (kStaged) {
+        __shared__ int s_nf, s_ng;
+        if (tid == 0) {
+            // perimeter rows and their ghost rows
+            int nf = 0, ng = 0;
+            for (int l = 0; l < np * nr; l++) {
+                const int p = l / nr, j = l - p * nr, x = x0 + p, y = y0 + j;
+                if (!(p == 0 || p + 1 == np || j == 0 || j + 1 == nr)) continue;
+                const bool active = y >= 1 && y <= ny - 2;
+                unsigned gi[4] = {0xffffu, 0xffffu, 0xffffu, 0xffffu};
+                const bool need[4] = {active && p == 0 && x - 1 >= 1, active && p + 1 == np && x + 1 <= a.nx - 2,
+                                      active && j == 0 && y - 1 >= 1, active && j + 1 == nr && y + 1 <= ny - 2};
+                const int sx[4] = {x - 1, x + 1, x, x}, sy[4] = {y, y, y - 1, y + 1};
+                for (int d = 0; d < 4; d++)
+                    if (need[d]) {
+                        st.gsrc[ng] = (unsigned)(((2ll * sx[d]) * ny + sy[d]) * nz2);
+                        gi[d] = (unsigned)ng++;
+                    }
+                st.ftab[nf] = (unsigned)p << 16 | (unsigned)j;
+                st.fgi[2 * nf] = gi[0] | gi[1] << 16;
+                st.fgi[2 * nf + 1] = gi[2] | gi[3] << 16;
+                nf++;
+            }
+            s_nf = nf;
+            s_ng = ng;
+        }
         __syncthreads();
+        const int nq = nz2 / 4, nfq = s_nf * nq, ngq = s_ng * nq;
+        const int ip = max(np - 2, 0), ir = max(nr - 2, 0), niq = ip * ir * nq;
+        const int nct = nth - kGhostThreads;
 #pragma unroll
-        for (int k = 0; k < kItems; k++) items[k] = make_item<T>(a, B, order, tid + k * nth);
+        for (int k = 0; k < kInner; k++) {
+            const int w = tid - kGhostThreads + k * nct;
+            inner[k] = Quad{0, 0u};
+            if (tid >= kGhostThreads && w < niq) {
+                const int r = w / nq, q = w - r * nq;
+                const int p = 1 + r / ir, j = 1 + r % ir;
+                inner[k].roff = (p * 2 * nr + j) * nz2 + 4 * q;
+                inner[k].flags = quad_flags(x0 + p, y0 + j, q, nq, nz);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kFace; k++) {
+            const int w = tid + k * nth;
+            face[k] = FaceQuad{0, 0u, 0u, 0u, 0u};
+            if (w < nfq) {
+                const int r = w / nq, q = w - r * nq;
+                const unsigned e = st.ftab[r];
+                const int p = (int)(e >> 16), j = (int)(e & 0xffffu), x = x0 + p, y = y0 + j;
+                if (y >= 1 && y <= ny - 2) {
+                    unsigned f = quad_flags(x, y, q, nq, nz);
+                    const unsigned gx = st.fgi[2 * r], gy = st.fgi[2 * r + 1];
+                    if (p > 0) f |= kQOwnXm;
+                    else if ((gx & 0xffffu) != 0xffffu) f |= kQGhXm;
+                    if (p + 1 < np) f |= kQOwnXp;
+                    else if ((gx >> 16) != 0xffffu) f |= kQGhXp;
+                    if (j > 0) f |= kQOwnYm;
+                    else if ((gy & 0xffffu) != 0xffffu) f |= kQGhYm;
+                    if (j + 1 < nr) f |= kQOwnYp;
+                    else if ((gy >> 16) != 0xffffu) f |= kQGhYp;
+                    face[k] = FaceQuad{(p * 2 * nr + j) * nz2 + 4 * q, f,
+                                       (unsigned)(((2ll * x) * ny + y) * nz2 + 4 * q), gx, gy};
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kGhost; k++) {
+            const int g = tid + k * kGhostThreads;
+            ghost[k] = GhostQuad{0u, -1};
+            if (tid < kGhostThreads && g < ngq) {
+                const int r = g / nq, q = g - r * nq;
+                ghost[k] = GhostQuad{st.gsrc[r] + 4u * q, r * nz2 + 4 * q};
+            }
+        }
+        // the first sweep reads zero ghosts
+        for (int e = tid; e < 2 * (a.P + a.R) * nz2; e += nth) st.gbuf[e] = 0.0f;
     }
 
     // ---- entry: zero delta (shared and own global mirror) -----------------
@@ -811,11 +980,25 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
                     // red(t) is half-sweep 2t+1, black(t) 2t+2; red reads black(t-1)
                     const unsigned tag_in = c == 0 ? (it == 0 ? 0u : 2u * t) : 2u * t + 1u;
                     const unsigned tag_out = 2u * t + 1u + (unsigned)c;
-                    if constexpr (kItems > 0) {
+                    if constexpr (kStaged) {
+                        // perimeter rows first, from the ghosts fetched during the
+                        // previous sweep; then the inner rows while the fetch threads
+                        // poll the neighbours' perimeter rows of this sweep for the next
+                        // one (zeros after a cycle's last sweep: the next cycle starts
+                        // from zero corrections)
+                        const long long cstride = (long long)ny * nz2;
+                        const bool track = it == m - 1;
 #pragma unroll
-                        for (int k = 0; k < kItems; k++)
-                            sweep_item<T>(a, items[k], c, hp, (long long)ny * nz2, sd, ss, tag_in, tag_out,
-                                          it == m - 1, last_max, failed);
+                        for (int k = 0; k < kFace; k++)
+                            sweep_face<T>(a, face[k], c, hp, cstride, sd, ss, st.gbuf, tag_out, track, last_max);
+                        __syncthreads();
+                        if (tid < kGhostThreads) {
+                            const unsigned tag_next = (c == 1 && it == m - 1) ? 0u : tag_out;
+                            fetch_ghosts<kGhost>(a.tmirror, ghost, c * cstride, tag_next, st.gbuf, a.status, failed);
+                        } else {
+#pragma unroll
+                            for (int k = 0; k < kInner; k++) sweep_inner<T>(a, inner[k], c, hp, sd, ss, track, last_max);
+                        }
                     } else {
                         sweep_quads_tagged<T>(a, B, c, sd, ss, order, it == m - 1, last_max, tag_out, tag_in,
                                               failed);
@@ -879,7 +1062,7 @@ static hv_status plan_for(hv_ctx *c) {
         for (int P = 1; P <= interior; P++)
             for (int R = 1; R <= g.ny; R++) {
                 const size_t own = (size_t)P * 2 * R * nz2;
-                const size_t smem = sizeof(S) * own * 2 + ((size_t)P * R * 4 + 15) / 16 * 16;
+                const size_t smem = sizeof(S) * own * 2 + Staged::bytes(P, R, nz2);
                 if (smem > limit) break;
                 const long long bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
                 if (bxn * byn > prop.multiProcessorCount) continue;
@@ -927,11 +1110,11 @@ static hv_status plan_for(hv_ctx *c) {
     if (!f.ok) return HV_OK;  // the fused path reports HV_ERR_UNSUPPORTED
     f.nz2 = nz2;
     f.threads = kSorThreads;
-    const void *kerns[4] = {(const void *)k_sor_fast<S, S, false, 0>, nullptr, nullptr, nullptr};
+    const void *kerns[4] = {(const void *)k_sor_fast<S, S, false, 0, 0, 0>, nullptr, nullptr, nullptr};
     if constexpr (sizeof(S) == 4) {
-        kerns[1] = (const void *)k_sor_fast<S, S, true, 0>;
-        kerns[2] = (const void *)k_sor_fast<S, S, true, 1>;
-        kerns[3] = (const void *)k_sor_fast<S, S, true, 2>;
+        kerns[1] = (const void *)k_sor_fast<S, S, true, 0, 0, 0>;
+        kerns[2] = (const void *)k_sor_fast<S, S, true, 1, 1, 2>;
+        kerns[3] = (const void *)k_sor_fast<S, S, true, 2, 1, 3>;
     }
     for (const void *kern : kerns) {
         if (!kern) continue;
@@ -1027,13 +1210,18 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.its_ring = its_ring;
     a.ring = ring;
     void *args[] = {&a};
-    const void *kern = (const void *)k_sor_fast<T, S, false, 0>;
+    const void *kern = (const void *)k_sor_fast<T, S, false, 0, 0, 0>;
     if constexpr (sizeof(S) == 4)
         if (a.vec4 && c->fast.sor_exchange == HV_SOR_EXCHANGE_AUTO) {
-            const long long per_thread = ((long long)f.P * f.R * (f.nz2 / 4) + f.threads - 1) / f.threads;
-            kern = per_thread == 1   ? (const void *)k_sor_fast<T, S, true, 1>
-                   : per_thread == 2 ? (const void *)k_sor_fast<T, S, true, 2>
-                                     : (const void *)k_sor_fast<T, S, true, 0>;
+            // staged sweep when its per-thread quad counts fit an instantiation
+            const long long nq = f.nz2 / 4, P = f.P, R = f.R;
+            const long long inner = std::max(P - 2, 0ll) * std::max(R - 2, 0ll);
+            const long long ni = (inner * nq + f.threads - kGhostThreads - 1) / (f.threads - kGhostThreads);
+            const long long nf = ((P * R - inner) * nq + f.threads - 1) / f.threads;
+            const long long ng = (2 * (P + R) * nq + kGhostThreads - 1) / kGhostThreads;
+            kern = (const void *)k_sor_fast<T, S, true, 0, 0, 0>;
+            if (ni <= 1 && nf <= 1 && ng <= 2) kern = (const void *)k_sor_fast<T, S, true, 1, 1, 2>;
+            else if (ni <= 2 && nf <= 1 && ng <= 3) kern = (const void *)k_sor_fast<T, S, true, 2, 1, 3>;
         }
     HV_CUDA(cudaLaunchCooperativeKernel(kern, dim3(f.nblocks), dim3(f.threads), args, f.smem, c->stream));
     return HV_OK;

@@ -310,7 +310,7 @@ typedef struct hv_fast_options {
     int sor_exchange;     /* hv_sor_exchange                                    */
 } hv_fast_options;
 
-/* Defaults: HV_WARM_PREVIOUS, inner 2..64, sort every 16 steps, 8-step graphs,
+/* Defaults: HV_WARM_PREVIOUS, inner 2..256, sort every 16 steps, 8-step graphs,
  * HV_SOR_EXCHANGE_AUTO. */
 HV_API void hv_fast_options_default(hv_fast_options *o);
 HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);
