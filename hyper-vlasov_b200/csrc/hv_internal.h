@@ -100,11 +100,15 @@ struct SorFast {
 };
 
 // Decomposed smoothing plan (k_smooth_fast.cu).
+constexpr int kSmoothMaxR = 16;  // largest |a|, |b| or z half-width handled
 struct SmoothFast {
-    bool ok = false;           // tap table is symmetric with contiguous z runs
+    bool ok = false;           // tap table is symmetric with contiguous runs
     int A = 0, B = 0, W = 0;   // max |a|, |b|, z half-width
-    float *g = nullptr;        // device: gx[A+1], gy[B+1], gz[W+1]
-    int *w = nullptr;          // device: w(|a|,|b|) or -1, (A+1) x (B+1)
+    float gx[kSmoothMaxR + 1] = {}, gy[kSmoothMaxR + 1] = {}, gz[kSmoothMaxR + 1] = {};
+    int bm[kSmoothMaxR + 1] = {};                        // largest |b| for each |a| (-1: none)
+    int wt[(kSmoothMaxR + 1) * (kSmoothMaxR + 1)] = {};  // w(|a|, |b|) (-1: none)
+    size_t smem = 0;
+    int per = 0;               // R = max(A, B, W): the kernel instantiation
 };
 
 // Fast-path (fused) buffers.

@@ -9,14 +9,13 @@
 //   rho_s(i,j,k) = sum_a g(a) sum_b g(b) Z_{w(|a|,|b|)}(i+a, j+b, k),
 //   Z_w(i,j,k)   = sum_{|c|<=w} g(c) rho(i,j,k+c),
 //
-// with the same pair set as the reference.  A block owns a BX x BY x BK
-// output tile of one species and marches over the input x-planes that touch
-// it.  Per input plane it stages the rho tile (with y and z halos) in shared
-// memory, builds Z_0..Z_W for its rows incrementally (2 FMA per w), forms the
-// (b)-disc sums Y_|a| for its own rows and adds g(a) Y_|a| into the
-// accumulators of the output planes x = i - a.  That is about
-// 1.6 x (20 + sum_a (2 B(a) + 1)) ~ 300 FMA per output node for the 3911-tap
-// stencil of a 128^3 grid at h = 0.25 fm, against 3911 for the direct sum.
+// with the same pair set as the reference.  A block owns a 16 x 16 (y, z)
+// column tile of one species and one x segment, and marches along x over the
+// input planes that reach it (see k_smooth_march): per input plane about
+// 2 (W + 1) FMA for the z-runs of each staged row and sum_a (bm(a) + 1) pair
+// sums for the disc sums of each column -- roughly 110 for the 3911-tap
+// stencil of a 128^3 grid at h = 0.25 fm (A = B = W = 9), against 3911 for
+// the direct sum.
 //
 // Used when the tap table passes the symmetry and contiguity checks in
 // smooth_fast_plan (all cubic grids); otherwise the direct kernel runs.
@@ -29,105 +28,164 @@
 namespace hv {
 namespace {
 
-constexpr int kBX = 32, kBY = 16, kBK = 32;
-constexpr int kThreads = kBY * kBK;
-constexpr int kMaxR = 16;  // largest |a|, |b| or w handled
+constexpr int kMBY = 16, kMBK = 16;         // output columns (y, z) of a block
+constexpr int kMThreads = kMBY * kMBK;
+constexpr int kMaxR = kSmoothMaxR;
+constexpr int kXSplit = 2;                   // x segments per column tile
 
-struct SmoothArgs {
+struct MarchArgs {
     int nx, ny, nz;
     long long G;
     int A, B, W;
     float term;
-    const float *g;   // gx[A+1] gy[B+1] gz[W+1]
-    const int *wtab;  // (A+1) x (B+1)
-    const float *src; // 2G
-    float *dst;       // 2G
+    float gx[kMaxR + 1], gy[kMaxR + 1], gz[kMaxR + 1];
+    int bm[kMaxR + 1];                        // largest |b| with a tap for each |a| (-1: none)
+    int wt[(kMaxR + 1) * (kMaxR + 1)];        // w(|a|, |b|) at |a| (kMaxR + 1) + |b| (-1: none)
+    const float *src;                         // 2G
+    float *dst;                               // 2G
 };
 
-__global__ void __launch_bounds__(kThreads) k_smooth_decomposed(SmoothArgs a) {
-    extern __shared__ __align__(16) float sm[];
-    const int A = a.A, B = a.B, W = a.W;
-    const int rows = kBY + 2 * B, cols = kBK + 2 * W;
-    float *s_rho = sm;                             // rows x cols
-    float *s_z = s_rho + rows * cols;              // (W+1) x rows x kBK
-    float *s_acc = s_z + (W + 1) * rows * kBK;     // kBX x kThreads
-    __shared__ float s_gx[kMaxR + 1], s_gy[kMaxR + 1], s_gz[kMaxR + 1];
-    __shared__ int s_w[(kMaxR + 1) * (kMaxR + 1)];
-    __shared__ int s_bm[kMaxR + 1];
+// Plane xi of the block's rho tile (y halo B, z halo W; zero outside the
+// grid) into registers: element e = tid + i * kMThreads.
+template <int R, int kPer>
+__device__ __forceinline__ void load_plane(const MarchArgs &a, const float *src, int xi, int Y0, int K0,
+                                           float (&v)[kPer]) {
+    constexpr int rows = kMBY + 2 * R, cols = kMBK + 2 * R;
+    const float *plane = src + (long long)xi * a.ny * a.nz;
+#pragma unroll
+    for (int i = 0; i < kPer; i++) {
+        const int e = threadIdx.x + i * kMThreads;
+        const int r = e / cols, cc = e - r * cols;
+        const int y = Y0 - R + r, z = K0 - R + cc;
+        v[i] = (e < rows * cols && xi >= 0 && xi < a.nx && y >= 0 && y < a.ny && z >= 0 && z < a.nz)
+                   ? __ldg(plane + (long long)y * a.nz + z)
+                   : 0.0f;
+    }
+}
 
+// One block: a 16 x 16 column tile (y, z) of one species and one x segment of
+// the outputs.  It marches over the input planes xi that reach the segment:
+// the plane's rho tile (the next plane's loads in flight in registers during
+// this plane's sums) gives the z-runs Z_w, w = 0..W, of every staged
+// row; each thread then forms, for its column, the disc sums
+// Y_|a| = sum_|b|<=bm(a) g(b) Z_w(|a|,|b|)(y + b) and adds g(a) Y_|a| to the
+// outputs x = xi -+ a, held in a thread-private ring of 2A + 1 planes in shared
+// memory.  Output plane xo is complete after plane xo + A and is written then.
+// R >= A, B, W is the halo and the unrolled extent of the loops over |a|, |b|
+// and w; the tables hold -1 (no tap) and zero weights beyond A, B, W.
+template <int R>
+__global__ void __launch_bounds__(kMThreads) k_smooth_march(const __grid_constant__ MarchArgs a) {
+    extern __shared__ __align__(16) float sm[];
+    constexpr int rows = kMBY + 2 * R, cols = kMBK + 2 * R;
+    constexpr int kPer = (rows * cols + kMThreads - 1) / kMThreads;
+    const int A = a.A, ring = 2 * A + 1;
+    float *s_rho = sm;                               // rows x cols
+    float *s_z = s_rho + rows * cols;                // (R + 1) x rows x kMBK
+    float *s_acc = s_z + (R + 1) * rows * kMBK;      // ring x kMThreads
     const int tid = threadIdx.x;
-    // block -> (species, x tile, y tile, z tile)
-    const int tz = (a.nz + kBK - 1) / kBK, ty = (a.ny + kBY - 1) / kBY, tx = (a.nx + kBX - 1) / kBX;
+    const int tz = (a.nz + kMBK - 1) / kMBK, ty = (a.ny + kMBY - 1) / kMBY;
+    const int xlen = (a.nx + kXSplit - 1) / kXSplit;
     int bid = blockIdx.x;
     const int kt = bid % tz;
     bid /= tz;
     const int yt = bid % ty;
     bid /= ty;
-    const int xt = bid % tx;
-    const int sp = bid / tx;
-    const int X0 = xt * kBX, Y0 = yt * kBY, K0 = kt * kBK;
+    const int xs = bid % kXSplit;
+    const int sp = bid / kXSplit;
+    const int Y0 = yt * kMBY, K0 = kt * kMBK, X0 = xs * xlen, X1 = min(a.nx, X0 + xlen);
+    if (X0 >= X1) return;
     const float *src = a.src + sp * a.G;
+    const int j = tid / kMBK, k = tid % kMBK, y = Y0 + j, z = K0 + k;
+    const bool out_ok = y < a.ny && z < a.nz;
 
-    if (tid <= A) s_gx[tid] = a.g[tid];
-    if (tid <= B) s_gy[tid] = a.g[A + 1 + tid];
-    if (tid <= W) s_gz[tid] = a.g[A + 1 + B + 1 + tid];
-    for (int e = tid; e < (A + 1) * (B + 1); e += kThreads) s_w[e] = a.wtab[e];
-    for (int e = tid; e < kBX * kThreads; e += kThreads) s_acc[e] = 0.0f;
-    __syncthreads();
-    if (tid <= A) {  // largest |b| with a tap for this |a|
-        int bm = -1;
-        for (int b = 0; b <= B; b++)
-            if (s_w[tid * (B + 1) + b] >= 0) bm = b;
-        s_bm[tid] = bm;
-    }
-
-    const int j = tid / kBK, k = tid % kBK;
-    const int xlo = max(0, X0 - A), xhi = min(a.nx, X0 + kBX + A);
-    for (int xi = xlo; xi < xhi; xi++) {
-        // 1. rho tile of plane xi with y and z halos (zero outside the grid)
-        const float *plane = src + (long long)xi * a.ny * a.nz;
-        for (int e = tid; e < rows * cols; e += kThreads) {
-            int r = e / cols, cc = e % cols;
-            int y = Y0 - B + r, z = K0 - W + cc;
-            s_rho[e] = (y >= 0 && y < a.ny && z >= 0 && z < a.nz) ? __ldg(plane + (long long)y * a.nz + z) : 0.0f;
-        }
-        __syncthreads();
-        // 2. z-runs Z_w for every staged row, w = 0..W
-        for (int e = tid; e < rows * kBK; e += kThreads) {
-            int r = e / kBK, kk = e % kBK;
-            const float *line = s_rho + r * cols + kk + W;
-            float zsum = s_gz[0] * line[0];
-            s_z[r * kBK + kk] = zsum;
-            for (int w = 1; w <= W; w++) {
-                zsum += s_gz[w] * (line[w] + line[-w]);
-                s_z[(w * rows + r) * kBK + kk] = zsum;
+    for (int s = 0; s < ring; s++) s_acc[s * kMThreads + tid] = 0.0f;
+    const int xfirst = max(0, X0 - A), xlast = min(a.nx - 1, X1 - 1 + A);
+    float v[kPer];
+    load_plane<R, kPer>(a, src, xfirst, Y0, K0, v);
+    int slot = xfirst % ring;  // ring slot of plane xi
+    for (int xi = xfirst; xi <= X1 - 1 + A; xi++, slot = slot + 1 == ring ? 0 : slot + 1) {
+        const bool have = xi <= xlast;
+        if (have) {
+#pragma unroll
+            for (int i = 0; i < kPer; i++) {
+                const int e = tid + i * kMThreads;
+                if (e < rows * cols) s_rho[e] = v[i];
             }
         }
         __syncthreads();
-        // 3. disc sums over b for each |a|, scattered to the output planes
-        for (int aa = 0; aa <= A; aa++) {
-            const int bm = s_bm[aa];
-            if (bm < 0) continue;
-            const int xo1 = xi - aa - X0, xo2 = xi + aa - X0;
-            const bool h1 = xo1 >= 0 && xo1 < kBX, h2 = aa > 0 && xo2 >= 0 && xo2 < kBX;
-            if (!h1 && !h2) continue;
-            float ysum = 0.0f;
-            const int *wr = s_w + aa * (B + 1);
-            for (int b = -bm; b <= bm; b++) {
-                const int w = wr[b < 0 ? -b : b];
-                if (w < 0) continue;
-                ysum += s_gy[b < 0 ? -b : b] * s_z[(w * rows + j + B + b) * kBK + k];
+        if (have) {
+            // z-runs of every staged row
+            for (int e = tid; e < rows * kMBK; e += kMThreads) {
+                const int r = e / kMBK, kk = e - r * kMBK;
+                const float *line = s_rho + r * cols + kk + R;
+                float zsum = a.gz[0] * line[0];
+                s_z[r * kMBK + kk] = zsum;
+#pragma unroll
+                for (int w = 1; w <= R; w++) {
+                    zsum += a.gz[w] * (line[w] + line[-w]);
+                    s_z[(w * rows + r) * kMBK + kk] = zsum;
+                }
             }
-            const float gy = s_gx[aa] * ysum;
-            if (h1) s_acc[xo1 * kThreads + tid] += gy;
-            if (h2) s_acc[xo2 * kThreads + tid] += gy;
         }
+        // the next plane's loads overlap this plane's sums
+        if (xi + 1 <= xlast) load_plane<R, kPer>(a, src, xi + 1, Y0, K0, v);
         __syncthreads();
+        if (have) {
+            const float *zc = s_z + (j + R) * kMBK + k;  // this column's row, width 0
+            constexpr int zstride = rows * kMBK;
+#pragma unroll
+            for (int aa = 0; aa <= R; aa++) {
+                const int bm = a.bm[aa];
+                if (bm < 0) continue;
+                const int xo1 = xi - aa, xo2 = xi + aa;
+                const bool h1 = xo1 >= X0 && xo1 < X1, h2 = aa > 0 && xo2 >= X0 && xo2 < X1;
+                if (!h1 && !h2) continue;
+                const int *wr = a.wt + aa * (kMaxR + 1);
+                float y0 = a.gy[0] * zc[wr[0] * zstride], y1 = 0.0f;
+#pragma unroll
+                for (int b = 1; b <= R; b++) {
+                    if (b > bm) break;
+                    const float *pb = zc + wr[b] * zstride;
+                    const float t = a.gy[b] * (pb[b * kMBK] + pb[-b * kMBK]);
+                    if (b & 1) y0 += t;
+                    else y1 += t;
+                }
+                const float c = a.gx[aa] * (y0 + y1);
+                const int s1 = slot - aa < 0 ? slot - aa + ring : slot - aa;
+                const int s2 = slot + aa >= ring ? slot + aa - ring : slot + aa;
+                if (h1) s_acc[s1 * kMThreads + tid] += c;
+                if (h2) s_acc[s2 * kMThreads + tid] += c;
+            }
+        }
+        // output plane xi - A is complete
+        const int xo = xi - A;
+        if (xo >= X0 && xo < X1) {
+            float *acc = s_acc + (slot - A < 0 ? slot - A + ring : slot - A) * kMThreads + tid;
+            if (out_ok) a.dst[sp * a.G + ((long long)xo * a.ny + y) * a.nz + z] = *acc * a.term;
+            *acc = 0.0f;
+        }
     }
-    const int y = Y0 + j, z = K0 + k;
-    if (y < a.ny && z < a.nz) {
-        for (int xo = 0; xo < kBX && X0 + xo < a.nx; xo++)
-            a.dst[sp * a.G + ((long long)(X0 + xo) * a.ny + y) * a.nz + z] = s_acc[xo * kThreads + tid] * a.term;
+}
+
+const void *march_kernel(int r) {
+    switch (r) {
+    case 1: return (const void *)k_smooth_march<1>;
+    case 2: return (const void *)k_smooth_march<2>;
+    case 3: return (const void *)k_smooth_march<3>;
+    case 4: return (const void *)k_smooth_march<4>;
+    case 5: return (const void *)k_smooth_march<5>;
+    case 6: return (const void *)k_smooth_march<6>;
+    case 7: return (const void *)k_smooth_march<7>;
+    case 8: return (const void *)k_smooth_march<8>;
+    case 9: return (const void *)k_smooth_march<9>;
+    case 10: return (const void *)k_smooth_march<10>;
+    case 11: return (const void *)k_smooth_march<11>;
+    case 12: return (const void *)k_smooth_march<12>;
+    case 13: return (const void *)k_smooth_march<13>;
+    case 14: return (const void *)k_smooth_march<14>;
+    case 15: return (const void *)k_smooth_march<15>;
+    case 16: return (const void *)k_smooth_march<16>;
+    default: return nullptr;
     }
 }
 
@@ -159,7 +217,8 @@ hv_status smooth_fast_plan(hv_ctx *c) {
         int &w = wtab[std::abs(a) * (B + 1) + std::abs(b)];
         w = std::max(w, std::abs(cz));
     }
-    // each present (a,b) column must be the full run |c| <= w
+    // each present (a,b) column must be the full run |c| <= w, and for each
+    // |a| the present |b| must be 0..bm(a)
     size_t expect = 0;
     for (int a = -A; a <= A; a++)
         for (int b = -B; b <= B; b++) {
@@ -167,6 +226,17 @@ hv_status smooth_fast_plan(hv_ctx *c) {
             if (w >= 0) expect += 2 * w + 1;
         }
     if (expect != taps.size()) return HV_OK;
+    for (int i = 0; i <= kMaxR; i++) f.bm[i] = -1;
+    for (int i = 0; i < (kMaxR + 1) * (kMaxR + 1); i++) f.wt[i] = -1;
+    for (int a = 0; a <= A; a++) {
+        int bm = -1;
+        for (int b = 0; b <= B; b++)
+            if (wtab[a * (B + 1) + b] >= 0) bm = b;
+        for (int b = 0; b <= bm; b++)
+            if (wtab[a * (B + 1) + b] < 0) return HV_OK;
+        f.bm[a] = bm;
+        for (int b = 0; b <= B; b++) f.wt[a * (kMaxR + 1) + b] = wtab[a * (B + 1) + b];
+    }
     // separable weights from the same node coordinates as the table
     const hv_world &wd = c->world;
     const double sig = c->params.sigma_r, e = 1.0 / (2.0 * sig * sig);
@@ -176,37 +246,29 @@ hv_status smooth_fast_plan(hv_ctx *c) {
         double d = dm * (2.0 * ctr / n - 1.0) - dm * (2.0 * (ctr + off) / n - 1.0);
         return (float)std::exp(-d * d * e);
     };
-    std::vector<float> g;
-    for (int a = 0; a <= A; a++) g.push_back(g1(0, a));
-    for (int b = 0; b <= B; b++) g.push_back(g1(1, b));
-    for (int cz = 0; cz <= W; cz++) g.push_back(g1(2, cz));
-    HV_CUDA(cudaMalloc((void **)&f.g, sizeof(float) * g.size()));
-    HV_CUDA(cudaMalloc((void **)&f.w, sizeof(int) * wtab.size()));
-    HV_CUDA(cudaMemcpyAsync(f.g, g.data(), sizeof(float) * g.size(), cudaMemcpyHostToDevice, c->stream));
-    HV_CUDA(cudaMemcpyAsync(f.w, wtab.data(), sizeof(int) * wtab.size(), cudaMemcpyHostToDevice, c->stream));
-    const size_t smem = sizeof(float) * ((size_t)(kBY + 2 * B) * (kBK + 2 * W) + (size_t)(W + 1) * (kBY + 2 * B) * kBK +
-                                         (size_t)kBX * kThreads);
-    HV_CUDA(cudaFuncSetAttribute(k_smooth_decomposed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int i = 0; i <= kMaxR; i++) f.gx[i] = f.gy[i] = f.gz[i] = 0.0f;
+    for (int a = 0; a <= A; a++) f.gx[a] = g1(0, a);
+    for (int b = 0; b <= B; b++) f.gy[b] = g1(1, b);
+    for (int cz = 0; cz <= W; cz++) f.gz[cz] = g1(2, cz);
+    const int R = std::max(1, std::max(A, std::max(B, W)));
+    const int rows = kMBY + 2 * R, cols = kMBK + 2 * R;
+    f.per = R;
+    f.smem = sizeof(float) * ((size_t)rows * cols + (size_t)(R + 1) * rows * kMBK + (size_t)(2 * A + 1) * kMThreads);
+    HV_CUDA(cudaFuncSetAttribute(march_kernel(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
     f.A = A;
     f.B = B;
     f.W = W;
     f.ok = true;
-    HV_CUDA(cudaStreamSynchronize(c->stream));
     return HV_OK;
 }
 
-void smooth_fast_release(hv_ctx *c) {
-    SmoothFast &f = c->fused.smooth;
-    if (f.g) cudaFree(f.g);
-    if (f.w) cudaFree(f.w);
-    f = SmoothFast();
-}
+void smooth_fast_release(hv_ctx *c) { c->fused.smooth = SmoothFast(); }
 
 hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
     const SmoothFast &f = c->fused.smooth;
     const Geom &g = c->geom;
     const hv_run_params &p = c->params;
-    SmoothArgs a;
+    MarchArgs a;
     a.nx = g.nx;
     a.ny = g.ny;
     a.nz = g.nz;
@@ -216,15 +278,19 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
     a.W = f.W;
     const double sig = p.sigma_r;
     a.term = (float)((1.0 / p.part_per_nucleon) * (1.0 / std::pow(2.0 * kPi * sig * sig, 1.5)));
-    a.g = f.g;
-    a.wtab = f.w;
+    for (int i = 0; i <= kMaxR; i++) {
+        a.gx[i] = f.gx[i];
+        a.gy[i] = f.gy[i];
+        a.gz[i] = f.gz[i];
+        a.bm[i] = f.bm[i];
+    }
+    for (int i = 0; i < (kMaxR + 1) * (kMaxR + 1); i++) a.wt[i] = f.wt[i];
     a.src = rho_raw;
     a.dst = rho;
-    const int tz = (g.nz + kBK - 1) / kBK, ty = (g.ny + kBY - 1) / kBY, tx = (g.nx + kBX - 1) / kBX;
-    const size_t smem = sizeof(float) * ((size_t)(kBY + 2 * f.B) * (kBK + 2 * f.W) +
-                                         (size_t)(f.W + 1) * (kBY + 2 * f.B) * kBK + (size_t)kBX * kThreads);
-    k_smooth_decomposed<<<2 * tx * ty * tz, kThreads, smem, c->stream>>>(a);
-    HV_CUDA(cudaGetLastError());
+    const int tz = (g.nz + kMBK - 1) / kMBK, ty = (g.ny + kMBY - 1) / kMBY;
+    void *args[] = {&a};
+    HV_CUDA(cudaLaunchKernel(march_kernel(f.per), dim3(2 * kXSplit * ty * tz), dim3(kMThreads), args, f.smem,
+                             c->stream));
     return HV_OK;
 }
 

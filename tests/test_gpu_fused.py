@@ -229,3 +229,29 @@ def test_tagged_exchange_matches_flag_exchange(hv, n):
     assert max_rel(o1["dipole"], o0["dipole"]) < 1e-5
     assert max_rel(c1, c0) < 1e-5
     assert all(np.max(np.abs(a - b)) < 1e-4 for a, b in zip(p0, p1))
+
+
+@pytest.mark.parametrize("wname", ["40Ca-4k-32^3", "208Pb-104k-64^3", "208Pb-20.8k-128^3"])
+def test_fused_smoothing_matches_direct_sum(hv, wname):
+    """The fused path's decomposed smoothing (z-runs and disc sums marched along
+    x) on the raw density of a fused run's final state, against the direct tap
+    sum of hv_smooth_density in double on the same raw density: within 5e-6
+    relative, and no further from it than twice the float direct sum is (both
+    float results carry the rounding of sums of up to ~4000 terms)."""
+    w = hv.WORKLOADS[wname]
+    p = hv.workload_particles(w, np.float32)
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        s.upload_particles(*p)
+        s.run(2, hv.HV_PATH_FUSED)
+        fast = s.download_field(hv.HV_FIELD_DENSITY)
+        raw = s.download_field(hv._lib.HV_FIELD_DENSITY_RAW)
+        s.smooth()
+        direct = s.download_field(hv.HV_FIELD_DENSITY)
+    with hv.Session.from_workload(w, hv.HV_F64) as s:
+        s.upload_field(hv._lib.HV_FIELD_DENSITY_RAW, raw.astype(np.float64))
+        s.smooth()
+        ref = s.download_field(hv.HV_FIELD_DENSITY)
+    assert np.abs(ref).max() > 0
+    e_fast, e_direct = max_rel(fast, ref), max_rel(direct, ref)
+    assert e_fast < 5e-6
+    assert e_fast <= 2 * e_direct + 1e-7
