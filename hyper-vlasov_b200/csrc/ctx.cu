@@ -299,6 +299,10 @@ hv_status plain_step(hv_ctx *c, hv_observables *row) {
 bool slots_permuted(hv_ctx *c) { return c->permuted; }
 
 }  // namespace
+
+hv_status plain_step_f64(hv_ctx *c, hv_observables *row) { return plain_step<double>(c, row); }
+hv_status plain_fields_f64(hv_ctx *c, int *sor_its) { return fields_and_gather<double>(c, sor_its); }
+
 }  // namespace hv
 
 using namespace hv;
@@ -420,6 +424,7 @@ hv_status hv_ctx_destroy(hv_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     fused_release(c);
+    adjoint_release(c);
     for (cudaEvent_t e : c->prof.events) cudaEventDestroy(e);
     c->prof.events.clear();
     free_state(c->d64);

@@ -142,6 +142,10 @@ struct Profile {
 
 }  // namespace hv
 
+namespace hv {
+struct Adjoint;  // adjoint.cu
+}
+
 struct hv_ctx {
     hv_world world{};
     hv::Geom geom{};
@@ -168,6 +172,7 @@ struct hv_ctx {
     int step_index = 0;      // steps taken so far (time = step_index * dt)
     void *staging = nullptr; // pinned host staging
     size_t staging_bytes = 0;
+    hv::Adjoint *adjoint = nullptr;  // checkpoints and work arrays of the adjoint
 };
 
 namespace hv {
@@ -208,6 +213,10 @@ hv_status fused_prepare(hv_ctx *c);
 hv_status fused_release(hv_ctx *c);
 hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs);
 void fused_invalidate(hv_ctx *c);
+void adjoint_release(hv_ctx *c);
+// one plain FP64 step / the field solve and gather of the current positions
+hv_status plain_step_f64(hv_ctx *c, hv_observables *row);
+hv_status plain_fields_f64(hv_ctx *c, int *sor_its);
 
 // geometry helpers
 inline Geom make_geom(const hv_world &w) {

@@ -138,6 +138,8 @@ SIGNATURES = {
     "hv_initial_solve": (_S, [_P, _P]),
     "hv_run": (_S, [_P, _I, _I, _P]),
     "hv_simulate": (_S, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "hv_adjoint_forward": (_S, [_P, _I, _I, _P]),
+    "hv_adjoint_backward": (_S, [_P, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -235,6 +235,24 @@ class Session:
         L.check(self.lib.hv_run(self._ctx, steps, path, C.c_void_p(obs.ctypes.data)), "hv_run")
         return obs
 
+    # -- adjoint ---------------------------------------------------------------
+    def adjoint_forward(self, steps, checkpoint_every):
+        """hv_adjoint_forward: `steps` plain FP64 steps with checkpoints every
+        `checkpoint_every` steps; returns the observable rows."""
+        obs = np.zeros(steps, L.OBS_DTYPE)
+        L.check(self.lib.hv_adjoint_forward(self._ctx, steps, checkpoint_every, C.c_void_p(obs.ctypes.data)),
+                "hv_adjoint_forward")
+        return obs
+
+    def adjoint_backward(self, dJ_dD, theta):
+        """hv_adjoint_backward: (dJ/d(t0, t3, sigma, a_sym), dJ/d(A, B, C, gamma))
+        for dJ/dD of the rows of the last adjoint_forward, at theta."""
+        g = np.ascontiguousarray(dJ_dD, dtype=np.float64)
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        gt, gs = np.zeros(4), np.zeros(4)
+        L.check(self.lib.hv_adjoint_backward(self._ctx, _p(g), _p(th), _p(gt), _p(gs)), "hv_adjoint_backward")
+        return gt, gs
+
 
 def simulate(w: Workload, x, y, z, kx, ky, kz, steps, precision=L.HV_F64, path=L.HV_PATH_PLAIN):
     """hv_simulate: the whole GPU run with host buffers (advanced in place).

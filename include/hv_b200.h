@@ -364,6 +364,32 @@ HV_API hv_status hv_simulate(const hv_world *world, int protons, int neutrons,
                       int n_steps, void *x, void *y, void *z,
                       void *kx, void *ky, void *kz, hv_observables *obs);
 
+/* ---- adjoint: gradients of a D(t) objective ----------------------------
+ * No counterpart in the reference, which has no derivative code: the
+ * hand-written adjoint of the plain FP64 step (cpu_simulate's order,
+ * src/hyper_vlasov.cpp:63-104), for the gradient of an objective J(D_0 ..
+ * D_{n-1}) with respect to the Skyrme parameters theta = (t0, t3, sigma,
+ * a_sym) that hv_skyrme_from_t0t3 maps to the context's hv_skyrme.  HV_F64
+ * contexts only (HV_ERR_UNSUPPORTED otherwise).
+ *
+ * hv_adjoint_forward runs n_steps plain steps from the context's current
+ * state (solving its fields first if nothing has), writing one observable row
+ * per step as hv_run does, and keeps the particle state and phi every
+ * checkpoint_every steps (device memory: (n / K + 1) (9 N + G) doubles for the
+ * checkpoints, K (3 N + 8 G) for a recomputed segment).
+ * hv_adjoint_backward takes dJ/dD_n for those rows and returns dJ/dtheta at
+ * theta (which must be the parameters the forward ran with), and, when
+ * grad_skyrme is not NULL, dJ/d(A, B, C, gamma).  It recomputes each segment
+ * from its checkpoint and runs the reversed steps through it: the transposed
+ * gather is a deposit, the transposed deposit a gather of weight gradients,
+ * the transposed Poisson solve a second SOR solve with the context's SOR
+ * settings (warm-started from the previous one).  The context is left in the
+ * state the forward run ended in, with its fields marked stale.  A later
+ * hv_adjoint_forward replaces the checkpoints. */
+HV_API hv_status hv_adjoint_forward(hv_ctx *ctx, int n_steps, int checkpoint_every, hv_observables *obs);
+HV_API hv_status hv_adjoint_backward(hv_ctx *ctx, const double *dJ_dD, const double theta[4],
+                                     double grad_theta[4], double grad_skyrme[4]);
+
 #ifdef __cplusplus
 }
 #endif
