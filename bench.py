@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--cpu-steps", type=int, default=2, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-warmup", type=int, default=0, help=argparse.SUPPRESS)
@@ -244,6 +246,49 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- adjoint
+def adjoint_cost(args, local):
+    """Cost of the gradient of the D(t)-spectrum power (10-25 MeV) with
+    respect to (t0, t3, sigma, a_sym) against a forward run: 40Ca with 1000
+    test particles per nucleon, 32^3 at h = 1 fm, dt = 0.5 fm/c, checkpoints
+    every 50 steps, FP64 plain path.  Host wall time around the synchronous
+    calls (each is a sequence of launches with host-tested SOR)."""
+    from dataclasses import replace
+
+    import numpy as np
+    import torch
+
+    import hv_b200 as hv
+    from hv_b200.spectrum import power_in_band
+    w = replace(hv.CA40_SMALL, ppn=1000, deposit_mode=hv.HV_DEPOSIT_SORTED)
+    steps, every = args.adjoint_steps, 50
+    parts = hv.workload_particles(w, np.float64)
+    theta = np.array([w.t0, w.t3, w.sigma, w.a_sym])
+    with hv.Session.from_workload(w, hv.HV_F64, device=local) as s:
+        s.upload_particles(*parts)
+        s.initial_solve()
+        t0 = time.perf_counter()
+        s.run(steps, hv.HV_PATH_PLAIN)
+        plain = time.perf_counter() - t0
+    with hv.Session.from_workload(w, hv.HV_F64, device=local) as s:
+        s.upload_particles(*parts)
+        s.initial_solve()
+        t0 = time.perf_counter()
+        obs = s.adjoint_forward(steps, every)
+        t1 = time.perf_counter()
+        d = torch.tensor(obs["dipole"], dtype=torch.float64, requires_grad=True)
+        t = np.arange(steps) * w.dt
+        J = power_in_band(d, t, steps * w.dt, w.dt)
+        J.backward()
+        grad, _ = s.adjoint_backward(d.grad.numpy(), theta)
+        t2 = time.perf_counter()
+    return {"workload": f"40Ca, {w.particles} test particles, {w.n}^3, h {w.h} fm, dt {w.dt} fm/c, FP64 plain path",
+            "steps": steps, "checkpoint_every": every, "objective": "power of the D(t) spectrum in 10-25 MeV",
+            "plain_forward_s": plain, "checkpointed_forward_s": t1 - t0, "backward_s": t2 - t1,
+            "backward_over_forward": (t2 - t1) / plain, "gradient_over_forward": (t2 - t0) / plain,
+            "grad_t0_t3_sigma_asym": [float(v) for v in grad], "timing": "host wall time"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def our_arm(args, world, rank, local):
     import numpy as np
@@ -371,6 +416,9 @@ def our_arm(args, world, rank, local):
                              "sor_iterations_per_step": float(ob64["sor_iterations"].mean()),
                              "dipole_max_rel_diff_fused_f32": float(np.max(np.abs(obf["dipole"] - ob64["dipole"])) /
                                                                     dmax) if dmax > 0 else None}
+
+    if not args.no_adjoint and rank == 0:
+        line["adjoint"] = adjoint_cost(args, local)
 
     if not args.no_cpu and rank == 0 and world == 1:
         try:
