@@ -131,3 +131,37 @@ def test_adjoint_rejects_float_contexts_and_missing_forward(hv):
     with hv.Session.from_workload(w, hv.HV_F64) as s:
         with pytest.raises(hv.HVError):
             s.adjoint_backward(np.zeros(2), np.zeros(4))
+
+
+def test_adjoint_matches_fp64_tangent_linear_cpu_run(hv):
+    """The adjoint gradient against the FP64 tangent-linear run on the CPU
+    oracle (oracle/hv_tangent.py, itself pinned to finite differences in
+    tests/test_tangent.py): both differentiate the same discrete map exactly,
+    so they agree far below the finite-difference noise -- within 1e-6 of the
+    largest component, in each of the four directions."""
+    from hv_oracle import RunSpec
+    from hv_tangent import Tangent, skyrme_from_theta
+
+    from hv_b200.adjoint import AdjointRun
+    steps = 24
+    w, parts, theta = _setup(hv, steps)
+    wts = np.random.default_rng(5).standard_normal(steps)
+    run = AdjointRun(w, parts, steps, checkpoint_every=8)
+    try:
+        d_gpu = run.forward(theta)
+        g_adj = run.backward(wts)
+    finally:
+        run.close()
+    A, B, C, g = skyrme_from_theta(theta)
+    spec = RunSpec(z=w.Z, n=w.N, part_per_nucleon=w.ppn, sigma_r=w.sigma_r, dt=w.dt, t_exc=w.t_exc,
+                   eta_exc=w.eta, A=A, B=B, C=C, gamma=g, sor_omega=w.sor_omega, sor_tol=w.sor_tol,
+                   sor_criterion=w.sor_criterion, sor_max_iter=w.sor_max_iter)
+    t = Tangent(w.world_tuple(), spec, w.protons, w.neutrons)
+    g_tl = np.zeros(4)
+    for i in range(4):
+        e = np.zeros(4)
+        e[i] = 1.0
+        d_cpu, dD = t.run(*parts, steps, theta, e)
+        g_tl[i] = wts @ dD
+    assert np.max(np.abs(d_cpu - d_gpu)) <= 1e-9 * np.abs(d_cpu).max()
+    assert np.all(np.abs(g_adj - g_tl) <= 1e-6 * np.abs(g_tl).max()), (g_adj, g_tl)
