@@ -301,6 +301,17 @@ bool slots_permuted(hv_ctx *c) { return c->permuted; }
 }  // namespace
 
 hv_status plain_step_f64(hv_ctx *c, hv_observables *row) { return plain_step<double>(c, row); }
+
+hv_status allow_max_dynamic_smem(const void *kern, int device) {
+    cudaFuncAttributes fa;
+    HV_CUDA(cudaFuncGetAttributes(&fa, kern));
+    int optin = 0;
+    HV_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    if (fa.maxDynamicSharedSizeBytes < dyn)
+        HV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    return HV_OK;
+}
 hv_status plain_fields_f64(hv_ctx *c, int *sor_its) { return fields_and_gather<double>(c, sor_its); }
 
 }  // namespace hv

@@ -90,6 +90,7 @@ struct SorFast {
     size_t smem = 0;
     int nz2 = 0;               // (nz + 1) / 2: length of one colour half-line
     bool src_smem = false;     // the residual source also lives in shared memory
+    bool tables = false;       // shared memory also holds the tagged sweeps' row tables
     void *delta = nullptr;     // SOR correction, colour-split layout
     void *src = nullptr;       // residual source, colour-split layout
     double *partials = nullptr;
@@ -213,6 +214,35 @@ hv_status fused_prepare(hv_ctx *c);
 hv_status fused_release(hv_ctx *c);
 hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs);
 void fused_invalidate(hv_ctx *c);
+
+// Several float SOR solves run by one cooperative launch (k_sor_fast.cu).
+struct SorWave {
+    int nblocks = 0;                 // all instances' blocks
+    size_t smem = 0;                 // the largest instance's dynamic shared memory
+    const void *kern = nullptr;
+    void *args = nullptr;            // device: the instances' kernel arguments
+    int *binst = nullptr, *bfirst = nullptr;  // device: block -> instance, instance -> first block
+    std::vector<hv_ctx *> ctx;
+};
+hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std::vector<const float *> &rho,
+                         const std::vector<int *> &ctl, const std::vector<int *> &its_ring, int ring);
+hv_status sor_wave_launch(const SorWave &w, cudaStream_t st);
+void sor_wave_release(SorWave &w);
+// Lets a kernel launch with up to the device's opt-in shared memory per block.
+// The attribute belongs to the function, which every context shares, so it is
+// raised to the maximum once rather than set to one plan's need.
+hv_status allow_max_dynamic_smem(const void *kern, int device);
+// re-plans a context's fused SOR with at most max_blocks blocks (0: all SMs)
+hv_status sor_fast_replan(hv_ctx *c, int max_blocks);
+
+// parts of fused float steps for the batched driver (k_fused.cu)
+hv_status fused_batch_ready(hv_ctx *c);
+hv_status fused_batch_begin(hv_ctx *c, int n_steps, int *exc);
+hv_status fused_batch_phase_a(hv_ctx *c, cudaStream_t s);
+hv_status fused_batch_phase_c(hv_ctx *c, cudaStream_t s);
+hv_status fused_batch_rows(hv_ctx *c, cudaStream_t s, int s0, int k, hv_observables *obs);
+hv_status fused_batch_end(hv_ctx *c, int n_steps, int exc);
+void fused_batch_sor_inputs(hv_ctx *c, const float **rho, int **ctl, int **its_ring, int *ring);
 void adjoint_release(hv_ctx *c);
 // one plain FP64 step / the field solve and gather of the current positions
 hv_status plain_step_f64(hv_ctx *c, hv_observables *row);

@@ -344,8 +344,11 @@ void prof_collect(hv_ctx *c) {
 }
 
 // Enqueues one fused step on the context stream (graph-capturable).
+// A step in three parts, so that several contexts can interleave them (the
+// batched driver): A = particle step, smoothing, Skyrme; the SOR; C = forces
+// and the step counter.
 template <typename T>
-hv_status enqueue_step(hv_ctx *c) {
+hv_status enqueue_phase_a(hv_ctx *c) {
     State<T> &s = st<T>(c);
     Fused &f = c->fused;
     const Geom &g = c->geom;
@@ -392,10 +395,15 @@ hv_status enqueue_step(hv_ctx *c) {
                                                                 s.U);
     }
     HV_CUDA(cudaGetLastError());
-    {
-        ProfScope ps(c, HV_K_SOR);
-        HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, f.sor_its, kRing));
-    }
+    return HV_OK;
+}
+
+template <typename T>
+hv_status enqueue_phase_c(hv_ctx *c) {
+    State<T> &s = st<T>(c);
+    Fused &f = c->fused;
+    const Geom &g = c->geom;
+    int *ctl = ctl_of(c);
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
     {
@@ -407,6 +415,16 @@ hv_status enqueue_step(hv_ctx *c) {
     k_advance<<<1, 1, 0, c->stream>>>(ctl);
     HV_CUDA(cudaGetLastError());
     return HV_OK;
+}
+
+template <typename T>
+hv_status enqueue_step(hv_ctx *c) {
+    HV_TRY(enqueue_phase_a<T>(c));
+    {
+        ProfScope ps(c, HV_K_SOR);
+        HV_TRY(sor_fast_launch<T>(c, st<T>(c).rho, ctl_of(c), c->fused.sor_its, kRing));
+    }
+    return enqueue_phase_c<T>(c);
 }
 
 // The initial field solve of cpu_simulate (src/hyper_vlasov.cpp:53-62) on the
@@ -469,8 +487,10 @@ hv_status enqueue_steps(hv_ctx *c, int n) {
     return HV_OK;
 }
 
+// Before n_steps fused steps: the fused state brought up to date with the plain
+// buffers and the control words set; returns the excitation step (or -1).
 template <typename T>
-hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
+hv_status run_begin(hv_ctx *c, int n_steps, int *exc_out) {
     State<T> &s = st<T>(c);
     Fused &f = c->fused;
     const Geom &g = c->geom;
@@ -496,7 +516,58 @@ hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
     int h_ctl[5] = {c->step_index, f.m_hint, 0, exc, 0};
     HV_CUDA(cudaMemcpyAsync(ctl + CTL_STEP, &h_ctl[0], sizeof(int), cudaMemcpyHostToDevice, c->stream));
     HV_CUDA(cudaMemcpyAsync(ctl + CTL_EXCITE, &h_ctl[3], sizeof(int) * 2, cudaMemcpyHostToDevice, c->stream));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    *exc_out = exc;
+    return HV_OK;
+}
 
+// After k steps that started at step s0: their observable rows (obs[0..k)),
+// and the SOR status; synchronous.
+template <typename T>
+hv_status run_rows(hv_ctx *c, int s0, int k, hv_observables *obs) {
+    Fused &f = c->fused;
+    std::vector<double> rows((size_t)k * 8);
+    std::vector<int> its(kRing);
+    k_reduce_rows<<<k, 32, 0, c->stream>>>(f.obs_partials, f.obs_blocks, s0, k, f.obs_rows_dev);
+    HV_CUDA(cudaGetLastError());
+    HV_CUDA(cudaMemcpyAsync(rows.data(), f.obs_rows_dev, sizeof(double) * 8 * k, cudaMemcpyDeviceToHost, c->stream));
+    HV_CUDA(cudaMemcpyAsync(its.data(), f.sor_its, sizeof(int) * kRing, cudaMemcpyDeviceToHost, c->stream));
+    int status[3] = {0, 0, 0};
+    HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    prof_collect(c);
+    if (status[0]) {
+        set_last_error("SOR: a bounded device-side wait timed out");
+        return HV_ERR_TIMEOUT;
+    }
+    if (obs) {
+        const double zz = c->params.z, nn = c->params.n;
+        for (int r = 0; r < k; r++) {
+            hv_observables &o = obs[r];
+            const double *v = &rows[(size_t)r * 8];
+            std::memset(&o, 0, sizeof(o));
+            o.t = (double)(T(s0 + r) * T(c->params.dt));
+            o.zcm_p = v[0] / (double)c->protons;
+            o.zcm_n = v[1] / (double)c->neutrons;
+            o.rms_p = std::sqrt(v[2] / v[4]);
+            o.rms_n = std::sqrt(v[3] / v[5]);
+            o.dipole = (nn * zz) / (nn + zz) * (o.zcm_p - o.zcm_n);
+            int it = its[(s0 + r) % kRing];
+            o.sor_iterations = it < 0 ? -it : it;
+            if (it < 0) o.flags |= HV_OBS_SOR_NOT_CONVERGED;
+        }
+    }
+    return HV_OK;
+}
+
+template <typename T>
+hv_status run_end(hv_ctx *c, int n_steps, int exc);
+
+template <typename T>
+hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
+    Fused &f = c->fused;
+    int exc = -1;
+    HV_TRY(run_begin<T>(c, n_steps, &exc));
     const int chunk = c->fast.graph_steps > 0 ? std::min(c->fast.graph_steps, kRing) : std::min(8, kRing);
     int done = 0;
     std::vector<double> rows;
@@ -531,44 +602,22 @@ hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
             }
         }
         if (!launched) HV_TRY(enqueue_steps<T>(c, k));
-        // observables of the k steps
-        const int s0 = c->step_index + done;
-        k_reduce_rows<<<k, 32, 0, c->stream>>>(f.obs_partials, f.obs_blocks, s0, k, f.obs_rows_dev);
-        HV_CUDA(cudaGetLastError());
-        rows.resize((size_t)k * 8);
-        HV_CUDA(cudaMemcpyAsync(rows.data(), f.obs_rows_dev, sizeof(double) * 8 * k, cudaMemcpyDeviceToHost, c->stream));
-        HV_CUDA(cudaMemcpyAsync(its.data(), f.sor_its, sizeof(int) * kRing, cudaMemcpyDeviceToHost, c->stream));
-        int status[3] = {0, 0, 0};
-        HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
-        HV_CUDA(cudaStreamSynchronize(c->stream));
-        prof_collect(c);
-        if (status[0]) {
-            set_last_error("SOR: a bounded device-side wait timed out");
-            return HV_ERR_TIMEOUT;
-        }
-        if (obs) {
-            const double zz = c->params.z, nn = c->params.n;
-            for (int r = 0; r < k; r++) {
-                hv_observables &o = obs[done + r];
-                const double *v = &rows[(size_t)r * 8];
-                std::memset(&o, 0, sizeof(o));
-                o.t = (double)(T(s0 + r) * T(c->params.dt));
-                o.zcm_p = v[0] / (double)c->protons;
-                o.zcm_n = v[1] / (double)c->neutrons;
-                o.rms_p = std::sqrt(v[2] / v[4]);
-                o.rms_n = std::sqrt(v[3] / v[5]);
-                o.dipole = (nn * zz) / (nn + zz) * (o.zcm_p - o.zcm_n);
-                int it = its[(s0 + r) % kRing];
-                o.sor_iterations = it < 0 ? -it : it;
-                if (it < 0) o.flags |= HV_OBS_SOR_NOT_CONVERGED;
-            }
-        }
+        HV_TRY(run_rows<T>(c, c->step_index + done, k, obs ? obs + done : nullptr));
         done += k;
     }
+    return run_end<T>(c, n_steps, exc);
+}
+
+// After a run of n_steps: step counter, excitation flag, the closing kick/2
+// and the plain-path view of the fields.
+template <typename T>
+hv_status run_end(hv_ctx *c, int n_steps, int exc) {
+    Fused &f = c->fused;
+    const Geom &g = c->geom;
+    int *ctl = ctl_of(c);
     if (exc >= 0) c->excited = true;
     c->step_index += n_steps;
-    // closing kick/2 and the plain-path view of the fields
-    State<T> &S = s;
+    State<T> &S = st<T>(c);
     if (c->total > 0)
         k_close_kick<T><<<nblk(c->total, 256), 256, 0, c->stream>>>(g, c->protons, c->total, S.x, S.y, S.z, S.kx, S.ky,
                                                                     S.kz, S.fx, S.fy, S.fz,
@@ -643,6 +692,45 @@ hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs) {
         return st;
     }
     return c->prec == HV_F64 ? run_typed<double>(c, n_steps, obs) : run_typed<float>(c, n_steps, obs);
+}
+
+// ---- batched driver support (batch.cu): float contexts, parts of a step on a
+// caller's stream
+namespace {
+struct StreamSwap {
+    hv_ctx *c;
+    cudaStream_t saved;
+    StreamSwap(hv_ctx *c_, cudaStream_t s) : c(c_), saved(c_->stream) { c->stream = s; }
+    ~StreamSwap() { c->stream = saved; }
+};
+}  // namespace
+
+hv_status fused_batch_ready(hv_ctx *c) {
+    if (c->prec != HV_F32) return HV_ERR_UNSUPPORTED;
+    if (!c->fields_valid) HV_TRY(fused_initial_solve(c));
+    hv_status st = fused_prepare(c);
+    if (st != HV_OK) fused_release(c);
+    return st;
+}
+hv_status fused_batch_begin(hv_ctx *c, int n_steps, int *exc) { return run_begin<float>(c, n_steps, exc); }
+hv_status fused_batch_phase_a(hv_ctx *c, cudaStream_t s) {
+    StreamSwap sw(c, s);
+    return enqueue_phase_a<float>(c);
+}
+hv_status fused_batch_phase_c(hv_ctx *c, cudaStream_t s) {
+    StreamSwap sw(c, s);
+    return enqueue_phase_c<float>(c);
+}
+hv_status fused_batch_rows(hv_ctx *c, cudaStream_t s, int s0, int k, hv_observables *obs) {
+    StreamSwap sw(c, s);
+    return run_rows<float>(c, s0, k, obs);
+}
+hv_status fused_batch_end(hv_ctx *c, int n_steps, int exc) { return run_end<float>(c, n_steps, exc); }
+void fused_batch_sor_inputs(hv_ctx *c, const float **rho, int **ctl, int **its_ring, int *ring) {
+    *rho = c->d32.rho;
+    *ctl = ctl_of(c);
+    *its_ring = c->fused.sor_its;
+    *ring = kRing;
 }
 
 // Marks the fused copies stale after the plain path or an upload changed the state.

@@ -254,7 +254,7 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     const int rows = kMBY + 2 * R, cols = kMBK + 2 * R;
     f.per = R;
     f.smem = sizeof(float) * ((size_t)rows * cols + (size_t)(R + 1) * rows * kMBK + (size_t)(2 * A + 1) * kMThreads);
-    HV_CUDA(cudaFuncSetAttribute(march_kernel(R), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
+    HV_TRY(allow_max_dynamic_smem(march_kernel(R), c->device));
     f.A = A;
     f.B = B;
     f.W = W;

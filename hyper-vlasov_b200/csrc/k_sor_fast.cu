@@ -40,6 +40,8 @@
 // corrections being zero.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "hv_internal.h"
 
@@ -76,6 +78,10 @@ struct SorArgs {
     int *ctl;               // [0] step counter, [1] m hint, [2] previous-phi valid
     int *its_ring;          // per-step iterations, indexed by step % ring
     int ring;
+    // several solves in one launch: block -> instance, first block of an
+    // instance, and the instances' arguments (null for a single solve)
+    const SorArgs *batch;
+    const int *binst, *bfirst;
 };
 
 __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
@@ -692,12 +698,12 @@ __device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block
 // thread, perimeter quads per thread and ghost quads per fetch thread, decoded
 // once per solve; kInner = 0: the generic tagged sweep.
 template <typename T, typename S, bool kTag, int kInner, int kFace, int kGhost>
-__global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
+__device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double s_tot[3];
     __shared__ int s_m;
 
-    const int b = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    const int tid = threadIdx.x, nth = blockDim.x;
     const int bx = b % a.bxn, by = b / a.bxn;
     const int x0 = 1 + bx * a.P, x1 = min(x0 + a.P, a.nx - 1);
     const int y0 = by * a.R, y1 = min(y0 + a.R, a.ny);
@@ -1039,16 +1045,36 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> a) {
     }
 }
 
+// One solve (kBatch false: the arguments are the kernel parameter), or several
+// independent solves in one cooperative launch (kBatch: block blockIdx.x works
+// on instance binst[blockIdx.x], as its block blockIdx.x - bfirst[instance];
+// barriers, residual sums and the exchange stay within an instance, and an
+// instance that has converged leaves while the others go on).
+template <typename T, typename S, bool kTag, int kInner, int kFace, int kGhost, bool kBatch = false>
+__global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> p) {
+    if constexpr (kBatch) {
+        __shared__ SorArgs<T, S> s_inst;
+        const int inst = p.binst[blockIdx.x];
+        if (threadIdx.x == 0) s_inst = p.batch[inst];
+        __syncthreads();
+        sor_body<T, S, kTag, kInner, kFace, kGhost>(s_inst, (int)blockIdx.x - p.bfirst[inst]);
+    } else {
+        sor_body<T, S, kTag, kInner, kFace, kGhost>(p, (int)blockIdx.x);
+    }
+}
+
 }  // namespace
 
 template <typename S>
-static hv_status plan_for(hv_ctx *c) {
+static hv_status plan_for(hv_ctx *c, int max_blocks) {
     SorFast &f = c->fused.sor;
     const Geom &g = c->geom;
     cudaDeviceProp prop;
     HV_CUDA(cudaGetDeviceProperties(&prop, c->device));
     const size_t static_smem = 2048;
     const size_t limit = prop.sharedMemPerBlockOptin > static_smem ? prop.sharedMemPerBlockOptin - static_smem : 0;
+    // blocks of one solve: all SMs, or fewer when the solve shares a launch
+    const long long cap = max_blocks > 0 ? std::min(max_blocks, prop.multiProcessorCount) : prop.multiProcessorCount;
     const int nz2 = (g.nz + 1) / 2;
     const int interior = g.nx - 2;
     f.ok = false;
@@ -1065,7 +1091,7 @@ static hv_status plan_for(hv_ctx *c) {
                 const size_t smem = sizeof(S) * own * 2 + Staged::bytes(P, R, nz2);
                 if (smem > limit) break;
                 const long long bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
-                if (bxn * byn > prop.multiProcessorCount) continue;
+                if (bxn * byn > cap) continue;
                 const long long key[3] = {((long long)P * R * nq + kSorThreads - 1) / kSorThreads,
                                           bxn * byn * (P + R), bxn * byn};
                 if (f.ok && !(key[0] < best[0] || (key[0] == best[0] && (key[1] < best[1] ||
@@ -1081,6 +1107,7 @@ static hv_status plan_for(hv_ctx *c) {
                 f.nblocks = (int)(bxn * byn);
                 f.smem = smem;
                 f.src_smem = true;
+                f.tables = true;
                 f.ok = true;
             }
     }
@@ -1094,7 +1121,7 @@ static hv_status plan_for(hv_ctx *c) {
                 const size_t smem = sizeof(S) * own * (with_src ? 2 : 1);
                 if (smem > limit) break;
                 const int bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
-                if ((long long)bxn * byn > prop.multiProcessorCount) continue;
+                if ((long long)bxn * byn > cap) continue;
                 f.P = P;
                 f.R = R;
                 f.bx = bxn;
@@ -1102,6 +1129,7 @@ static hv_status plan_for(hv_ctx *c) {
                 f.nblocks = bxn * byn;
                 f.smem = smem;
                 f.src_smem = with_src;
+                f.tables = false;
                 f.ok = true;
                 break;
             }
@@ -1118,7 +1146,7 @@ static hv_status plan_for(hv_ctx *c) {
     }
     for (const void *kern : kerns) {
         if (!kern) continue;
-        HV_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem));
+        HV_TRY(allow_max_dynamic_smem(kern, c->device));
         int per_sm = 0;
         HV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, f.threads, f.smem));
         if (per_sm < 1 || (long long)per_sm * prop.multiProcessorCount < f.nblocks) {
@@ -1144,8 +1172,9 @@ static hv_status plan_for(hv_ctx *c) {
 }
 
 hv_status sor_fast_plan(hv_ctx *c) {
-    return c->prec == HV_F64 ? plan_for<double>(c) : plan_for<float>(c);
+    return c->prec == HV_F64 ? plan_for<double>(c, 0) : plan_for<float>(c, 0);
 }
+
 
 void sor_fast_release(hv_ctx *c) {
     SorFast &f = c->fused.sor;
@@ -1155,15 +1184,21 @@ void sor_fast_release(hv_ctx *c) {
     f = SorFast();
 }
 
+hv_status sor_fast_replan(hv_ctx *c, int max_blocks) {
+    sor_fast_release(c);
+    return c->prec == HV_F64 ? plan_for<double>(c, max_blocks) : plan_for<float>(c, max_blocks);
+}
+
+// The arguments of one solve and its kernel form: 0 phase counters, 1 the
+// generic tagged sweep, 2 and 3 the staged sweep for at most (1, 1, 2) and
+// (2, 1, 3) inner / perimeter / ghost quads per thread.
 template <typename T>
-hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring) {
+static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, SorArgs<T, T> &a) {
     using S = T;
     SorFast &f = c->fused.sor;
     const Geom &g = c->geom;
     const hv_sor_params &sp = c->params.sor;
-    HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
-    HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, c->stream));
-    SorArgs<T, S> a;
+    std::memset(&a, 0, sizeof(a));
     a.nx = g.nx;
     a.ny = g.ny;
     a.nz = g.nz;
@@ -1209,22 +1244,115 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     a.ctl = ctl;
     a.its_ring = its_ring;
     a.ring = ring;
-    void *args[] = {&a};
-    const void *kern = (const void *)k_sor_fast<T, S, false, 0, 0, 0>;
-    if constexpr (sizeof(S) == 4)
-        if (a.vec4 && c->fast.sor_exchange == HV_SOR_EXCHANGE_AUTO) {
-            // staged sweep when its per-thread quad counts fit an instantiation
-            const long long nq = f.nz2 / 4, P = f.P, R = f.R;
-            const long long inner = std::max(P - 2, 0ll) * std::max(R - 2, 0ll);
-            const long long ni = (inner * nq + f.threads - kGhostThreads - 1) / (f.threads - kGhostThreads);
-            const long long nf = ((P * R - inner) * nq + f.threads - 1) / f.threads;
-            const long long ng = (2 * (P + R) * nq + kGhostThreads - 1) / kGhostThreads;
-            kern = (const void *)k_sor_fast<T, S, true, 0, 0, 0>;
-            if (ni <= 1 && nf <= 1 && ng <= 2) kern = (const void *)k_sor_fast<T, S, true, 1, 1, 2>;
-            else if (ni <= 2 && nf <= 1 && ng <= 3) kern = (const void *)k_sor_fast<T, S, true, 2, 1, 3>;
+    int form = 0;
+    // the tagged sweeps need their row tables in shared memory
+    if (sizeof(S) == 4 && a.vec4 && f.tables && c->fast.sor_exchange == HV_SOR_EXCHANGE_AUTO) {
+        // staged sweep when its per-thread quad counts fit an instantiation
+        const long long nq = f.nz2 / 4, P = f.P, R = f.R;
+        const long long inner = std::max(P - 2, 0ll) * std::max(R - 2, 0ll);
+        const long long ni = (inner * nq + f.threads - kGhostThreads - 1) / (f.threads - kGhostThreads);
+        const long long nf = ((P * R - inner) * nq + f.threads - 1) / f.threads;
+        const long long ng = (2 * (P + R) * nq + kGhostThreads - 1) / kGhostThreads;
+        form = 1;
+        if (ni <= 1 && nf <= 1 && ng <= 2) form = 2;
+        else if (ni <= 2 && nf <= 1 && ng <= 3) form = 3;
+    }
+    return form;
+}
+
+template <typename T, bool kBatch>
+static const void *sor_kernel(int form) {
+    if constexpr (sizeof(T) == 4) {
+        switch (form) {
+        case 1: return (const void *)k_sor_fast<T, T, true, 0, 0, 0, kBatch>;
+        case 2: return (const void *)k_sor_fast<T, T, true, 1, 1, 2, kBatch>;
+        case 3: return (const void *)k_sor_fast<T, T, true, 2, 1, 3, kBatch>;
+        default: break;
         }
-    HV_CUDA(cudaLaunchCooperativeKernel(kern, dim3(f.nblocks), dim3(f.threads), args, f.smem, c->stream));
+    }
+    if constexpr (kBatch) return nullptr;
+    else return (const void *)k_sor_fast<T, T, false, 0, 0, 0>;
+}
+
+template <typename T>
+hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring) {
+    SorFast &f = c->fused.sor;
+    HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
+    HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, c->stream));
+    SorArgs<T, T> a;
+    const int form = sor_fast_args<T>(c, rho, ctl, its_ring, ring, a);
+    void *args[] = {&a};
+    HV_CUDA(cudaLaunchCooperativeKernel(sor_kernel<T, false>(form), dim3(f.nblocks), dim3(f.threads), args, f.smem,
+                                        c->stream));
     return HV_OK;
+}
+
+// ---- several float solves in one cooperative launch ------------------------
+
+hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std::vector<const float *> &rho,
+                         const std::vector<int *> &ctl, const std::vector<int *> &its_ring, int ring) {
+    sor_wave_release(w);
+    const int n = (int)cs.size();
+    std::vector<SorArgs<float, float>> args(n);
+    std::vector<int> binst, bfirst(n);
+    // one kernel form for all: the generic tagged sweep if any instance needs
+    // it, else the staged sweep whose per-thread counts cover every instance
+    bool any1 = false, all2 = true;
+    size_t smem = 0;
+    for (int i = 0; i < n; i++) {
+        hv_ctx *c = cs[i];
+        if (c->prec != HV_F32 || !c->fused.sor.ok) return HV_ERR_UNSUPPORTED;
+        const int fi = sor_fast_args<float>(c, rho[i], ctl[i], its_ring[i], ring, args[i]);
+        if (fi == 0) return HV_ERR_UNSUPPORTED;  // the batched form needs the tagged exchange
+        any1 = any1 || fi == 1;
+        all2 = all2 && fi == 2;
+        bfirst[i] = (int)binst.size();
+        for (int b = 0; b < c->fused.sor.nblocks; b++) binst.push_back(i);
+        smem = std::max(smem, c->fused.sor.smem);
+    }
+    const int form = any1 ? 1 : all2 ? 2 : 3;
+    int dev = 0;
+    HV_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    HV_CUDA(cudaGetDeviceProperties(&prop, dev));
+    w.kern = sor_kernel<float, true>(form);
+    HV_TRY(allow_max_dynamic_smem(w.kern, dev));
+    int per_sm = 0;
+    HV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, w.kern, kSorThreads, smem));
+    if ((long long)per_sm * prop.multiProcessorCount < (long long)binst.size()) return HV_ERR_UNSUPPORTED;
+    HV_CUDA(cudaMalloc(&w.args, sizeof(SorArgs<float, float>) * n));
+    HV_CUDA(cudaMalloc((void **)&w.binst, sizeof(int) * binst.size()));
+    HV_CUDA(cudaMalloc((void **)&w.bfirst, sizeof(int) * n));
+    HV_CUDA(cudaMemcpy(w.args, args.data(), sizeof(SorArgs<float, float>) * n, cudaMemcpyHostToDevice));
+    HV_CUDA(cudaMemcpy(w.binst, binst.data(), sizeof(int) * binst.size(), cudaMemcpyHostToDevice));
+    HV_CUDA(cudaMemcpy(w.bfirst, bfirst.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    w.ctx = cs;
+    w.nblocks = (int)binst.size();
+    w.smem = smem;
+    return HV_OK;
+}
+
+hv_status sor_wave_launch(const SorWave &w, cudaStream_t st) {
+    for (hv_ctx *c : w.ctx) {
+        const SorFast &f = c->fused.sor;
+        HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), st));
+        HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, st));
+    }
+    SorArgs<float, float> p;
+    std::memset(&p, 0, sizeof(p));
+    p.batch = reinterpret_cast<const SorArgs<float, float> *>(w.args);
+    p.binst = w.binst;
+    p.bfirst = w.bfirst;
+    void *args[] = {&p};
+    HV_CUDA(cudaLaunchCooperativeKernel(w.kern, dim3(w.nblocks), dim3(kSorThreads), args, w.smem, st));
+    return HV_OK;
+}
+
+void sor_wave_release(SorWave &w) {
+    if (w.args) cudaFree(w.args);
+    if (w.binst) cudaFree(w.binst);
+    if (w.bfirst) cudaFree(w.bfirst);
+    w = SorWave();
 }
 
 template hv_status sor_fast_launch<float>(hv_ctx *, const float *, int *, int *, int);

@@ -112,6 +112,9 @@ class Workload:
         p.deposit_mode = self.deposit_mode
         return p
 
+    def with_grid(self, n: int):
+        return replace(self, n=n)
+
     def with_reference_sor(self):
         """The reference's hard-wired SOR: omega 1.5, max|dphi| < 1e-4, 512
         iterations (include/physics.hpp:103-104,152)."""
@@ -130,3 +133,32 @@ PB208_2M = Workload("208Pb-2.08M-128^3", Z=82, N=126, ppn=10000, n=128, h=0.25, 
 PB208_20K_128 = Workload("208Pb-20.8k-128^3", Z=82, N=126, ppn=100, n=128, h=0.25, dt=0.2, steps=1000)
 
 WORKLOADS = {w.name: w for w in (CA40_SMALL, PB208_104K, PB208_2M, PB208_20K_128)}
+
+
+# Nuclei of the batched workload: (name, Z, N).
+BATCH_NUCLEI = (("16O", 8, 8), ("40Ca", 20, 20), ("90Zr", 40, 50), ("208Pb", 82, 126))
+
+
+def batch_workloads(n: int = 64, seed: int = 0, steps: int = 500, h: float = 0.5, dt: float = 0.25):
+    """n independent runs: nuclei drawn from 16O, 40Ca, 90Zr, 208Pb; 200-2000
+    test particles per nucleon (log-uniform); cubic grids of 32-96 nodes per
+    axis at h (the smallest of 32, 48, ... 96 that leaves 4 fm around the
+    nucleus, or larger at random); t0 and t3 jittered +-5 % uniform; dipole
+    boosts of 10-40 MeV/c; each run with its own generator seed."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    grids = (32, 48, 64, 80, 96)
+    for i in range(n):
+        name, Z, N = BATCH_NUCLEI[rng.integers(len(BATCH_NUCLEI))]
+        ppn = int(round(math.exp(rng.uniform(math.log(200.0), math.log(2000.0)))))
+        radius = 1.2 * (Z + N) ** (1.0 / 3.0)
+        fits = [g for g in grids if g * h / 2.0 >= radius + 4.0]
+        ng = int(fits[rng.integers(len(fits))])
+        w = Workload(f"{name}-{ppn}x{Z + N}-{ng}^3#{i}", Z=Z, N=N, ppn=ppn, n=ng, h=h, dt=dt, steps=steps,
+                     seed=seed * 1000 + i,
+                     t0=-2645.0 * (1.0 + rng.uniform(-0.05, 0.05)),
+                     t3=15595.0 * (1.0 + rng.uniform(-0.05, 0.05)),
+                     boost_mev=float(rng.uniform(10.0, 40.0)))
+        out.append(w)
+    return out

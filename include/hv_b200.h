@@ -390,6 +390,35 @@ HV_API hv_status hv_adjoint_forward(hv_ctx *ctx, int n_steps, int checkpoint_eve
 HV_API hv_status hv_adjoint_backward(hv_ctx *ctx, const double *dJ_dD, const double theta[4],
                                      double grad_theta[4], double grad_skyrme[4]);
 
+/* ---- batched runs -------------------------------------------------------
+ * No counterpart in the reference, which runs one nucleus per process: many
+ * independent runs (own nucleus, test particles, grid and parameters, each an
+ * HV_F32 context on the same device, particles uploaded) advanced together on
+ * the fused path.  Per step every instance's particle step, smoothing and
+ * Skyrme potential run as parallel branches, the Coulomb solves as a few
+ * cooperative launches that each solve several instances ("waves"), then the
+ * forces; chunks of steps are replayed from one CUDA graph.  Each instance's
+ * observables are those of hv_run(HV_PATH_FUSED) on its own, up to float
+ * rounding.  The contexts stay owned by the caller and must outlive the batch;
+ * while it exists they are advanced only through it.
+ *
+ * hv_batch_create solves each instance's initial fields if needed and plans
+ * with each instance's own SOR plan.  hv_batch_plan re-plans every instance's
+ * SOR with at most sor_max_blocks blocks (0: the instance's own plan; an
+ * instance whose grid needs more blocks' shared memory gets twice the cap, and
+ * so on) and packs the solves into waves of at most one block per SM.  hv_batch_autotune
+ * times trial_steps batched steps (plus one) for each candidate cap and keeps
+ * the fastest; the trial steps advance every run.  hv_batch_run advances all
+ * instances n_steps and writes n_steps observable rows per instance,
+ * instance-major (obs[i * n_steps + s]; may be NULL). */
+typedef struct hv_batch hv_batch;
+HV_API hv_status hv_batch_create(int n_instances, hv_ctx *const *ctxs, hv_batch **out);
+HV_API hv_status hv_batch_destroy(hv_batch *batch);
+HV_API hv_status hv_batch_plan(hv_batch *batch, int sor_max_blocks);
+HV_API hv_status hv_batch_autotune(hv_batch *batch, int trial_steps, int *chosen_cap);
+HV_API hv_status hv_batch_run(hv_batch *batch, int n_steps, hv_observables *obs);
+HV_API int hv_batch_waves(const hv_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif

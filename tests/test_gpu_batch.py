@@ -1,0 +1,86 @@
+"""GPU: batched runs (hv_batch_*) against the same instances run one by one.
+
+Six instances drawn like the 64-run batched workload (nuclei 16O..208Pb,
+grids 32^3..96^3 at h = 0.5 fm, jittered Skyrme parameters and boosts), with
+at most 100 test particles per nucleon to keep the test short.  Tolerance:
+D(t) of every instance within 1e-4 of its largest |D| against the instance's
+own fused run (the float atomic deposit makes two runs of one instance differ
+at ~1e-6), SOR iteration counts within one residual check (256)."""
+from __future__ import annotations
+
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _instances(hv, n=6, seed=7):
+    from hv_b200.workloads import batch_workloads
+    return [replace(w, ppn=min(w.ppn, 100)) for w in batch_workloads(n, seed=seed)]
+
+
+def _sessions(hv, ws):
+    out = []
+    for w in ws:
+        s = hv.Session.from_workload(w, hv.HV_F32)
+        s.upload_particles(*hv.workload_particles(w, np.float32))
+        out.append(s)
+    return out
+
+
+@pytest.mark.parametrize("cap", [0, 8])
+def test_batch_matches_individual_runs(hv, cap):
+    from hv_b200.batch import Batch
+    ws = _instances(hv)
+    steps = 16
+    alone = []
+    for s in _sessions(hv, ws):
+        with s:
+            alone.append(s.run(steps, hv.HV_PATH_FUSED))
+    sess = _sessions(hv, ws)
+    try:
+        with Batch(sess) as b:
+            b.plan(cap)
+            assert b.waves() >= 1
+            obs = b.run(steps)
+    finally:
+        for s in sess:
+            s.close()
+    for i, a in enumerate(alone):
+        d = np.abs(a["dipole"]).max()
+        assert d > 0
+        assert np.max(np.abs(obs[i]["dipole"] - a["dipole"])) <= 1e-4 * d, ws[i].name
+        assert np.all(np.abs(obs[i]["sor_iterations"] - a["sor_iterations"]) <= 256)
+        assert not np.any(obs[i]["flags"] & 1)
+        assert np.allclose(obs[i]["t"], a["t"])
+
+
+def test_batch_autotune_and_continued_runs(hv):
+    """The autotuner picks a cap among its candidates; runs continue across
+    calls (step counters and time advance per instance)."""
+    from hv_b200.batch import Batch
+    ws = _instances(hv, n=4, seed=11)
+    sess = _sessions(hv, ws)
+    try:
+        with Batch(sess) as b:
+            cap = b.autotune(2)
+            assert cap in (0, 64, 32, 16, 8, 4)
+            o1 = b.run(8)
+            o2 = b.run(9)
+    finally:
+        for s in sess:
+            s.close()
+    for i, w in enumerate(ws):
+        # autotune ran 1 + 2 steps per candidate before o1
+        assert np.isclose(o2[i]["t"][0] - o1[i]["t"][0], 8 * w.dt)
+        assert np.all(np.isfinite(o2[i]["dipole"]))
+
+
+def test_batch_rejects_double_contexts(hv):
+    from hv_b200.batch import Batch
+    w = hv.CA40_SMALL
+    with hv.Session.from_workload(w, hv.HV_F64) as s:
+        with pytest.raises(hv.HVError):
+            Batch([s])
