@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--cpu-steps", type=int, default=2, help=argparse.SUPPRESS)
@@ -289,6 +291,60 @@ def adjoint_cost(args, local):
             "grad_t0_t3_sigma_asym": [float(v) for v in grad], "timing": "host wall time"}
 
 
+# ---------------------------------------------------------------- batched
+def batched(args, local):
+    """The batched form: 64 independent runs (16O..208Pb, 200-2000 test
+    particles per nucleon, 32^3-96^3 at h = 0.5 fm, jittered Skyrme
+    parameters and boosts) advanced together by hv_batch_run after the
+    autotuner chose the SOR block cap; against the same instances stepped one
+    after another by their own fused runs.  Host wall time around the calls
+    (each synchronises at its end)."""
+    import numpy as np
+
+    import hv_b200 as hv
+    from hv_b200.batch import Batch
+    from hv_b200.workloads import batch_workloads
+    ws = batch_workloads(64, seed=0)
+    K = args.batch_steps
+    parts = [hv.workload_particles(w, np.float32) for w in ws]
+    sess = []
+    try:
+        for w, p in zip(ws, parts):
+            s = hv.Session.from_workload(w, hv.HV_F32, device=local)
+            s.upload_particles(*p)
+            sess.append(s)
+        t0 = time.perf_counter()
+        with Batch(sess) as b:
+            setup = time.perf_counter() - t0
+            cap = b.autotune(2)
+            b.run(3)
+            t0 = time.perf_counter()
+            obs = b.run(K)
+            el = time.perf_counter() - t0
+            waves = b.waves()
+        # the same instances one after another, each on its own fused path
+        ks = 8
+        for s in sess:
+            s.run(2, hv.HV_PATH_FUSED)
+        t0 = time.perf_counter()
+        for s in sess:
+            s.run(ks, hv.HV_PATH_FUSED)
+        seq = time.perf_counter() - t0
+    finally:
+        for s in sess:
+            s.close()
+    N = sum(w.particles for w in ws)
+    value = N * K / el
+    return {"value": value, "unit": UNIT, "instances": len(ws), "particles": N,
+            "grid_nodes": sum(w.G for w in ws), "steps": K, "ms_per_step": 1e3 * el / K,
+            "sor_waves": waves, "autotuned_sor_block_cap": cap, "setup_s": setup,
+            "sor_iterations_per_step_mean": float(obs["sor_iterations"].mean()),
+            "sequential_value": N * ks / seq, "speedup_over_sequential": value / (N * ks / seq),
+            "workload": "64 runs: 16O/40Ca/90Zr/208Pb, 200-2000 tp/nucleon log-uniform, 32^3-96^3 at h 0.5 fm, "
+                        "t0 and t3 +-5 %, boosts 10-40 MeV/c, dt 0.25 fm/c, FP32 fused",
+            "timing": "host wall time around hv_batch_run"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def our_arm(args, world, rank, local):
     import numpy as np
@@ -419,6 +475,8 @@ def our_arm(args, world, rank, local):
 
     if not args.no_adjoint and rank == 0:
         line["adjoint"] = adjoint_cost(args, local)
+    if not args.no_batch and rank == 0:
+        line["batched"] = batched(args, local)
 
     if not args.no_cpu and rank == 0 and world == 1:
         try:
