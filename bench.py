@@ -292,19 +292,25 @@ def adjoint_cost(args, local):
 
 
 # ---------------------------------------------------------------- batched
-def batched(args, local):
+def batched(args, local, world=1, rank=0):
     """The batched form: 64 independent runs (16O..208Pb, 200-2000 test
     particles per nucleon, 32^3-96^3 at h = 0.5 fm, jittered Skyrme
     parameters and boosts) advanced together by hv_batch_run after the
-    autotuner chose the SOR block cap; against the same instances stepped one
-    after another by their own fused runs.  Host wall time around the calls
-    (each synchronises at its end)."""
+    autotuner chose the SOR block cap; on one GPU, against the same instances
+    stepped one after another by their own fused runs.  With N ranks every
+    rank takes the runs that longest-processing-time-first assigns it by
+    estimated cost (no per-step collective), the timed region is bracketed by
+    barriers and maxed over ranks, and the D(t) series are gathered at the
+    end.  Host wall time around the calls (each synchronises at its end)."""
     import numpy as np
 
     import hv_b200 as hv
+    from hv_b200 import replicas
     from hv_b200.batch import Batch
     from hv_b200.workloads import batch_workloads
-    ws = batch_workloads(64, seed=0)
+    all_ws = batch_workloads(64, seed=0)
+    mine = replicas.assign_runs([replicas.run_cost(w.particles, w.G) for w in all_ws], world)[rank]
+    ws = [all_ws[i] for i in mine]
     K = args.batch_steps
     parts = [hv.workload_particles(w, np.float32) for w in ws]
     sess = []
@@ -318,31 +324,40 @@ def batched(args, local):
             setup = time.perf_counter() - t0
             cap = b.autotune(2)
             b.run(3)
+            barrier(world)
             t0 = time.perf_counter()
             obs = b.run(K)
             el = time.perf_counter() - t0
+            barrier(world)
             waves = b.waves()
-        # the same instances one after another, each on its own fused path
-        ks = 8
-        for s in sess:
-            s.run(2, hv.HV_PATH_FUSED)
-        t0 = time.perf_counter()
-        for s in sess:
-            s.run(ks, hv.HV_PATH_FUSED)
-        seq = time.perf_counter() - t0
+        seq = None
+        if world == 1:  # the same instances one after another, each on its own fused path
+            ks = 8
+            for s in sess:
+                s.run(2, hv.HV_PATH_FUSED)
+            t0 = time.perf_counter()
+            for s in sess:
+                s.run(ks, hv.HV_PATH_FUSED)
+            seq = time.perf_counter() - t0
     finally:
         for s in sess:
             s.close()
-    N = sum(w.particles for w in ws)
+    el = max_over_ranks(world, el)
+    series = replicas.gather_series({i: obs[j]["dipole"].tolist() for j, i in enumerate(mine)}, world)
+    N = sum(w.particles for w in all_ws)
     value = N * K / el
-    return {"value": value, "unit": UNIT, "instances": len(ws), "particles": N,
-            "grid_nodes": sum(w.G for w in ws), "steps": K, "ms_per_step": 1e3 * el / K,
-            "sor_waves": waves, "autotuned_sor_block_cap": cap, "setup_s": setup,
-            "sor_iterations_per_step_mean": float(obs["sor_iterations"].mean()),
-            "sequential_value": N * ks / seq, "speedup_over_sequential": value / (N * ks / seq),
+    out = {"value": value, "unit": UNIT, "instances": len(all_ws), "particles": N, "n_gpus": world,
+           "grid_nodes": sum(w.G for w in all_ws), "steps": K, "ms_per_step": 1e3 * el / K,
+           "sor_waves_rank0": waves, "autotuned_sor_block_cap_rank0": cap, "setup_s": setup,
+           "sor_iterations_per_step_mean_rank0": float(obs["sor_iterations"].mean()),
+           "dipole_series_gathered": len(series)}
+    if seq is not None:
+        out.update({"sequential_value": N * ks / seq, "speedup_over_sequential": value / (N * ks / seq)})
+    out.update({
             "workload": "64 runs: 16O/40Ca/90Zr/208Pb, 200-2000 tp/nucleon log-uniform, 32^3-96^3 at h 0.5 fm, "
                         "t0 and t3 +-5 %, boosts 10-40 MeV/c, dt 0.25 fm/c, FP32 fused",
-            "timing": "host wall time around hv_batch_run"}
+            "timing": "host wall time around hv_batch_run, max over ranks"})
+    return out
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -475,8 +490,10 @@ def our_arm(args, world, rank, local):
 
     if not args.no_adjoint and rank == 0:
         line["adjoint"] = adjoint_cost(args, local)
-    if not args.no_batch and rank == 0:
-        line["batched"] = batched(args, local)
+    if not args.no_batch:
+        bl = batched(args, local, world, rank)  # every rank takes part (its share of the runs)
+        if rank == 0:
+            line["batched"] = bl
 
     if not args.no_cpu and rank == 0 and world == 1:
         try:
