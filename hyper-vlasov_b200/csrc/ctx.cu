@@ -302,6 +302,31 @@ bool slots_permuted(hv_ctx *c) { return c->permuted; }
 
 hv_status plain_step_f64(hv_ctx *c, hv_observables *row) { return plain_step<double>(c, row); }
 
+namespace {
+template <typename T>
+hv_status download_slots_t(hv_ctx *c, const T *d, T *host) {
+    const size_t bytes = sizeof(T) * c->total;
+    if (slots_permuted(c)) {
+        T *stage = nullptr;
+        HV_CUDA(cudaMallocAsync((void **)&stage, bytes, c->stream));
+        k_unpermute<T><<<div_up(c->total, 256), 256, 0, c->stream>>>(c->total, c->perm, d, stage);
+        HV_CUDA(cudaGetLastError());
+        HV_CUDA(cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+        HV_CUDA(cudaFreeAsync(stage, c->stream));
+    } else {
+        HV_CUDA(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+    }
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    return HV_OK;
+}
+}  // namespace
+
+hv_status download_slots(hv_ctx *c, const void *dev, void *host) {
+    if (c->total == 0) return HV_OK;
+    return c->prec == HV_F64 ? download_slots_t<double>(c, (const double *)dev, (double *)host)
+                             : download_slots_t<float>(c, (const float *)dev, (float *)host);
+}
+
 hv_status allow_max_dynamic_smem(const void *kern, int device) {
     cudaFuncAttributes fa;
     HV_CUDA(cudaFuncGetAttributes(&fa, kern));

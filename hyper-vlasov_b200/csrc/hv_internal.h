@@ -232,6 +232,16 @@ void sor_wave_release(SorWave &w);
 // The attribute belongs to the function, which every context shares, so it is
 // raised to the maximum once rather than set to one plan's need.
 hv_status allow_max_dynamic_smem(const void *kern, int device);
+// the context's particle and field buffers of type T (ctx.cu)
+template <typename T>
+State<T> &state(hv_ctx *c);
+template <>
+State<double> &state<double>(hv_ctx *c);
+template <>
+State<float> &state<float>(hv_ctx *c);
+// a per-particle device array in slot order to a host array in the caller's
+// particle order (element type of the context's precision; synchronous)
+hv_status download_slots(hv_ctx *c, const void *dev, void *host);
 // re-plans a context's fused SOR with at most max_blocks blocks (0: all SMs)
 hv_status sor_fast_replan(hv_ctx *c, int max_blocks);
 

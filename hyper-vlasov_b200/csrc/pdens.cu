@@ -1,0 +1,227 @@
+// Per-particle densities of the initialisation, compute_particle_densities
+// (include/tools.hpp:170-203), with cell lists.
+//
+// The reference sums, for every particle, exp(-d^2 / (2 sigma_r^2)) over all
+// particles within d^2 <= 16 sigma_r^2 -- an O(N^2) double loop.  Here the
+// particles are binned into cubic cells of edge 4 sigma_r over their bounding
+// box and sorted by cell (CUB radix sort), so every partner of a particle lies
+// in the 27 cells around its own.  One thread per particle, in sorted order:
+// the threads of a warp share a cell, hence scan the same neighbour cells, and
+// their partner loads are broadcasts.  The per-particle sums keep the
+// reference's arithmetic type; only their order differs (cell by cell instead
+// of index order).
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "hv_internal.h"
+
+namespace hv {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kMaxCells = 1 << 22;  // cells of the bounding box (coarser cells beyond)
+
+inline int nb(long long n) { return div_up(n > 0 ? n : 1, kBlock); }
+
+template <typename T>
+__global__ void k_bbox_partials(int total, const T *__restrict__ x, const T *__restrict__ y,
+                                const T *__restrict__ z, double *partials) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const double v[3] = {(double)x[i], (double)y[i], (double)z[i]};
+        for (int a = 0; a < 3; a++) {
+            lo[a] = fmin(lo[a], v[a]);
+            hi[a] = fmax(hi[a], v[a]);
+        }
+    }
+    __shared__ double sh[6][kBlock];
+    for (int a = 0; a < 3; a++) {
+        sh[a][threadIdx.x] = lo[a];
+        sh[3 + a][threadIdx.x] = hi[a];
+    }
+    __syncthreads();
+    for (int o = kBlock / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int a = 0; a < 3; a++) {
+                sh[a][threadIdx.x] = fmin(sh[a][threadIdx.x], sh[a][threadIdx.x + o]);
+                sh[3 + a][threadIdx.x] = fmax(sh[3 + a][threadIdx.x], sh[3 + a][threadIdx.x + o]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) partials[6 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+struct Cells {
+    double lo[3];
+    double inv;  // 1 / cell edge
+    int n[3];
+};
+
+__device__ __forceinline__ int cell_axis(double v, double lo, double inv, int n) {
+    int c = (int)((v - lo) * inv);
+    return c < 0 ? 0 : c >= n ? n - 1 : c;
+}
+
+template <typename T>
+__global__ void k_cell_of(int total, Cells cl, const T *__restrict__ x, const T *__restrict__ y,
+                          const T *__restrict__ z, unsigned *keys, int *idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int cx = cell_axis((double)x[i], cl.lo[0], cl.inv, cl.n[0]);
+    const int cy = cell_axis((double)y[i], cl.lo[1], cl.inv, cl.n[1]);
+    const int cz = cell_axis((double)z[i], cl.lo[2], cl.inv, cl.n[2]);
+    keys[i] = (unsigned)((cx * cl.n[1] + cy) * cl.n[2] + cz);
+    idx[i] = i;
+}
+
+// start[c] = first sorted slot of cell c, start[ncells] = total.
+__global__ void k_cell_ranges(int total, int ncells, const unsigned *__restrict__ keys, int *start) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > total) return;
+    const int k = s < total ? (int)keys[s] : ncells;
+    const int prev = s > 0 ? (int)keys[s - 1] : -1;
+    for (int c = prev + 1; c <= k; c++) start[c] = s;
+}
+
+template <typename T>
+__global__ void k_sorted_positions(int total, int protons, const int *__restrict__ idx, const T *__restrict__ x,
+                                   const T *__restrict__ y, const T *__restrict__ z, T *sx, T *sy, T *sz,
+                                   unsigned char *proton) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= total) return;
+    const int i = idx[s];
+    sx[s] = x[i];
+    sy[s] = y[i];
+    sz[s] = z[i];
+    proton[s] = i < protons;
+}
+
+// Sums over the 27 neighbour cells of particle s (sorted order); results to
+// the particle's own slot.
+template <typename T>
+__global__ void k_pair_densities(int total, Cells cl, T exp_term, T cutoff, T term, const int *__restrict__ idx,
+                                 const int *__restrict__ start, const T *__restrict__ sx, const T *__restrict__ sy,
+                                 const T *__restrict__ sz, const unsigned char *__restrict__ proton, T *dp, T *dn) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= total) return;
+    const T xi = sx[s], yi = sy[s], zi = sz[s];
+    const int cx = cell_axis((double)xi, cl.lo[0], cl.inv, cl.n[0]);
+    const int cy = cell_axis((double)yi, cl.lo[1], cl.inv, cl.n[1]);
+    const int cz = cell_axis((double)zi, cl.lo[2], cl.inv, cl.n[2]);
+    T a = T(0), b = T(0);
+    for (int ix = max(cx - 1, 0); ix <= min(cx + 1, cl.n[0] - 1); ix++)
+        for (int iy = max(cy - 1, 0); iy <= min(cy + 1, cl.n[1] - 1); iy++) {
+            const int row = (ix * cl.n[1] + iy) * cl.n[2];
+            const int j0 = start[row + max(cz - 1, 0)], j1 = start[row + min(cz + 1, cl.n[2] - 1) + 1];
+            for (int j = j0; j < j1; j++) {
+                const T ex = xi - sx[j], ey = yi - sy[j], ez = zi - sz[j];
+                const T d2 = ex * ex + ey * ey + ez * ez;
+                if (d2 > cutoff) continue;
+                const T f = exp(-d2 * exp_term);
+                if (proton[j]) a += f;
+                else b += f;
+            }
+        }
+    const int i = idx[s];
+    dp[i] = a * term;
+    dn[i] = b * term;
+}
+
+template <typename T>
+hv_status particle_densities(hv_ctx *c, T *dp_dev, T *dn_dev) {
+    const int N = c->total;
+    if (N == 0) return HV_OK;
+    State<T> &st = state<T>(c);
+    cudaStream_t s = c->stream;
+    // bounding box
+    const int bb = std::min(nb(N), 4 * c->sm_count);
+    double *part = nullptr;
+    HV_CUDA(cudaMallocAsync((void **)&part, sizeof(double) * 6 * bb, s));
+    k_bbox_partials<T><<<bb, kBlock, 0, s>>>(N, st.x, st.y, st.z, part);
+    std::vector<double> hp((size_t)6 * bb);
+    HV_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * 6 * bb, cudaMemcpyDeviceToHost, s));
+    HV_CUDA(cudaFreeAsync(part, s));
+    HV_CUDA(cudaStreamSynchronize(s));
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int b = 0; b < bb; b++)
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], hp[6 * b + a]);
+            hi[a] = std::max(hi[a], hp[6 * b + 3 + a]);
+        }
+    // cells no smaller than the cutoff radius 4 sigma_r
+    const double sig = c->params.sigma_r;
+    double edge = 4.0 * sig;
+    Cells cl;
+    for (;;) {
+        long long cells = 1;
+        for (int a = 0; a < 3; a++) {
+            cl.n[a] = (int)std::floor((hi[a] - lo[a]) / edge) + 1;
+            cells *= cl.n[a];
+        }
+        if (cells <= kMaxCells) break;
+        edge *= 2.0;
+    }
+    for (int a = 0; a < 3; a++) cl.lo[a] = lo[a];
+    cl.inv = 1.0 / edge;
+    const int ncells = cl.n[0] * cl.n[1] * cl.n[2];
+    // sort particles by cell
+    unsigned *keys = nullptr, *keys2 = nullptr;
+    int *idx = nullptr, *idx2 = nullptr, *start = nullptr;
+    T *sx = nullptr, *sy = nullptr, *sz = nullptr;
+    unsigned char *pr = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int bits = 1;
+    while ((1ll << bits) < ncells + 1) bits++;
+    HV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, idx, idx2, N, 0, bits, s));
+    HV_CUDA(cudaMallocAsync((void **)&keys, sizeof(unsigned) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&keys2, sizeof(unsigned) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&idx, sizeof(int) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&idx2, sizeof(int) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&start, sizeof(int) * (ncells + 1), s));
+    HV_CUDA(cudaMallocAsync((void **)&sx, sizeof(T) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&sy, sizeof(T) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&sz, sizeof(T) * N, s));
+    HV_CUDA(cudaMallocAsync((void **)&pr, N, s));
+    HV_CUDA(cudaMallocAsync(&tmp, tmp_bytes, s));
+    k_cell_of<T><<<nb(N), kBlock, 0, s>>>(N, cl, st.x, st.y, st.z, keys, idx);
+    HV_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, idx, idx2, N, 0, bits, s));
+    k_cell_ranges<<<nb(N + 1), kBlock, 0, s>>>(N, ncells, keys2, start);
+    k_sorted_positions<T><<<nb(N), kBlock, 0, s>>>(N, c->protons, idx2, st.x, st.y, st.z, sx, sy, sz, pr);
+    const T sr = T(sig);
+    const T exp_term = T(1.0) / (T(2.0) * sr * sr), cutoff = T(16.0) * sr * sr;
+    const T term = (T(1.0) / c->params.part_per_nucleon) * (T(1.0) / std::pow(T(2.0) * T(kPi) * sr * sr, T(1.5)));
+    k_pair_densities<T><<<nb(N), kBlock, 0, s>>>(N, cl, exp_term, cutoff, term, idx2, start, sx, sy, sz, pr, dp_dev,
+                                                 dn_dev);
+    HV_CUDA(cudaGetLastError());
+    void *bufs[] = {keys, keys2, idx, idx2, start, sx, sy, sz, pr, tmp};
+    for (void *p : bufs) HV_CUDA(cudaFreeAsync(p, s));
+    return HV_OK;
+}
+
+}  // namespace
+}  // namespace hv
+
+using namespace hv;
+
+extern "C" hv_status hv_particle_densities(hv_ctx *c, void *density_p, void *density_n) {
+    if (!c || (!density_p && c->total) || (!density_n && c->total)) return HV_ERR_BAD_ARG;
+    HV_CUDA(cudaSetDevice(c->device));
+    if (c->total == 0) return HV_OK;
+    const size_t es = c->prec == HV_F64 ? 8 : 4, bytes = es * c->total;
+    void *dp = nullptr, *dn = nullptr;
+    HV_CUDA(cudaMallocAsync(&dp, bytes, c->stream));
+    HV_CUDA(cudaMallocAsync(&dn, bytes, c->stream));
+    hv_status st = c->prec == HV_F64
+                       ? particle_densities<double>(c, (double *)dp, (double *)dn)
+                       : particle_densities<float>(c, (float *)dp, (float *)dn);
+    if (st == HV_OK) st = download_slots(c, dp, density_p);
+    if (st == HV_OK) st = download_slots(c, dn, density_n);
+    cudaFreeAsync(dp, c->stream);
+    cudaFreeAsync(dn, c->stream);
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    return st;
+}

@@ -140,6 +140,7 @@ SIGNATURES = {
     "hv_simulate": (_S, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "hv_adjoint_forward": (_S, [_P, _I, _I, _P]),
     "hv_adjoint_backward": (_S, [_P, _P, _P, _P, _P]),
+    "hv_particle_densities": (_S, [_P, _P, _P]),
     "hv_batch_create": (_S, [_I, _P, _P]),
     "hv_batch_destroy": (_S, [_P]),
     "hv_batch_plan": (_S, [_P, _I]),

@@ -220,6 +220,13 @@ class Session:
         L.check(self.lib.hv_observe(self._ctx, C.byref(o)), "hv_observe")
         return o
 
+    def particle_densities(self):
+        """(density_p, density_n) of every particle: compute_particle_densities
+        (tools.hpp:170-203) on the device, with cell lists."""
+        dp, dn = np.empty(self.total, self.dtype), np.empty(self.total, self.dtype)
+        L.check(self.lib.hv_particle_densities(self._ctx, _p(dp), _p(dn)), "hv_particle_densities")
+        return dp, dn
+
     def write_vtk(self, path):
         """One VTK frame of the current forces, density and potential in the
         reference's format (include/init.hpp:159-254)."""

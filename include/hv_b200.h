@@ -364,6 +364,16 @@ HV_API hv_status hv_simulate(const hv_world *world, int protons, int neutrons,
                       int n_steps, void *x, void *y, void *z,
                       void *kx, void *ky, void *kz, hv_observables *obs);
 
+/* compute_particle_densities (include/tools.hpp:170-203), part of the
+ * reference's initialisation (initialize_particles, include/physics.hpp:34-97):
+ * for every particle of the context, the Gaussian-weighted (sigma_r of the
+ * run parameters) sum over all particles within 4 sigma_r, by species, times
+ * 1 / (part_per_nucleon (2 pi sigma_r^2)^1.5) -- the reference's
+ * TestParticles<T>::density_p / density_n.  The reference loops over all pairs
+ * (O(N^2)); here cell lists of edge 4 sigma_r find the partners.  Host arrays
+ * of the context's precision, in the caller's particle order. */
+HV_API hv_status hv_particle_densities(hv_ctx *ctx, void *density_p, void *density_n);
+
 /* ---- adjoint: gradients of a D(t) objective ----------------------------
  * No counterpart in the reference, which has no derivative code: the
  * hand-written adjoint of the plain FP64 step (cpu_simulate's order,

@@ -77,6 +77,8 @@ typedef struct orc_obs {
     void orc_excite_##S(int protons, int neutrons, R *kz, int Z, int N, R eta);               \
     void orc_observe_##S(const orc_world *w, int protons, int neutrons, const R *x,           \
                          const R *y, const R *z, orc_obs *out);                               \
+    void orc_particle_densities_##S(int protons, int neutrons, const R *x, const R *y,         \
+                                    const R *z, double sigma_r, int ppn, R *dp, R *dn);        \
     int orc_simulate_##S(const orc_world *w, const orc_run *run, int protons, int neutrons,    \
                          R *x, R *y, R *z, R *kx, R *ky, R *kz, int steps, orc_obs *obs,      \
                          R *fields_out, double *step_seconds);

@@ -200,6 +200,15 @@ class Oracle:
         f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, ct]
         f(protons, neutrons, _ptr(kz), Z, N, eta)
 
+    def particle_densities(self, protons, neutrons, x, y, z, sigma_r, ppn):
+        """(density_p, density_n) per particle (compute_particle_densities)."""
+        self._chk(x, y, z)
+        dp, dn = np.empty_like(x), np.empty_like(x)
+        f = self._f("orc_particle_densities")
+        f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+        f(protons, neutrons, _ptr(x), _ptr(y), _ptr(z), sigma_r, ppn, _ptr(dp), _ptr(dn))
+        return dp, dn
+
     def observe(self, world, protons, neutrons, x, y, z):
         o = orc_obs()
         self._f("orc_observe")(C.byref(make_world(*world)), protons, neutrons, _ptr(x), _ptr(y), _ptr(z), C.byref(o))
@@ -258,6 +267,15 @@ class Reference:
         n = (C.c_int * 3)(*[int(v) for v in world[0]])
         d = (C.c_double * 3)(*[float(v) for v in world[1]])
         return n, d
+
+    def particle_densities(self, protons, neutrons, x, y, z, sigma_r, ppn):
+        """The reference's compute_particle_densities (include/tools.hpp:170-203)."""
+        x, y, z = (np.array(v, dtype=self.dtype, copy=True) for v in (x, y, z))
+        dp, dn = np.empty_like(x), np.empty_like(x)
+        f = self._f("particle_densities")
+        f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+        f(protons, neutrons, _ptr(x), _ptr(y), _ptr(z), sigma_r, ppn, _ptr(dp), _ptr(dn))
+        return dp, dn
 
     def deposit(self, world, protons, neutrons, x, y, z):
         G = int(np.prod(world[0]))

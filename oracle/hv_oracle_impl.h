@@ -357,6 +357,37 @@ void FN(orc_observe)(const orc_world *w, int protons, int neutrons, const R *x, 
     out->rms_n = sqrt(r2s[1] / (double)cnt[1]);
 }
 
+/* compute_particle_densities (include/tools.hpp:170-203): for every particle
+ * i, the sum over all particles j (itself included, j in index order) within
+ * |r_i - r_j|^2 <= 16 sigma_r^2 of exp(-|r_i - r_j|^2 / (2 sigma_r^2)), by
+ * the species of j, times 1 / (ppn (2 pi sigma_r^2)^1.5); differences r_i - r_j
+ * and their dot product as sub_vec / dot (include/math_functions.hpp:42-68). */
+void FN(orc_particle_densities)(int protons, int neutrons, const R *x, const R *y, const R *z,
+                                double sigma_r_d, int ppn, R *dp, R *dn) {
+    const int total = protons + neutrons;
+    const R sigma_r = (R)sigma_r_d, exp_term = (R)1.0 / ((R)2.0 * sigma_r * sigma_r);
+    const R cutoff = (R)16.0 * sigma_r * sigma_r;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < total; i++) {
+        R a = (R)0.0, b = (R)0.0;
+        for (int j = 0; j < total; j++) {
+            const R ex = x[i] - x[j], ey = y[i] - y[j], ez = z[i] - z[j];
+            const R d2 = ex * ex + ey * ey + ez * ez;
+            if (d2 > cutoff) continue;
+            const R f = EXPR(-d2 * exp_term);
+            if (j < protons) a += f;
+            else b += f;
+        }
+        dp[i] = a;
+        dn[i] = b;
+    }
+    const R term = ((R)1.0 / ppn) * ((R)1.0 / POWR((R)2.0 * (R)ORC_PI * sigma_r * sigma_r, (R)1.5));
+    for (int i = 0; i < total; i++) {
+        dp[i] *= term;
+        dn[i] *= term;
+    }
+}
+
 /* cpu_simulate (src/hyper_vlasov.cpp:32-104) without VTK/stats I/O; one
  * observable row per step, recorded where the reference records it. */
 int FN(orc_simulate)(const orc_world *w, const orc_run *run, int protons, int neutrons, R *x, R *y,

@@ -137,6 +137,19 @@ Parameters<T> mk_param(double sigma_r, int ppn, int z, int n, double eta) {
 REF_API(double, d)
 REF_API(float, f)
 
+// compute_particle_densities (include/tools.hpp:170-203) into dp, dn.
+#define REF_PDENS(T, S)                                                                            \
+    extern "C" void ref_particle_densities_##S(int protons, int neutrons, T *x, T *y, T *z,        \
+                                               double sigma_r, int ppn, T *dp, T *dn) {            \
+        TestParticles<T> p = mk_part<T>(protons, neutrons, x, y, z, 0, 0, 0, 0, 0, 0);             \
+        p.density_p = dp;                                                                          \
+        p.density_n = dn;                                                                          \
+        Parameters<T> pr = mk_param<T>(sigma_r, ppn, 0, 0, 0.0);                                   \
+        compute_particle_densities(&p, pr);                                                        \
+    }
+REF_PDENS(double, d)
+REF_PDENS(float, f)
+
 // OpenMP thread count of the reference routines (1 gives the reproducible
 // particle-order summation of the deposit's array reduction, tools.hpp:45).
 extern "C" void ref_set_threads(int n) { omp_set_num_threads(n); }
