@@ -291,6 +291,42 @@ def adjoint_cost(args, local):
             "grad_t0_t3_sigma_asym": [float(v) for v in grad], "timing": "host wall time"}
 
 
+# ---------------------------------------------------------------- init
+def particle_densities_cost(args, local, world):
+    """compute_particle_densities (the initialisation's O(N^2) per-particle
+    densities) on the device with cell lists: 208Pb with 500 test particles
+    per nucleon (104k, FP64) and with 10000 (2.08M, FP32), against the
+    reference's own routine on all host threads at 104k (one GPU only)."""
+    import numpy as np
+
+    import hv_b200 as hv
+    out = {}
+    for key, w, prec in (("pb208_104k_f64", hv.PB208_104K, hv.HV_F64), ("pb208_2m_f32", hv.PB208_2M, hv.HV_F32)):
+        dt = np.float64 if prec == hv.HV_F64 else np.float32
+        p = hv.workload_particles(w, dt)
+        with hv.Session.from_workload(w, prec, device=local) as s:
+            s.upload_particles(*p)
+            s.particle_densities()
+            t0 = time.perf_counter()
+            s.particle_densities()
+            out[key + "_gpu_s"] = time.perf_counter() - t0
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from hv_oracle import Reference, reference_available
+        if reference_available("_portable"):
+            w = hv.PB208_104K
+            p = hv.workload_particles(w, np.float64)
+            r = Reference(np.float64, "_portable")
+            r.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            r.particle_densities(w.protons, w.neutrons, *p[:3], w.sigma_r, w.ppn)
+            out["pb208_104k_f64_cpu_reference_s"] = time.perf_counter() - t0
+            out["cpu_cores"] = os.cpu_count()
+            out["speedup_104k"] = out["pb208_104k_f64_cpu_reference_s"] / out["pb208_104k_f64_gpu_s"]
+    out["timing"] = "host wall time of hv_particle_densities (incl. download), second call"
+    return out
+
+
 # ---------------------------------------------------------------- batched
 def batched(args, local, world=1, rank=0):
     """The batched form: 64 independent runs (16O..208Pb, 200-2000 test
@@ -490,6 +526,8 @@ def our_arm(args, world, rank, local):
 
     if not args.no_adjoint and rank == 0:
         line["adjoint"] = adjoint_cost(args, local)
+    if not args.no_adjoint and rank == 0:
+        line["particle_densities"] = particle_densities_cost(args, local, world)
     if not args.no_batch:
         bl = batched(args, local, world, rank)  # every rank takes part (its share of the runs)
         if rank == 0:
