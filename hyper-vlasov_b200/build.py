@@ -4,8 +4,9 @@
 
 Each csrc/*.cu and csrc/*.cpp is compiled by nvcc for
 ``-gencode arch=compute_100a,code=sm_100a`` with line info; the plain-path
-kernels (k_plain.cu) additionally get ``--fmad=false`` so that their double
-results can match the reference's arithmetic bit for bit.  The CUDA runtime is
+kernels (k_plain.cu) and the initialisation (init_ws.cu) additionally get
+``--fmad=false`` so that their double results can match the reference's
+arithmetic bit for bit.  The CUDA runtime is
 linked statically so the library needs only the driver on the GPU host.
 Objects go to _build/ (incremental: rebuilt when a source or header changes).
 """
@@ -32,6 +33,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-I", INCLUDE, "-I", CSRC, "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 PER_FILE = {
     "k_plain.cu": ["--fmad=false"],
+    "init_ws.cu": ["--fmad=false"],
 }
 
 

@@ -321,6 +321,26 @@ hv_status download_slots_t(hv_ctx *c, const T *d, T *host) {
 }
 }  // namespace
 
+template <typename T>
+hv_status store_particles(hv_ctx *c, const T *const src[6]) {
+    if (c->total == 0) return HV_OK;
+    State<T> &st = state<T>(c);
+    T *dst[6] = {st.x, st.y, st.z, st.kx, st.ky, st.kz};
+    for (int a = 0; a < 6; a++) {
+        if (slots_permuted(c)) {
+            k_permute<T><<<div_up(c->total, 256), 256, 0, c->stream>>>(c->total, c->perm, src[a], dst[a]);
+            HV_CUDA(cudaGetLastError());
+        } else {
+            HV_CUDA(cudaMemcpyAsync(dst[a], src[a], sizeof(T) * c->total, cudaMemcpyDeviceToDevice, c->stream));
+        }
+    }
+    c->fields_valid = false;
+    fused_invalidate(c);
+    return HV_OK;
+}
+template hv_status store_particles<double>(hv_ctx *, const double *const[6]);
+template hv_status store_particles<float>(hv_ctx *, const float *const[6]);
+
 hv_status download_slots(hv_ctx *c, const void *dev, void *host) {
     if (c->total == 0) return HV_OK;
     return c->prec == HV_F64 ? download_slots_t<double>(c, (const double *)dev, (double *)host)

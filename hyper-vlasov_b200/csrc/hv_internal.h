@@ -254,6 +254,14 @@ hv_status fused_batch_rows(hv_ctx *c, cudaStream_t s, int s0, int k, hv_observab
 hv_status fused_batch_end(hv_ctx *c, int n_steps, int exc);
 void fused_batch_sor_inputs(hv_ctx *c, const float **rho, int **ctl, int **its_ring, int *ring);
 void adjoint_release(hv_ctx *c);
+// compute_particle_densities of N particles (protons first) given by device
+// positions, into dp / dn at the same indices (pdens.cu; stream-ordered)
+template <typename T>
+hv_status particle_densities_at(hv_ctx *c, int N, int protons, const T *x, const T *y, const T *z, T *dp, T *dn);
+// writes per-particle device arrays in the caller's order into the context's
+// particle slots (x, y, z, kx, ky, kz; ctx.cu; stream-ordered)
+template <typename T>
+hv_status store_particles(hv_ctx *c, const T *const src[6]);
 // one plain FP64 step / the field solve and gather of the current positions
 hv_status plain_step_f64(hv_ctx *c, hv_observables *row);
 hv_status plain_fields_f64(hv_ctx *c, int *sor_its);

@@ -130,17 +130,18 @@ __global__ void k_pair_densities(int total, Cells cl, T exp_term, T cutoff, T te
     dn[i] = b * term;
 }
 
+}  // namespace
+
 template <typename T>
-hv_status particle_densities(hv_ctx *c, T *dp_dev, T *dn_dev) {
-    const int N = c->total;
+hv_status particle_densities_at(hv_ctx *c, int N, int protons, const T *px, const T *py, const T *pz, T *dp_dev,
+                                T *dn_dev) {
     if (N == 0) return HV_OK;
-    State<T> &st = state<T>(c);
     cudaStream_t s = c->stream;
     // bounding box
     const int bb = std::min(nb(N), 4 * c->sm_count);
     double *part = nullptr;
     HV_CUDA(cudaMallocAsync((void **)&part, sizeof(double) * 6 * bb, s));
-    k_bbox_partials<T><<<bb, kBlock, 0, s>>>(N, st.x, st.y, st.z, part);
+    k_bbox_partials<T><<<bb, kBlock, 0, s>>>(N, px, py, pz, part);
     std::vector<double> hp((size_t)6 * bb);
     HV_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(double) * 6 * bb, cudaMemcpyDeviceToHost, s));
     HV_CUDA(cudaFreeAsync(part, s));
@@ -187,10 +188,10 @@ hv_status particle_densities(hv_ctx *c, T *dp_dev, T *dn_dev) {
     HV_CUDA(cudaMallocAsync((void **)&sz, sizeof(T) * N, s));
     HV_CUDA(cudaMallocAsync((void **)&pr, N, s));
     HV_CUDA(cudaMallocAsync(&tmp, tmp_bytes, s));
-    k_cell_of<T><<<nb(N), kBlock, 0, s>>>(N, cl, st.x, st.y, st.z, keys, idx);
+    k_cell_of<T><<<nb(N), kBlock, 0, s>>>(N, cl, px, py, pz, keys, idx);
     HV_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, idx, idx2, N, 0, bits, s));
     k_cell_ranges<<<nb(N + 1), kBlock, 0, s>>>(N, ncells, keys2, start);
-    k_sorted_positions<T><<<nb(N), kBlock, 0, s>>>(N, c->protons, idx2, st.x, st.y, st.z, sx, sy, sz, pr);
+    k_sorted_positions<T><<<nb(N), kBlock, 0, s>>>(N, protons, idx2, px, py, pz, sx, sy, sz, pr);
     const T sr = T(sig);
     const T exp_term = T(1.0) / (T(2.0) * sr * sr), cutoff = T(16.0) * sr * sr;
     const T term = (T(1.0) / c->params.part_per_nucleon) * (T(1.0) / std::pow(T(2.0) * T(kPi) * sr * sr, T(1.5)));
@@ -202,7 +203,11 @@ hv_status particle_densities(hv_ctx *c, T *dp_dev, T *dn_dev) {
     return HV_OK;
 }
 
-}  // namespace
+template hv_status particle_densities_at<double>(hv_ctx *, int, int, const double *, const double *, const double *,
+                                                 double *, double *);
+template hv_status particle_densities_at<float>(hv_ctx *, int, int, const float *, const float *, const float *,
+                                                float *, float *);
+
 }  // namespace hv
 
 using namespace hv;
@@ -216,8 +221,10 @@ extern "C" hv_status hv_particle_densities(hv_ctx *c, void *density_p, void *den
     HV_CUDA(cudaMallocAsync(&dp, bytes, c->stream));
     HV_CUDA(cudaMallocAsync(&dn, bytes, c->stream));
     hv_status st = c->prec == HV_F64
-                       ? particle_densities<double>(c, (double *)dp, (double *)dn)
-                       : particle_densities<float>(c, (float *)dp, (float *)dn);
+                       ? particle_densities_at<double>(c, c->total, c->protons, c->d64.x, c->d64.y, c->d64.z,
+                                                       (double *)dp, (double *)dn)
+                       : particle_densities_at<float>(c, c->total, c->protons, c->d32.x, c->d32.y, c->d32.z,
+                                                      (float *)dp, (float *)dn);
     if (st == HV_OK) st = download_slots(c, dp, density_p);
     if (st == HV_OK) st = download_slots(c, dn, density_n);
     cudaFreeAsync(dp, c->stream);

@@ -82,6 +82,35 @@ class hv_observables(C.Structure):
     ]
 
 
+class hv_woods_saxon(C.Structure):
+    _fields_ = [("V0", C.c_double), ("R12", C.c_double), ("a", C.c_double)]
+
+
+class hv_fermi(C.Structure):
+    _fields_ = [("epsilon_p", C.c_double), ("epsilon_n", C.c_double)]
+
+
+HV_RNG_LIBC = 0
+HV_RNG_PHILOX = 1
+
+
+class hv_init_params(C.Structure):
+    _fields_ = [("sigma_k", C.c_double), ("r_max", C.c_double), ("max_test_part", C.c_int),
+                ("max_iterations", C.c_int), ("rng", C.c_int), ("seed", C.c_uint64)]
+
+
+class hv_init_row(C.Structure):
+    _fields_ = [("equal_p", C.c_int), ("equal_n", C.c_int), ("epsilon_p", C.c_double), ("epsilon_n", C.c_double),
+                ("delta_epsilon", C.c_double), ("ws", hv_woods_saxon * 2), ("fit_iterations", C.c_int * 2),
+                ("fit_status", C.c_int * 2)]
+
+
+class hv_init_report(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("delta_epsilon", C.c_double),
+                ("chi_squared_p", C.c_double), ("chi_squared_n", C.c_double), ("candidates", C.c_longlong),
+                ("max_test_part", C.c_int), ("r_max", C.c_double)]
+
+
 OBS_DTYPE = np.dtype([
     ("t", "f8"), ("rms_p", "f8"), ("rms_n", "f8"), ("zcm_p", "f8"), ("zcm_n", "f8"),
     ("dipole", "f8"), ("sor_iterations", "i4"), ("flags", "i4"),
@@ -141,6 +170,10 @@ SIGNATURES = {
     "hv_adjoint_forward": (_S, [_P, _I, _I, _P]),
     "hv_adjoint_backward": (_S, [_P, _P, _P, _P, _P]),
     "hv_particle_densities": (_S, [_P, _P, _P]),
+    "hv_init_params_default": (None, [_P]),
+    "hv_initialize_particles": (_S, [_P, _P, _P, _P, _P, _P, _P]),
+    "hv_fit_woods_saxon": (_S, [_P, _P, _P, _P, _P]),
+    "hv_particle_energies": (_S, [_P, _P, _D, _P]),
     "hv_batch_create": (_S, [_I, _P, _P]),
     "hv_batch_destroy": (_S, [_P]),
     "hv_batch_plan": (_S, [_P, _I]),

@@ -17,6 +17,10 @@ gather()                       distribute_forces_to_particles_cic (tools.hpp:98-
 kick_half(dt) / drift(dt)      update_momenta_half / update_positions_full (physics.hpp:248-270)
 excite(eta)                    nuclear_excitation (physics.hpp:236-246)
 observe()                      center_of_mass / mean_squared_radius (tools.hpp:302-338)
+particle_densities()           compute_particle_densities (tools.hpp:170-203)
+particle_energies(ws, sigma_k) compute_particle_energies (tools.hpp:226-232)
+fit_woods_saxon(ws)            minim_woods_saxon (fit_algorithm.hpp:95-137), GSL restated
+initialize_particles(ws, eps)  initialize_particles (physics.hpp:34-97)
 initial_solve() / run(steps)   cpu_simulate (src/hyper_vlasov.cpp:32-104)
 =============================  =============================================
 
@@ -36,6 +40,17 @@ from .workloads import Workload
 
 def _p(a):
     return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _ws_array(ws):
+    w = (L.hv_woods_saxon * 2)()
+    for q in range(2):
+        w[q].V0, w[q].R12, w[q].a = (float(v) for v in ws[q])
+    return w
+
+
+def _ws_tuple(w):
+    return tuple((w[q].V0, w[q].R12, w[q].a) for q in range(2))
 
 
 def generate_nucleus(seed, protons, neutrons, radius, k_fermi, dtype=np.float64):
@@ -226,6 +241,52 @@ class Session:
         dp, dn = np.empty(self.total, self.dtype), np.empty(self.total, self.dtype)
         L.check(self.lib.hv_particle_densities(self._ctx, _p(dp), _p(dn)), "hv_particle_densities")
         return dp, dn
+
+    def particle_energies(self, ws, sigma_k):
+        """compute_particle_energies (tools.hpp:226-232) of every particle with
+        Woods-Saxon parameters ws = ((V0, R12, a) protons, (V0, R12, a) neutrons)."""
+        w = _ws_array(ws)
+        e = np.empty(self.total, self.dtype)
+        L.check(self.lib.hv_particle_energies(self._ctx, C.byref(w), float(sigma_k), _p(e)), "hv_particle_energies")
+        return e
+
+    def fit_woods_saxon(self, ws, skyrme=None):
+        """minim_woods_saxon (fit_algorithm.hpp:95-137) on the particles and
+        their densities, from ws; returns (fitted ws, iterations, status)."""
+        w = _ws_array(ws)
+        it, st = (C.c_int * 2)(), (C.c_int * 2)()
+        sk = C.byref(skyrme) if skyrme is not None else None
+        L.check(self.lib.hv_fit_woods_saxon(self._ctx, sk, C.byref(w), it, st), "hv_fit_woods_saxon")
+        return _ws_tuple(w), tuple(it), tuple(st)
+
+    def initialize_particles(self, ws, fermi, sigma_k=None, rng=L.HV_RNG_PHILOX, seed=128, max_iterations=0,
+                             max_test_part=0, r_max=0.0, skyrme=None):
+        """initialize_particles (physics.hpp:34-97) on the device: replaces the
+        session's particles by the Woods-Saxon loop's.  ws as for
+        fit_woods_saxon, fermi = (eps_p, eps_n) starting values; sigma_k None
+        takes calc_sigma(0.346).  HV_RNG_LIBC draws rand() in the reference's
+        order (seed it with srand first).  Returns (ws, fermi, report, rows):
+        the final parameters, the hv_init_report fields as a dict and one
+        hv_init_row per pass."""
+        ip = L.hv_init_params()
+        self.lib.hv_init_params_default(C.byref(ip))
+        if sigma_k is not None:
+            ip.sigma_k = float(sigma_k)
+        ip.rng, ip.seed = int(rng), int(seed)
+        ip.max_iterations, ip.max_test_part, ip.r_max = int(max_iterations), int(max_test_part), float(r_max)
+        w = _ws_array(ws)
+        f = L.hv_fermi(float(fermi[0]), float(fermi[1]))
+        rep = L.hv_init_report()
+        rows = (L.hv_init_row * (ip.max_iterations or 32))()
+        sk = C.byref(skyrme) if skyrme is not None else None
+        L.check(self.lib.hv_initialize_particles(self._ctx, sk, C.byref(w), C.byref(f), C.byref(ip), C.byref(rep),
+                                                 rows), "hv_initialize_particles")
+        report = {k: getattr(rep, k) for k, _ in L.hv_init_report._fields_}
+        out_rows = [{"equal_p": r.equal_p, "equal_n": r.equal_n, "epsilon_p": r.epsilon_p,
+                     "epsilon_n": r.epsilon_n, "delta_epsilon": r.delta_epsilon,
+                     "ws": _ws_tuple(r.ws), "fit_iterations": tuple(r.fit_iterations),
+                     "fit_status": tuple(r.fit_status)} for r in rows[:rep.iterations]]
+        return _ws_tuple(w), (f.epsilon_p, f.epsilon_n), report, out_rows
 
     def write_vtk(self, path):
         """One VTK frame of the current forces, density and potential in the

@@ -121,6 +121,25 @@ class Workload:
         return replace(self, sor_omega=1.5, sor_tol=1e-4, sor_criterion=L.HV_SOR_MAX_UPDATE, sor_max_iter=512)
 
 
+# Starting values of the initialisation loop in the reference's driver
+# (auto_compute.py:41-55): Woods-Saxon V0 = -50 MeV, a = 0.66 fm, R12 = 0.8 r_max
+# (include/init.hpp:335-336), Fermi levels -8 / -12 MeV, momentum FWHM 0.346
+# fm^-1, Skyrme A = -356.8, B = 303.9, C = 32 MeV, gamma = 7/6.
+INIT_V0, INIT_A, INIT_EPS_P, INIT_EPS_N, INIT_K_FWHM = -50.0, 0.66, -8.0, -12.0, 0.346
+INIT_SKYRME = (-356.8, 303.9, 32.0, 7.0 / 6.0)
+
+
+def nuclear_radius(A: int) -> float:
+    """r_max = 1.5 A^(1/3) fm (include/physics_formulas.hpp:27-32)."""
+    return 1.5 * A ** (1.0 / 3.0)
+
+
+def init_start(Z: int, N: int):
+    """(ws, fermi) starting values: ((V0, R12, a) x 2), (eps_p, eps_n)."""
+    r12 = 0.8 * nuclear_radius(Z + N)
+    return ((INIT_V0, r12, INIT_A), (INIT_V0, r12, INIT_A)), (INIT_EPS_P, INIT_EPS_N)
+
+
 # 40Ca, 100 test particles per nucleon, 32^3, h = 1 fm, dt = 0.5 fm/c, 200 steps
 CA40_SMALL = Workload("40Ca-4k-32^3", Z=20, N=20, ppn=100, n=32, h=1.0, dt=0.5, steps=200)
 # 208Pb, 500 per nucleon (104,000 particles), 64^3, h = 0.5 fm, dt = 0.25, 2000 steps

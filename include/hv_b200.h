@@ -374,6 +374,96 @@ HV_API hv_status hv_simulate(const hv_world *world, int protons, int neutrons,
  * of the context's precision, in the caller's particle order. */
 HV_API hv_status hv_particle_densities(hv_ctx *ctx, void *density_p, void *density_n);
 
+/* ---- initialisation: the Woods-Saxon self-consistency loop ---------------
+ * initialize_particles (include/physics.hpp:34-97) on the device: Fermi levels
+ * from 2M temporary particles, the run's particles as (r, k) / (-r, -k) pairs
+ * below the levels, their densities, a Woods-Saxon fit per species, relaxation
+ * by 0.6, repeated until |d eps_p| + |d eps_n| <= 0.1 or max_iterations. */
+
+/* WoodsSaxon<T> (include/sim_structs.hpp:78-81): V(r) = V0 / (1 + exp((r - R12) / a)). */
+typedef struct hv_woods_saxon {
+    double V0, R12, a;
+} hv_woods_saxon;
+
+/* Fermi<T> (include/sim_structs.hpp:88-90). */
+typedef struct hv_fermi {
+    double epsilon_p, epsilon_n;
+} hv_fermi;
+
+/* Source of the uniform numbers of the rejection sampling. */
+typedef enum hv_rng {
+    /* the C library's rand(), drawn on the host in the reference's order
+     * (rand_val, include/math_functions.hpp:29-33): after srand(seed) the run
+     * is the reference's, and rand() continues afterwards exactly as after the
+     * reference's loop.  Host-bound (6 rand() calls per candidate pair). */
+    HV_RNG_LIBC = 0,
+    /* Philox4x32-10 on the device, keyed by hv_init_params.seed */
+    HV_RNG_PHILOX = 1
+} hv_rng;
+
+typedef struct hv_init_params {
+    double sigma_k;      /* Parameters::sigma_k = calc_sigma(k_fwhm) (init.hpp:322) */
+    double r_max;        /* 0: nuclear_radius(Z + N) = 1.5 A^(1/3) (init.hpp:55)    */
+    int max_test_part;   /* temporaries per species; 0: max_particles(r_max, k_max, ppn) (init.hpp:57) */
+    int max_iterations;  /* 0: MAX_INIT_ITERATIONS = 32 (sim_structs.hpp:28)        */
+    int rng;             /* hv_rng                                                 */
+    unsigned long long seed;  /* HV_RNG_PHILOX key                                 */
+} hv_init_params;
+
+/* One pass of the loop: what the reference prints (physics.hpp:85-90). */
+typedef struct hv_init_row {
+    int equal_p, equal_n;          /* 2 x temporaries below each Fermi level     */
+    double epsilon_p, epsilon_n;   /* Fermi levels after the update              */
+    double delta_epsilon;          /* |d eps_n| + |d eps_p|                      */
+    hv_woods_saxon ws[2];          /* after the fit and the relaxation           */
+    int fit_iterations[2];         /* iterations of the fit, protons / neutrons  */
+    int fit_status[2];             /* as hv_fit_woods_saxon's status             */
+} hv_init_row;
+
+typedef struct hv_init_report {
+    int iterations;                /* passes of the loop                         */
+    int converged;                 /* the last |d eps| sum was <= 0.1 (else the  */
+                                   /* reference prints "INITIALIZATION DID NOT CONVERGE!") */
+    double delta_epsilon;
+    double chi_squared_p, chi_squared_n;  /* chi_squared (tools.hpp:340-366)   */
+    long long candidates;          /* candidates drawn (3 or 6 numbers each)     */
+    int max_test_part;             /* temporaries per species used               */
+    double r_max;                  /* sampling radius used                       */
+} hv_init_report;
+
+/* Defaults: sigma_k = calc_sigma(0.346) (auto_compute.py:54), r_max and
+ * max_test_part derived, 32 passes, HV_RNG_PHILOX, seed 128. */
+HV_API void hv_init_params_default(hv_init_params *p);
+
+/* initialize_particles (include/physics.hpp:34-97): replaces the context's
+ * particles (which must number Z ppn protons and N ppn neutrons, an even total,
+ * from the run parameters) by the loop's final ones, in the reference's order.
+ * ws[2] (protons, neutrons) and fermi are the starting values and receive the
+ * final ones, as the reference's pointers do; skm NULL takes the run
+ * parameters' Skyrme.  rows (NULL or max_iterations entries) receives one row
+ * per pass.  The Woods-Saxon fit restates GSL's driver (absent here) as
+ * Levenberg-Marquardt; HV_ERR_NOT_CONVERGED when no candidate can be kept
+ * (the reference would loop for ever). */
+HV_API hv_status hv_initialize_particles(hv_ctx *ctx, const hv_skyrme *skm, hv_woods_saxon ws[2],
+                                         hv_fermi *fermi, const hv_init_params *params,
+                                         hv_init_report *report, hv_init_row *rows);
+
+/* minim_woods_saxon (include/fit_algorithm.hpp:95-137) on the context's
+ * particles and their compute_particle_densities: per species, the least-squares
+ * fit of V0 / (1 + exp((r - R12) / a)) to skyrme_potential of the particle's
+ * densities, from ws (in/out).  Levenberg-Marquardt with More's scaling, step
+ * and gradient tests xtol = gtol = 1e-4, at most 100 iterations (the
+ * reference's GSL call arguments; its ftol is not tested).  status: 1 xtol,
+ * 2 gtol, 0 iterations exhausted, -1 no acceptable step, -2 fewer than 3
+ * particles (ws unchanged). */
+HV_API hv_status hv_fit_woods_saxon(hv_ctx *ctx, const hv_skyrme *skm, hv_woods_saxon ws[2],
+                                    int iterations[2], int status[2]);
+
+/* compute_particle_energies (include/tools.hpp:226-232) of the context's
+ * particles: host array of the context's precision, caller's order. */
+HV_API hv_status hv_particle_energies(hv_ctx *ctx, const hv_woods_saxon ws[2], double sigma_k,
+                                      void *energy);
+
 /* ---- adjoint: gradients of a D(t) objective ----------------------------
  * No counterpart in the reference, which has no derivative code: the
  * hand-written adjoint of the plain FP64 step (cpu_simulate's order,

@@ -79,6 +79,12 @@ typedef struct orc_obs {
                          const R *y, const R *z, orc_obs *out);                               \
     void orc_particle_densities_##S(int protons, int neutrons, const R *x, const R *y,         \
                                     const R *z, double sigma_r, int ppn, R *dp, R *dn);        \
+    void orc_particle_energies_##S(int protons, int neutrons, const R *x, const R *y,          \
+                                   const R *z, const R *kx, const R *ky, const R *kz,         \
+                                   const double *ws, double sigma_k, int zc, R *energy);      \
+    int orc_fit_woods_saxon_##S(int n, const R *x, const R *y, const R *z, const R *dp,       \
+                                const R *dn, int type, const orc_skyrme *skm, double *ws,     \
+                                int max_iter, double xtol, double gtol, int *iters);          \
     int orc_simulate_##S(const orc_world *w, const orc_run *run, int protons, int neutrons,    \
                          R *x, R *y, R *z, R *kx, R *ky, R *kz, int steps, orc_obs *obs,      \
                          R *fields_out, double *step_seconds);

@@ -209,6 +209,31 @@ class Oracle:
         f(protons, neutrons, _ptr(x), _ptr(y), _ptr(z), sigma_r, ppn, _ptr(dp), _ptr(dn))
         return dp, dn
 
+    def particle_energies(self, protons, neutrons, x, y, z, kx, ky, kz, ws, sigma_k, zc):
+        """compute_energy per particle; ws = ((V0, R12, a) protons, neutrons)."""
+        self._chk(x, y, z, kx, ky, kz)
+        e = np.empty_like(x)
+        w = (C.c_double * 6)(*[float(v) for t in ws for v in t])
+        f = self._f("orc_particle_energies")
+        f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 7 + [C.c_double, C.c_int, C.c_void_p]
+        f(protons, neutrons, _ptr(x), _ptr(y), _ptr(z), _ptr(kx), _ptr(ky), _ptr(kz), w, sigma_k, zc, _ptr(e))
+        return e
+
+    def fit_woods_saxon(self, x, y, z, dp, dn, species, skyrme, ws, max_iter=100, xtol=1e-4, gtol=1e-4):
+        """The Levenberg-Marquardt restatement of minim_woods_saxon for one
+        species' particles; returns ((V0, R12, a), iterations, status)."""
+        self._chk(x, y, z, dp, dn)
+        w = (C.c_double * 3)(*[float(v) for v in ws])
+        it = C.c_int(0)
+        sk = orc_skyrme(*[float(v) for v in skyrme])
+        f = self._f("orc_fit_woods_saxon")
+        f.argtypes = [C.c_int] + [C.c_void_p] * 5 + [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                                     C.c_double, C.c_void_p]
+        f.restype = C.c_int
+        st = f(len(x), _ptr(x), _ptr(y), _ptr(z), _ptr(dp), _ptr(dn), species, C.byref(sk), w, max_iter, xtol, gtol,
+               C.byref(it))
+        return (w[0], w[1], w[2]), it.value, st
+
     def observe(self, world, protons, neutrons, x, y, z):
         o = orc_obs()
         self._f("orc_observe")(C.byref(make_world(*world)), protons, neutrons, _ptr(x), _ptr(y), _ptr(z), C.byref(o))
@@ -276,6 +301,43 @@ class Reference:
         f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 3 + [C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         f(protons, neutrons, _ptr(x), _ptr(y), _ptr(z), sigma_r, ppn, _ptr(dp), _ptr(dn))
         return dp, dn
+
+    def particle_energies(self, protons, neutrons, x, y, z, kx, ky, kz, ws, sigma_k, zc):
+        """The reference's compute_particle_energies (include/tools.hpp:226-232)."""
+        arrs = [np.array(v, dtype=self.dtype, copy=True) for v in (x, y, z, kx, ky, kz)]
+        e = np.empty_like(arrs[0])
+        w = (C.c_double * 6)(*[float(v) for t in ws for v in t])
+        f = self._f("particle_energies")
+        f.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 6 + [C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+        f(protons, neutrons, *[_ptr(a) for a in arrs], w, sigma_k, zc, _ptr(e))
+        return e
+
+    def init_sizes(self, z, n, ppn):
+        """(r_max, max_test_part) as set_parameters derives them."""
+        r, m = C.c_double(), C.c_int()
+        self.lib.ref_init_sizes(z, n, ppn, C.byref(r), C.byref(m))
+        return r.value, m.value
+
+    def initialize_particles(self, z, n, ppn, sigma_k, sigma_r, skyrme, ws, fermi, seed):
+        """srand(seed) and the reference's initialize_particles
+        (include/physics.hpp:34-97), its GSL fit replaced by the oracle's
+        restatement.  Returns dict: x..kz, density_p/n, energy, ws, fermi,
+        passes, fit_iterations, fit_status."""
+        total = (z + n) * ppn
+        arrs = [np.zeros(total, self.dtype) for _ in range(9)]
+        sk = (C.c_double * 4)(*[float(v) for v in skyrme])
+        w = (C.c_double * 6)(*[float(v) for t in ws for v in t])
+        fe = (C.c_double * 2)(float(fermi[0]), float(fermi[1]))
+        info = (C.c_int * 5)()
+        f = self._f("initialize_particles")
+        f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_uint] + [C.c_void_p] * 10
+        f(z, n, ppn, sigma_k, sigma_r, sk, w, fe, seed, *[_ptr(a) for a in arrs], info)
+        names = ("x", "y", "z", "kx", "ky", "kz", "density_p", "density_n", "energy")
+        out = dict(zip(names, arrs))
+        out.update(ws=((w[0], w[1], w[2]), (w[3], w[4], w[5])), fermi=(fe[0], fe[1]), passes=info[0],
+                   fit_iterations=(info[1], info[2]), fit_status=(info[3], info[4]))
+        return out
 
     def deposit(self, world, protons, neutrons, x, y, z):
         G = int(np.prod(world[0]))

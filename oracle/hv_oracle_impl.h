@@ -458,6 +458,158 @@ int FN(orc_simulate)(const orc_world *w, const orc_run *run, int protons, int ne
     return rc;
 }
 
+/* ---- initialisation ---------------------------------------------------- */
+
+/* compute_energy (include/tools.hpp:205-224) for every particle: Woods-Saxon
+ * potential of the particle's species (physics_formulas.hpp:64-68), kinetic
+ * term k^2 hbar^2 c^2 / (2 m c^2) with k = |k| (physics_formulas.hpp:34-38),
+ * the uniform-sphere Coulomb potential for protons (physics_formulas.hpp:79-84)
+ * and the fluctuation term 3 e_kin sigma_k^2 (physics_formulas.hpp:40-44), summed
+ * in that order from 0.  ws = {V0, R12, a} of protons then neutrons. */
+void FN(orc_particle_energies)(int protons, int neutrons, const R *x, const R *y, const R *z,
+                               const R *kx, const R *ky, const R *kz, const double *ws,
+                               double sigma_k_d, int zc_i, R *energy) {
+    const R hc2 = (R)197.33 * (R)197.33, ekin = hc2 / ((R)2.0 * (R)935.0);
+    const R sigma_k = (R)sigma_k_d, zc = (R)zc_i;
+    const R efluc = (R)3.0 * ekin * sigma_k * sigma_k;
+    const int total = protons + neutrons;
+    for (int i = 0; i < total; i++) {
+        const int sp = i < protons ? 0 : 1;
+        const R V0 = (R)ws[3 * sp], R12 = (R)ws[3 * sp + 1], a = (R)ws[3 * sp + 2];
+        const R r = SQRTR(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+        const R k = SQRTR(kx[i] * kx[i] + ky[i] * ky[i] + kz[i] * kz[i]);
+        R e = (R)0.0;
+        e += V0 / ((R)1.0 + EXPR((r - R12) / a));
+        e += (k * k) * ekin;
+        if (sp == 0) {
+            if (r <= R12) e += (R)1.44 * (zc - (R)1.0) / R12 * ((R)1.5 - (R)0.5 * (r / R12) * (r / R12));
+            else e += (R)1.44 * (zc - (R)1.0) / r;
+        }
+        e += efluc;
+        energy[i] = e;
+    }
+}
+
+/* Sums of the Woods-Saxon fit at x = {V0, R12, a}: out[0] = f^T f, out[1..6] =
+ * J^T J (00, 01, 02, 11, 12, 22), out[7..9] = J^T f, in particle order.  The
+ * residual f_i = v_skyrme_i - V0 / (1 + exp((r_i - R12) / a)) and its Jacobian
+ * row are evaluated in R as woods_saxon_f / woods_saxon_df do
+ * (include/fit_algorithm.hpp:49-94), the parameters first rounded to R. */
+static void FN(orc_ws_sums)(int n, const R *r, const R *vs, const double *x, double *out) {
+    const R V0 = (R)x[0], R12 = (R)x[1], a = (R)x[2];
+    for (int q = 0; q < 10; q++) out[q] = 0.0;
+    for (int i = 0; i < n; i++) {
+        const R e = EXPR((r[i] - R12) / a);
+        const R f = vs[i] - V0 / ((R)1.0 + e);
+        const R e2 = ((R)1.0 + e) * ((R)1.0 + e);
+        const double j0 = (double)(-(R)1.0 / ((R)1.0 + e));
+        const double j1 = (double)(-(V0 * e) / (a * e2));
+        const double j2 = (double)(-(V0 * (r[i] - R12) * e) / (a * a * e2));
+        const double fd = (double)f;
+        out[0] += fd * fd;
+        out[1] += j0 * j0; out[2] += j0 * j1; out[3] += j0 * j2;
+        out[4] += j1 * j1; out[5] += j1 * j2; out[6] += j2 * j2;
+        out[7] += j0 * fd; out[8] += j1 * fd; out[9] += j2 * fd;
+    }
+}
+
+/* minim_woods_saxon (include/fit_algorithm.hpp:95-137) for one species: the
+ * least-squares fit of V0 / (1 + exp((r - R12) / a)) to the particles' Skyrme
+ * potentials, started from ws = {V0, R12, a} and written back there.  The
+ * reference calls GSL's trust-region driver (gsl_multifit_nlinear_trust, default
+ * parameters, at most 100 iterations, xtol = gtol = ftol = 1e-4).  GSL is not
+ * part of this restatement: the solver is Levenberg-Marquardt as published by
+ * Madsen, Nielsen and Tingleff (2004, algorithm 3.16: damping mu on the scaled
+ * normal equations (J^T J + mu D) h = -J^T f, gain ratio rho, mu *= max(1/3,
+ * 1 - (2 rho - 1)^3) on success, mu *= nu, nu *= 2 on failure, mu_0 = 1e-3),
+ * with More's scaling D = running max of diag(J^T J), and the step and
+ * gradient tests of GSL's manual: |h_i| <= xtol (|x_i| + xtol) for all i;
+ * max_i |g_i| max(|x_i|, 1) <= gtol max(F, 1) with F = f^T f / 2 (the
+ * relative-decrease test on ftol is not applied: a fit runs until its step or
+ * its gradient is small).  Returns 1 or 2 for the test that stopped it, 0 when
+ * max_iter ran out, -1 when the damping grew without an accepted step, -2 for
+ * fewer than 3 particles (ws unchanged).  *iters: iterations taken. */
+int FN(orc_fit_woods_saxon)(int n, const R *x, const R *y, const R *z, const R *dp, const R *dn,
+                            int type, const orc_skyrme *skm, double *ws, int max_iter,
+                            double xtol, double gtol, int *iters) {
+    *iters = 0;
+    if (n < 3) return -2;
+    R *r = (R *)malloc(sizeof(R) * (size_t)n), *vs = (R *)malloc(sizeof(R) * (size_t)n);
+    const R A = (R)skm->A, B = (R)skm->B, C = (R)skm->C, gam = (R)skm->gamma, rho0 = (R)0.16;
+    const R tau = type == 0 ? (R)-1.0 : (R)1.0;
+    for (int i = 0; i < n; i++) {
+        r[i] = SQRTR(x[i] * x[i] + y[i] * y[i] + z[i] * z[i]);
+        /* skyrme_potential (include/physics_formulas.hpp:70-77) */
+        const R rho = dp[i] + dn[i], t = rho / rho0;
+        vs[i] = A * t + B * POWR(t, gam) + (R)2.0 * tau * C * ((dn[i] - dp[i]) / rho0);
+    }
+    double p[3] = {ws[0], ws[1], ws[2]}, s[10], sn[10], D[3], h[3];
+    FN(orc_ws_sums)(n, r, vs, p, s);
+    for (int k = 0; k < 3; k++) D[k] = 0.0;
+    double mu = 1e-3, nu = 2.0;
+    int status = 0, it = 0;
+    static const int dg[3] = {1, 4, 6};
+    for (int k = 0; k < 3; k++) D[k] = s[dg[k]] > D[k] ? s[dg[k]] : D[k];
+    for (it = 1; it <= max_iter; it++) {
+        /* (J^T J + mu D) h = -J^T f by Gaussian elimination, partial pivoting */
+        double M[3][4] = {{s[1] + mu * D[0], s[2], s[3], -s[7]},
+                          {s[2], s[4] + mu * D[1], s[5], -s[8]},
+                          {s[3], s[5], s[6] + mu * D[2], -s[9]}};
+        int singular = 0;
+        for (int c = 0; c < 3 && !singular; c++) {
+            int pv = c;
+            for (int q = c + 1; q < 3; q++)
+                if (fabs(M[q][c]) > fabs(M[pv][c])) pv = q;
+            if (!(fabs(M[pv][c]) > 0.0)) { singular = 1; break; }
+            if (pv != c)
+                for (int q = 0; q < 4; q++) { double t = M[c][q]; M[c][q] = M[pv][q]; M[pv][q] = t; }
+            for (int q = c + 1; q < 3; q++) {
+                const double m = M[q][c] / M[c][c];
+                for (int u = c; u < 4; u++) M[q][u] -= m * M[c][u];
+            }
+        }
+        if (singular) { status = -1; break; }
+        for (int c = 2; c >= 0; c--) {
+            double v = M[c][3];
+            for (int u = c + 1; u < 3; u++) v -= M[c][u] * h[u];
+            h[c] = v / M[c][c];
+        }
+        const double pn[3] = {p[0] + h[0], p[1] + h[1], p[2] + h[2]};
+        FN(orc_ws_sums)(n, r, vs, pn, sn);
+        const double pred = 0.5 * (mu * (D[0] * h[0] * h[0] + D[1] * h[1] * h[1] + D[2] * h[2] * h[2]) -
+                                   (s[7] * h[0] + s[8] * h[1] + s[9] * h[2]));
+        const double rho = pred > 0.0 ? 0.5 * (s[0] - sn[0]) / pred : -1.0;
+        if (rho > 0.0 && isfinite(sn[0])) {
+            for (int k = 0; k < 3; k++) p[k] = pn[k];
+            for (int q = 0; q < 10; q++) s[q] = sn[q];
+            for (int k = 0; k < 3; k++) D[k] = s[dg[k]] > D[k] ? s[dg[k]] : D[k];
+            const double t = 2.0 * rho - 1.0, shrink = 1.0 - t * t * t;
+            mu *= shrink > 1.0 / 3.0 ? shrink : 1.0 / 3.0;
+            nu = 2.0;
+            int xs = 1;
+            for (int k = 0; k < 3; k++) xs = xs && fabs(h[k]) <= xtol * (fabs(p[k]) + xtol);
+            if (xs) { status = 1; break; }
+            const double F = 0.5 * s[0];
+            double gm = 0.0;
+            for (int k = 0; k < 3; k++) {
+                const double g = fabs(s[7 + k]) * (fabs(p[k]) > 1.0 ? fabs(p[k]) : 1.0);
+                gm = g > gm ? g : gm;
+            }
+            if (gm <= gtol * (F > 1.0 ? F : 1.0)) { status = 2; break; }
+        } else {
+            mu *= nu;
+            nu *= 2.0;
+            if (!(nu < 1e30)) { status = -1; break; }
+        }
+    }
+    if (it > max_iter) it = max_iter;
+    *iters = it;
+    ws[0] = p[0]; ws[1] = p[1]; ws[2] = p[2];
+    free(r); free(vs);
+    return status;
+}
+
+
 #undef IX
 #undef FN
 #undef CAT

@@ -8,16 +8,19 @@
 // Build: oracle/Makefile target `ref` (needs the reference tree; writes only
 // into oracle/_ref/).  FIT_ALGORITHM_H is predefined so that physics.hpp skips
 // include/fit_algorithm.hpp (GSL, absent here); its only user,
-// initialize_particles (include/physics.hpp:34-97), is a template that is
-// never instantiated below.
+// initialize_particles (include/physics.hpp:34-97), is instantiated below with
+// the oracle's restatement of the fit in GSL's place (ref_initialize_particles).
 #define FIT_ALGORITHM_H
 #include "init.hpp"
 #include "physics.hpp"
 #include "sim_structs.hpp"
 #include "tools.hpp"
 
+#include <cstdlib>
 #include <cstring>
 #include <omp.h>
+
+#include "hv_oracle.h"
 
 namespace {
 
@@ -149,6 +152,124 @@ REF_API(float, f)
     }
 REF_PDENS(double, d)
 REF_PDENS(float, f)
+
+// compute_particle_energies (include/tools.hpp:226-232) into energy; ws = {V0,
+// R12, a} of protons then neutrons.
+#define REF_ENERGY(T, S)                                                                           \
+    extern "C" void ref_particle_energies_##S(int protons, int neutrons, T *x, T *y, T *z, T *kx,  \
+                                              T *ky, T *kz, const double *ws, double sigma_k,      \
+                                              int zc, T *energy) {                                 \
+        TestParticles<T> p = mk_part<T>(protons, neutrons, x, y, z, kx, ky, kz, 0, 0, 0);          \
+        p.energy = energy;                                                                         \
+        Parameters<T> pr = mk_param<T>(0.0, 1, zc, 0, 0.0);                                        \
+        pr.sigma_k = T(sigma_k);                                                                   \
+        WoodsSaxon<T> w[2];                                                                        \
+        for (int s = 0; s < 2; s++) set_woods_saxon(&w[s], T(ws[3 * s]), T(ws[3 * s + 1]),         \
+                                                    T(ws[3 * s + 2]));                             \
+        compute_particle_energies(&p, w, pr);                                                      \
+    }
+REF_ENERGY(double, d)
+REF_ENERGY(float, f)
+
+// initialize_particles (include/physics.hpp:34-97), the reference's own loop,
+// with its Woods-Saxon fit.  The reference's fit (minim_woods_saxon,
+// include/fit_algorithm.hpp:95-137) calls GSL, which is absent; the overload
+// below, found by argument-dependent lookup when initialize_particles is
+// instantiated, runs the oracle's Levenberg-Marquardt restatement
+// (orc_fit_woods_saxon) on the same residuals instead.  Everything else -- the
+// rand() sampling, the energies, the Fermi-level update, the densities and the
+// relaxation -- is the reference's code.
+namespace {
+int g_fit_calls = 0;
+int g_fit_iters[2] = {0, 0}, g_fit_status[2] = {0, 0};
+}  // namespace
+
+inline int orc_fit(int n, const double *x, const double *y, const double *z, const double *dp, const double *dn,
+                   int type, const orc_skyrme *s, double *ws, int *it) {
+    return orc_fit_woods_saxon_d(n, x, y, z, dp, dn, type, s, ws, 100, 1e-4, 1e-4, it);
+}
+inline int orc_fit(int n, const float *x, const float *y, const float *z, const float *dp, const float *dn,
+                   int type, const orc_skyrme *s, double *ws, int *it) {
+    return orc_fit_woods_saxon_f(n, x, y, z, dp, dn, type, s, ws, 100, 1e-4, 1e-4, it);
+}
+
+template <typename T>
+void minim_woods_saxon(TestParticles<T> *part, WoodsSaxon<T> *ws, Skyrme<T> skm) {
+    g_fit_calls++;
+    const orc_skyrme s = {double(skm.A), double(skm.B), double(skm.C), double(skm.gamma)};
+    for (int type = 0; type <= 1; type++) {
+        const int start = type == 0 ? 0 : part->protons;
+        const int total = type == 0 ? part->protons : part->neutrons;
+        double w[3] = {double(ws[type].V0), double(ws[type].R12), double(ws[type].a)};
+        g_fit_status[type] = orc_fit(total, part->x + start, part->y + start, part->z + start,
+                                     part->density_p + start, part->density_n + start, type, &s, w,
+                                     &g_fit_iters[type]);
+        ws[type].V0 = T(w[0]);
+        ws[type].R12 = T(w[1]);
+        ws[type].a = T(w[2]);
+    }
+}
+
+// srand(seed), then initialize_particles with the parameters that
+// read_input_file and set_parameters derive (include/init.hpp:44-58,326-336):
+// r_max = 1.5 A^(1/3), max_test_part = max_particles(r_max, k_max, ppn).
+// io: ws[6] = {V0, R12, a} x 2 (in: the start, R12 is taken as given), fermi[2];
+// out: particles (protons * ppn ... as the reference orders them), their
+// densities and energies, info[0] = loop passes, info[1..2] = iterations of
+// the last fits, info[3..4] their status.
+#define REF_INIT(T, S)                                                                             \
+    extern "C" void ref_initialize_particles_##S(int z, int n, int ppn, double sigma_k,            \
+                                                 double sigma_r, const double *skm, double *ws,    \
+                                                 double *fermi, unsigned seed, T *x, T *y, T *zz,  \
+                                                 T *kx, T *ky, T *kz, T *dp, T *dn, T *energy,     \
+                                                 int *info) {                                      \
+        Parameters<T> pr;                                                                          \
+        std::memset(&pr, 0, sizeof(pr));                                                           \
+        set_parameters(&pr, z, n, ppn, 1, 1, false, T(sigma_k), T(sigma_r), T(1), T(0), T(0));     \
+        Skyrme<T> sk;                                                                              \
+        set_skyrme(&sk, T(skm[0]), T(skm[1]), T(skm[2]), T(skm[3]));                               \
+        WoodsSaxon<T> w[2];                                                                        \
+        for (int s = 0; s < 2; s++) set_woods_saxon(&w[s], T(ws[3 * s]), T(ws[3 * s + 1]),         \
+                                                    T(ws[3 * s + 2]));                             \
+        Fermi<T> fl;                                                                               \
+        set_fermi_levels(&fl, T(fermi[0]), T(fermi[1]));                                           \
+        TestParticles<T> part;                                                                     \
+        g_fit_calls = 0;                                                                           \
+        std::srand(seed);                                                                          \
+        initialize_particles(&part, w, sk, &fl, pr);                                               \
+        const int total = part.protons + part.neutrons;                                            \
+        std::memcpy(x, part.x, sizeof(T) * total);                                                 \
+        std::memcpy(y, part.y, sizeof(T) * total);                                                 \
+        std::memcpy(zz, part.z, sizeof(T) * total);                                                \
+        std::memcpy(kx, part.kx, sizeof(T) * total);                                               \
+        std::memcpy(ky, part.ky, sizeof(T) * total);                                               \
+        std::memcpy(kz, part.kz, sizeof(T) * total);                                               \
+        std::memcpy(dp, part.density_p, sizeof(T) * total);                                        \
+        std::memcpy(dn, part.density_n, sizeof(T) * total);                                        \
+        std::memcpy(energy, part.energy, sizeof(T) * total);                                       \
+        for (int s = 0; s < 2; s++) {                                                              \
+            ws[3 * s] = double(w[s].V0);                                                           \
+            ws[3 * s + 1] = double(w[s].R12);                                                      \
+            ws[3 * s + 2] = double(w[s].a);                                                        \
+        }                                                                                          \
+        fermi[0] = double(fl.epsilon_p);                                                           \
+        fermi[1] = double(fl.epsilon_n);                                                           \
+        info[0] = g_fit_calls;                                                                     \
+        info[1] = g_fit_iters[0]; info[2] = g_fit_iters[1];                                        \
+        info[3] = g_fit_status[0]; info[4] = g_fit_status[1];                                      \
+        free_particles(&part);                                                                     \
+    }
+REF_INIT(double, d)
+REF_INIT(float, f)
+
+// max_test_part and r_max as set_parameters derives them (init.hpp:55-57).
+extern "C" void ref_init_sizes(int z, int n, int ppn, double *r_max, int *max_test_part) {
+    Parameters<double> pr;
+    std::memset(&pr, 0, sizeof(pr));
+    set_parameters(&pr, z, n, ppn, 1, 1, false, 0.1, 0.6, 1.0, 0.0, 0.0);
+    *r_max = pr.r_max;
+    *max_test_part = pr.max_test_part;
+}
 
 // OpenMP thread count of the reference routines (1 gives the reproducible
 // particle-order summation of the deposit's array reduction, tools.hpp:45).

@@ -18,6 +18,13 @@ Fixtures:
   edge_f64.npz               non-cubic grid (12 x 10 x 14, unequal d_max) with
                              particles outside the grid, on node planes and
                              on the upper faces, through every stage
+  init_ca40_f64.npz          the reference's initialize_particles
+                             (include/physics.hpp:34-97) after srand(128) for
+                             40Ca with 100 test particles per nucleon and the
+                             driver's starting values (auto_compute.py), its
+                             GSL fit replaced by the oracle's restatement
+                             (`python tests/golden/make_golden.py init` writes
+                             only this one)
 """
 from __future__ import annotations
 
@@ -75,7 +82,30 @@ def stages(dtype, world, Z, N, ppn, P, Nn, x, y, z, kx, ky, kz, dt, eta):
     return out
 
 
+def init_fixture():
+    from hv_b200.workloads import INIT_K_FWHM, INIT_SKYRME, init_start, sigma_from_fwhm
+
+    Z, N, ppn, seed = 20, 20, 100, 128
+    ws, fermi = init_start(Z, N)
+    sigma_k, sigma_r = sigma_from_fwhm(INIT_K_FWHM), sigma_from_fwhm(1.444)
+    ref = Reference(np.float64)
+    ref.set_threads(os.cpu_count() or 1)
+    out = ref.initialize_particles(Z, N, ppn, sigma_k, sigma_r, INIT_SKYRME, ws, fermi, seed)
+    r_max, mtp = ref.init_sizes(Z, N, ppn)
+    np.savez_compressed(os.path.join(HERE, "init_ca40_f64.npz"), Z=Z, N=N, ppn=ppn, seed=seed, sigma_k=sigma_k,
+                        sigma_r=sigma_r, skyrme=np.array(INIT_SKYRME), ws0=np.array(ws), fermi0=np.array(fermi),
+                        ws=np.array(out["ws"]), fermi=np.array(out["fermi"]), passes=out["passes"],
+                        fit_iterations=np.array(out["fit_iterations"]), fit_status=np.array(out["fit_status"]),
+                        r_max=r_max, max_test_part=mtp,
+                        **{k: out[k] for k in ("x", "y", "z", "kx", "ky", "kz", "density_p", "density_n",
+                                               "energy")})
+    print("wrote init", out["passes"], out["ws"], out["fermi"])
+
+
 def main():
+    if sys.argv[1:] == ["init"]:
+        init_fixture()
+        return
     w = CA40_SMALL
     world = w.world_tuple()
     for dtype, tag in ((np.float64, "f64"), (np.float32, "f32")):
@@ -117,6 +147,7 @@ def main():
     out = stages(np.float64, (n, dm), 12, 8, 25, P, Nn, x, y, z, kx, ky, kz, 0.3, 0.1)
     np.savez_compressed(os.path.join(HERE, "edge_f64.npz"), **out)
     print("wrote edge")
+    init_fixture()
 
 
 if __name__ == "__main__":
