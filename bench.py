@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-init", action="store_true", help="skip the initialisation legs (densities, loop)")
     ap.add_argument("--batch-steps", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
@@ -327,6 +328,54 @@ def particle_densities_cost(args, local, world):
     return out
 
 
+def initialisation_cost(args, local, world):
+    """initialize_particles (the Woods-Saxon self-consistency loop) on the
+    device: 208Pb with 10000 test particles per nucleon (2.08M, FP32, Philox
+    random numbers), and 40Ca with 1000 (40k, FP64) drawing the C library's
+    rand() in the reference's order -- the reference's own loop, whose GSL fit
+    is replaced by the oracle's restatement, runs the same random stream on
+    all host threads (one GPU only).  Host wall time around each call."""
+    import ctypes
+
+    import numpy as np
+
+    import hv_b200 as hv
+    from dataclasses import replace
+    from hv_b200.workloads import INIT_K_FWHM, INIT_SKYRME, init_start, sigma_from_fwhm
+    libc = ctypes.CDLL(None)
+    sigma_k = sigma_from_fwhm(INIT_K_FWHM)
+    out = {}
+    for key, w, prec, rng in (("pb208_2m_f32_philox", hv.PB208_2M, hv.HV_F32, hv.HV_RNG_PHILOX),
+                              ("ca40_40k_f64_libc", replace(hv.CA40_SMALL, ppn=1000), hv.HV_F64, hv.HV_RNG_LIBC)):
+        params = w.run_params()
+        params.skyrme = hv._lib.hv_skyrme(*INIT_SKYRME)
+        ws, fermi = init_start(w.Z, w.N)
+        with hv.Session(w.world(), w.protons, w.neutrons, params, prec, device=local) as s:
+            libc.srand(128)
+            t0 = time.perf_counter()
+            _, _, rep, _ = s.initialize_particles(ws, fermi, sigma_k=sigma_k, rng=rng)
+            out[key + "_gpu_s"] = time.perf_counter() - t0
+        out[key + "_passes"] = rep["iterations"]
+        out[key + "_converged"] = bool(rep["converged"])
+        out[key + "_candidates"] = rep["candidates"]
+    if world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from hv_oracle import Reference, reference_available
+        if reference_available("_portable"):
+            w = replace(hv.CA40_SMALL, ppn=1000)
+            ws, fermi = init_start(w.Z, w.N)
+            r = Reference(np.float64, "_portable")
+            r.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            ro = r.initialize_particles(w.Z, w.N, w.ppn, sigma_k, w.sigma_r, INIT_SKYRME, ws, fermi, 128)
+            out["ca40_40k_f64_cpu_reference_s"] = time.perf_counter() - t0
+            out["ca40_40k_f64_cpu_reference_passes"] = ro["passes"]
+            out["cpu_cores"] = os.cpu_count()
+            out["speedup_40k"] = out["ca40_40k_f64_cpu_reference_s"] / out["ca40_40k_f64_libc_gpu_s"]
+    out["timing"] = "host wall time of hv_initialize_particles (incl. the final store of the particles)"
+    return out
+
+
 # ---------------------------------------------------------------- batched
 def batched(args, local, world=1, rank=0):
     """The batched form: 64 independent runs (16O..208Pb, 200-2000 test
@@ -526,8 +575,9 @@ def our_arm(args, world, rank, local):
 
     if not args.no_adjoint and rank == 0:
         line["adjoint"] = adjoint_cost(args, local)
-    if not args.no_adjoint and rank == 0:
+    if not args.no_init and rank == 0:
         line["particle_densities"] = particle_densities_cost(args, local, world)
+        line["initialisation"] = initialisation_cost(args, local, world)
     if not args.no_batch:
         bl = batched(args, local, world, rank)  # every rank takes part (its share of the runs)
         if rank == 0:

@@ -3,13 +3,13 @@
 //
 // The reference sums, for every particle, exp(-d^2 / (2 sigma_r^2)) over all
 // particles within d^2 <= 16 sigma_r^2 -- an O(N^2) double loop.  Here the
-// particles are binned into cubic cells of edge 4 sigma_r over their bounding
-// box and sorted by cell (CUB radix sort), so every partner of a particle lies
-// in the 27 cells around its own.  One thread per particle, in sorted order:
-// the threads of a warp share a cell, hence scan the same neighbour cells, and
-// their partner loads are broadcasts.  The per-particle sums keep the
-// reference's arithmetic type; only their order differs (cell by cell instead
-// of index order).
+// particles are binned into cubic cells of edge sigma_r over their bounding
+// box and sorted by cell (CUB radix sort); a particle scans, per (x, y) row of
+// cells within the cutoff, the z run of cells that the cutoff sphere reaches.
+// One thread per particle, in sorted order: the threads of a warp share a
+// cell, hence scan nearly the same cells, and their partner loads are
+// broadcasts.  The per-particle sums keep the reference's arithmetic type;
+// only their order differs (cell by cell instead of index order).
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -99,23 +99,35 @@ __global__ void k_sorted_positions(int total, int protons, const int *__restrict
     proton[s] = i < protons;
 }
 
-// Sums over the 27 neighbour cells of particle s (sorted order); results to
-// the particle's own slot.
+// Sums over the cells that the cutoff sphere of particle s (sorted order)
+// reaches, results to the particle's own slot.  Per (x, y) row of cells, only
+// the z range of cells within `reach` of the particle is scanned (a sorted,
+// contiguous slot range); reach is the cutoff radius with a margin for the
+// rounding of d^2 in T, whose test decides.
 template <typename T>
-__global__ void k_pair_densities(int total, Cells cl, T exp_term, T cutoff, T term, const int *__restrict__ idx,
-                                 const int *__restrict__ start, const T *__restrict__ sx, const T *__restrict__ sy,
-                                 const T *__restrict__ sz, const unsigned char *__restrict__ proton, T *dp, T *dn) {
+__global__ void k_pair_densities(int total, Cells cl, double edge, double reach, T exp_term, T cutoff, T term,
+                                 const int *__restrict__ idx, const int *__restrict__ start, const T *__restrict__ sx,
+                                 const T *__restrict__ sy, const T *__restrict__ sz,
+                                 const unsigned char *__restrict__ proton, T *dp, T *dn) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= total) return;
     const T xi = sx[s], yi = sy[s], zi = sz[s];
-    const int cx = cell_axis((double)xi, cl.lo[0], cl.inv, cl.n[0]);
-    const int cy = cell_axis((double)yi, cl.lo[1], cl.inv, cl.n[1]);
-    const int cz = cell_axis((double)zi, cl.lo[2], cl.inv, cl.n[2]);
+    const double px = (double)xi, py = (double)yi, pz = (double)zi, r2 = reach * reach;
+    const int x0 = cell_axis(px - reach, cl.lo[0], cl.inv, cl.n[0]), x1 = cell_axis(px + reach, cl.lo[0], cl.inv, cl.n[0]);
+    const int y0 = cell_axis(py - reach, cl.lo[1], cl.inv, cl.n[1]), y1 = cell_axis(py + reach, cl.lo[1], cl.inv, cl.n[1]);
     T a = T(0), b = T(0);
-    for (int ix = max(cx - 1, 0); ix <= min(cx + 1, cl.n[0] - 1); ix++)
-        for (int iy = max(cy - 1, 0); iy <= min(cy + 1, cl.n[1] - 1); iy++) {
+    for (int ix = x0; ix <= x1; ix++) {
+        const double clo = cl.lo[0] + ix * edge, chi = clo + edge;
+        const double dx = px < clo ? clo - px : px > chi ? px - chi : 0.0;
+        for (int iy = y0; iy <= y1; iy++) {
+            const double rlo = cl.lo[1] + iy * edge, rhi = rlo + edge;
+            const double dy = py < rlo ? rlo - py : py > rhi ? py - rhi : 0.0;
+            const double rem = r2 - dx * dx - dy * dy;
+            if (rem < 0.0) continue;
+            const double dz = sqrt(rem);
+            const int z0 = cell_axis(pz - dz, cl.lo[2], cl.inv, cl.n[2]), z1 = cell_axis(pz + dz, cl.lo[2], cl.inv, cl.n[2]);
             const int row = (ix * cl.n[1] + iy) * cl.n[2];
-            const int j0 = start[row + max(cz - 1, 0)], j1 = start[row + min(cz + 1, cl.n[2] - 1) + 1];
+            const int j0 = start[row + z0], j1 = start[row + z1 + 1];
             for (int j = j0; j < j1; j++) {
                 const T ex = xi - sx[j], ey = yi - sy[j], ez = zi - sz[j];
                 const T d2 = ex * ex + ey * ey + ez * ez;
@@ -125,6 +137,7 @@ __global__ void k_pair_densities(int total, Cells cl, T exp_term, T cutoff, T te
                 else b += f;
             }
         }
+    }
     const int i = idx[s];
     dp[i] = a * term;
     dn[i] = b * term;
@@ -152,9 +165,10 @@ hv_status particle_densities_at(hv_ctx *c, int N, int protons, const T *px, cons
             lo[a] = std::min(lo[a], hp[6 * b + a]);
             hi[a] = std::max(hi[a], hp[6 * b + 3 + a]);
         }
-    // cells no smaller than the cutoff radius 4 sigma_r
+    // cells of a quarter of the cutoff radius 4 sigma_r (coarser when the
+    // bounding box would need more than kMaxCells)
     const double sig = c->params.sigma_r;
-    double edge = 4.0 * sig;
+    double edge = sig;
     Cells cl;
     for (;;) {
         long long cells = 1;
@@ -195,7 +209,8 @@ hv_status particle_densities_at(hv_ctx *c, int N, int protons, const T *px, cons
     const T sr = T(sig);
     const T exp_term = T(1.0) / (T(2.0) * sr * sr), cutoff = T(16.0) * sr * sr;
     const T term = (T(1.0) / c->params.part_per_nucleon) * (T(1.0) / std::pow(T(2.0) * T(kPi) * sr * sr, T(1.5)));
-    k_pair_densities<T><<<nb(N), kBlock, 0, s>>>(N, cl, exp_term, cutoff, term, idx2, start, sx, sy, sz, pr, dp_dev,
+    const double reach = 4.0 * sig * (1.0 + 1e-5);
+    k_pair_densities<T><<<nb(N), kBlock, 0, s>>>(N, cl, edge, reach, exp_term, cutoff, term, idx2, start, sx, sy, sz, pr, dp_dev,
                                                  dn_dev);
     HV_CUDA(cudaGetLastError());
     void *bufs[] = {keys, keys2, idx, idx2, start, sx, sy, sz, pr, tmp};
