@@ -64,7 +64,9 @@ struct SorArgs {
     int nq_shift;           // log2(nz2 / 4) when a power of two, else -1
     u64 *tmirror;           // tagged mirror [x][colour][y][nz2]: value bits | half-sweep << 32
     S hx2i, hy2i, hz2i, inv_diag, omega;
+    S cx, cy, cz, cself;    // omega h^-2 / diag per axis, 1 - omega: the update's coefficients
     double dhx2i, dhy2i, dhz2i, ddiag, src_c;
+    double src_scale;       // omega / diag: the residual is stored pre-scaled
     double tol;
     int max_iter, criterion, inner_min, inner_max, extrapolate;
     const T *rho;
@@ -208,11 +210,14 @@ __device__ S block_max(S m) {
 }
 
 // One SOR update of a node: the reference's phi* and relaxation
-// (include/physics.hpp:114-125) applied to the correction.
+// (include/physics.hpp:114-125) applied to the correction,
+//   self + omega ((xs hx^-2 + ys hy^-2 + zs hz^-2 + r) / diag - self),
+// regrouped as four fused multiply-adds with the source s = omega r / diag
+// stored pre-scaled by the residual pass.
 template <typename S, typename T>
 __device__ __forceinline__ S sor_update(const SorArgs<T, S> &a, S self, S xs, S ys, S zs, S s, bool valid) {
-    const S star = (xs * a.hx2i + ys * a.hy2i + zs * a.hz2i + s) * a.inv_diag;
-    return valid ? self + a.omega * (star - self) : self;
+    const S v = fma(a.cx, xs, fma(a.cy, ys, fma(a.cz, zs, fma(a.cself, self, s))));
+    return valid ? v : self;
 }
 
 // Geometry of one block, shared by the sweeps.
@@ -740,7 +745,8 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     const int k_own = rz_start < zrows_step ? tid % nz : nz;
     const int jz_start = rz_start % nr, pz_start = rz_start / nr, djz = zrows_step % nr, dpz = zrows_step / nr;
 
-    if constexpr (kTag) {
+    constexpr bool kStaged = kTag && kInner > 0;
+    if constexpr (kTag && !kStaged) {
         if (tid == 0) {
             int n = 0;
             for (int pass = 0; pass < 2; pass++)
@@ -752,18 +758,25 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
                 }
         }
     }
-    constexpr bool kStaged = kTag && kInner > 0;
     [[maybe_unused]] Quad inner[kStaged ? kInner : 1];
     [[maybe_unused]] FaceQuad face[kStaged ? kFace : 1];
     [[maybe_unused]] GhostQuad ghost[kStaged ? kGhost : 1];
     if constexpr (kStaged) {
         __shared__ int s_nf, s_ng;
         if (tid == 0) {
-            // perimeter rows and their ghost rows
-            int nf = 0, ng = 0;
-            for (int l = 0; l < np * nr; l++) {
-                const int p = l / nr, j = l - p * nr, x = x0 + p, y = y0 + j;
-                if (!(p == 0 || p + 1 == np || j == 0 || j + 1 == nr)) continue;
+            // Perimeter rows and their ghost rows, and (in `order`) the inner
+            // rows, each listed by the parity of x + y first: a row's parity
+            // fixes which end of its other-colour half-row a quad reads, so
+            // warps whose rows share it take one path.
+            int nf = 0, ng = 0, ni = 0;
+            for (int l = 0; l < 2 * np * nr; l++) {
+                const int par = l / (np * nr), lr = l - par * np * nr;
+                const int p = lr / nr, j = lr - p * nr, x = x0 + p, y = y0 + j;
+                if (((x + y) & 1) != par) continue;
+                if (!(p == 0 || p + 1 == np || j == 0 || j + 1 == nr)) {
+                    order[ni++] = (unsigned)p << 16 | (unsigned)j;
+                    continue;
+                }
                 const bool active = y >= 1 && y <= ny - 2;
                 unsigned gi[4] = {0xffffu, 0xffffu, 0xffffu, 0xffffu};
                 const bool need[4] = {active && p == 0 && x - 1 >= 1, active && p + 1 == np && x + 1 <= a.nx - 2,
@@ -792,7 +805,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
             inner[k] = Quad{0, 0u};
             if (tid >= kGhostThreads && w < niq) {
                 const int r = w / nq, q = w - r * nq;
-                const int p = 1 + r / ir, j = 1 + r % ir;
+                const int p = (int)(order[r] >> 16), j = (int)(order[r] & 0xffffu);
                 inner[k].roff = (p * 2 * nr + j) * nz2 + 4 * q;
                 inner[k].flags = quad_flags(x0 + p, y0 + j, q, nq, nz);
             }
@@ -903,8 +916,8 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
             double r = bv + (pxp + pxm) * a.dhx2i + (pyp + pym) * a.dhy2i + (pzp + pzm) * a.dhz2i - a.ddiag * pc;
             rr += r * r;
             bb += bv * bv;
-            if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)r;
-            else a.src[B.mirror(x, c0, y) + kh] = (S)r;
+            if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)(r * a.src_scale);
+            else a.src[B.mirror(x, c0, y) + kh] = (S)(r * a.src_scale);
         }
         block_sum2(rr, bb);
         if (tid == 0) {
@@ -1223,6 +1236,11 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.hz2i = (S)a.dhz2i;
     a.inv_diag = (S)(1.0 / a.ddiag);
     a.omega = (S)sp.omega;
+    a.cx = (S)(sp.omega * a.dhx2i / a.ddiag);
+    a.cy = (S)(sp.omega * a.dhy2i / a.ddiag);
+    a.cz = (S)(sp.omega * a.dhz2i / a.ddiag);
+    a.cself = (S)(1.0 - sp.omega);
+    a.src_scale = sp.omega / a.ddiag;
     a.src_c = 4.0 * kPi * kE2;
     a.tol = sp.tol;
     a.max_iter = sp.max_iter;
