@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="208Pb-2.08M-128^3")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
-    ap.add_argument("--warm-start", choices=["previous", "extrapolate"], default="previous")
+    ap.add_argument("--warm-start", choices=["previous", "extrapolate"], default="extrapolate")
     ap.add_argument("--sor-exchange", choices=["auto", "flags"], default="auto")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-init", action="store_true", help="skip the initialisation legs (densities, loop)")
+    ap.add_argument("--no-extrap", action="store_true", help="skip the other warm start's comparison run")
     ap.add_argument("--batch-steps", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
@@ -518,6 +519,32 @@ def our_arm(args, world, rank, local):
     gpu_launches = K * launches_per_step + math.ceil(K / chunk)
     sess.close()
 
+    # the same K steps from the other initial guess of the solve (the
+    # reference's: the previous step's phi), same stopping rule, for comparison
+    extrap = None
+    other = hv.HV_WARM_PREVIOUS if warm_mode == hv.HV_WARM_EXTRAPOLATE else hv.HV_WARM_EXTRAPOLATE
+    if not args.no_extrap:
+        with hv.Session.from_workload(w, prec, device=local) as sx:
+            sx.set_fast_options(sor_warm_start=other)
+            sx.upload_particles(*parts)
+            sx.run(W, hv.HV_PATH_FUSED)
+            sstream = torch.cuda.ExternalStream(sx.stream())
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            f0.record(sstream)
+            obs_x = sx.run(K, hv.HV_PATH_FUSED)
+            f1.record(sstream)
+            f1.synchronize()
+            msx = f0.elapsed_time(f1)
+        dref = np.max(np.abs(obs["dipole"]))
+        extrap = {"value": w.particles * K / (msx / 1e3), "ms_per_step": msx / K,
+                  "sor_iterations_per_step": float(obs_x["sor_iterations"].mean()),
+                  "dipole_max_rel_diff_vs_headline": float(np.max(np.abs(obs_x["dipole"] - obs["dipole"])) / dref)
+                  if dref > 0 else None,
+                  "note": ("SOR started from the previous step's phi (the reference's guess)"
+                           if other == hv.HV_WARM_PREVIOUS else "SOR started from 2 phi_n - phi_(n-1)") +
+                          ", same stopping rule"}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -533,6 +560,8 @@ def our_arm(args, world, rank, local):
         "roofline": roofline, "kernels": kernels, "gpu_launches": gpu_launches,
         "clocks": clk.summary(),
     }
+    if extrap:
+        line["warm_start_previous" if other == hv.HV_WARM_PREVIOUS else "warm_start_extrapolate"] = extrap
 
     if not args.no_e2e:
         pinned = [torch.from_numpy(p.copy()).pin_memory() for p in parts]

@@ -50,24 +50,31 @@ def _fused(hv, w, steps, prec, parts, **opts):
 
 
 def test_fused_f32_dipole_within_1e_3_of_double_oracle(hv):
+    """Both initial guesses of the fused SOR: the reference's (the previous
+    phi; then every solve takes at least the oracle's iterations, less one) and
+    the default extrapolated one (fewer iterations, the same stopping rule)."""
     w = hv.CA40_SMALL
     steps = 200
     p32 = hv.workload_particles(w, np.float32)
     obs_o, _ = _oracle(w, steps, [p.astype(np.float64) for p in p32])
-    obs, _ = _fused(hv, w, steps, hv.HV_F32, p32)
+    obs, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_PREVIOUS)
     assert np.array_equal(obs["t"], obs_o["t"].astype(np.float32).astype(np.float64)) or \
         np.max(np.abs(obs["t"] - obs_o["t"])) < 1e-4
     err = max_rel(obs["dipole"], obs_o["dipole"])
     assert err <= 1e-3, err
     assert not np.any(obs["flags"] & 1)
     assert np.all(obs["sor_iterations"] >= obs_o["sor_iterations"] - 1)
+    obs_x, _ = _fused(hv, w, steps, hv.HV_F32, p32)
+    assert max_rel(obs_x["dipole"], obs_o["dipole"]) <= 1e-3
+    assert not np.any(obs_x["flags"] & 1)
+    assert obs_x["sor_iterations"][10:].sum() < obs["sor_iterations"][10:].sum()
 
 
 def test_fused_f64_matches_plain_f64(hv):
     w = hv.CA40_SMALL
     steps = 30
     p = hv.workload_particles(w, np.float64)
-    obs_f, out_f = _fused(hv, w, steps, hv.HV_F64, p)
+    obs_f, out_f = _fused(hv, w, steps, hv.HV_F64, p, sor_warm_start=hv.HV_WARM_PREVIOUS)
     with hv.Session.from_workload(w, hv.HV_F64) as s:
         s.upload_particles(*p)
         s.initial_solve()
@@ -93,7 +100,8 @@ def test_extrapolated_warm_start_saves_iterations(hv):
     w = hv.CA40_SMALL
     steps = 60
     p32 = hv.workload_particles(w, np.float32)
-    obs_a, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_inner_min=1, sor_inner_max=8)
+    obs_a, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_PREVIOUS, sor_inner_min=1,
+                      sor_inner_max=8)
     obs_b, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_EXTRAPOLATE, sor_inner_min=1,
                       sor_inner_max=8)
     assert obs_b["sor_iterations"][10:].sum() < obs_a["sor_iterations"][10:].sum()
