@@ -110,6 +110,7 @@ struct SmoothFast {
     int wt[(kSmoothMaxR + 1) * (kSmoothMaxR + 1)] = {};  // w(|a|, |b|) (-1: none)
     size_t smem = 0;
     int per = 0;               // R = max(A, B, W): the kernel instantiation
+    int xsplit = 1;            // x segments per column tile (the plan's choice)
 };
 
 // Fast-path (fused) buffers.
