@@ -86,18 +86,36 @@ __global__ void k_cell_ranges(int total, int ncells, const unsigned *__restrict_
     for (int c = prev + 1; c <= k; c++) start[c] = s;
 }
 
+// Sorted positions packed with the species: (x, y, z, 1 for a proton, 0 for
+// a neutron), one vector load per partner.
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+    using type = float4;
+};
+template <>
+struct Vec4<double> {
+    using type = double4;
+};
+
 template <typename T>
 __global__ void k_sorted_positions(int total, int protons, const int *__restrict__ idx, const T *__restrict__ x,
-                                   const T *__restrict__ y, const T *__restrict__ z, T *sx, T *sy, T *sz,
-                                   unsigned char *proton) {
+                                   const T *__restrict__ y, const T *__restrict__ z, typename Vec4<T>::type *sp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= total) return;
     const int i = idx[s];
-    sx[s] = x[i];
-    sy[s] = y[i];
-    sz[s] = z[i];
-    proton[s] = i < protons;
+    typename Vec4<T>::type v;
+    v.x = x[i];
+    v.y = y[i];
+    v.z = z[i];
+    v.w = i < protons ? T(1) : T(0);
+    sp[s] = v;
 }
+
+// exp(-d2 * e): in float as exp2f(d2 * c) with c = -e log2(e), in double exp.
+__device__ __forceinline__ float gauss(float d2, float e, float c) { return exp2f(d2 * c); }
+__device__ __forceinline__ double gauss(double d2, double e, double) { return exp(-d2 * e); }
 
 // Sums over the cells that the cutoff sphere of particle s (sorted order)
 // reaches, results to the particle's own slot.  Per (x, y) row of cells, only
@@ -105,13 +123,13 @@ __global__ void k_sorted_positions(int total, int protons, const int *__restrict
 // contiguous slot range); reach is the cutoff radius with a margin for the
 // rounding of d^2 in T, whose test decides.
 template <typename T>
-__global__ void k_pair_densities(int total, Cells cl, double edge, double reach, T exp_term, T cutoff, T term,
-                                 const int *__restrict__ idx, const int *__restrict__ start, const T *__restrict__ sx,
-                                 const T *__restrict__ sy, const T *__restrict__ sz,
-                                 const unsigned char *__restrict__ proton, T *dp, T *dn) {
+__global__ void k_pair_densities(int total, Cells cl, double edge, double reach, T exp_term, T exp2_term, T cutoff,
+                                 T term, const int *__restrict__ idx, const int *__restrict__ start,
+                                 const typename Vec4<T>::type *__restrict__ sp, T *dp, T *dn) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= total) return;
-    const T xi = sx[s], yi = sy[s], zi = sz[s];
+    const typename Vec4<T>::type me = sp[s];
+    const T xi = me.x, yi = me.y, zi = me.z;
     const double px = (double)xi, py = (double)yi, pz = (double)zi, r2 = reach * reach;
     const int x0 = cell_axis(px - reach, cl.lo[0], cl.inv, cl.n[0]), x1 = cell_axis(px + reach, cl.lo[0], cl.inv, cl.n[0]);
     const int y0 = cell_axis(py - reach, cl.lo[1], cl.inv, cl.n[1]), y1 = cell_axis(py + reach, cl.lo[1], cl.inv, cl.n[1]);
@@ -129,12 +147,13 @@ __global__ void k_pair_densities(int total, Cells cl, double edge, double reach,
             const int row = (ix * cl.n[1] + iy) * cl.n[2];
             const int j0 = start[row + z0], j1 = start[row + z1 + 1];
             for (int j = j0; j < j1; j++) {
-                const T ex = xi - sx[j], ey = yi - sy[j], ez = zi - sz[j];
+                const typename Vec4<T>::type o = sp[j];
+                const T ex = xi - o.x, ey = yi - o.y, ez = zi - o.z;
                 const T d2 = ex * ex + ey * ey + ez * ez;
                 if (d2 > cutoff) continue;
-                const T f = exp(-d2 * exp_term);
-                if (proton[j]) a += f;
-                else b += f;
+                const T f = gauss(d2, exp_term, exp2_term);
+                a += o.w * f;        // protons
+                b += f - o.w * f;    // neutrons
             }
         }
     }
@@ -185,8 +204,7 @@ hv_status particle_densities_at(hv_ctx *c, int N, int protons, const T *px, cons
     // sort particles by cell
     unsigned *keys = nullptr, *keys2 = nullptr;
     int *idx = nullptr, *idx2 = nullptr, *start = nullptr;
-    T *sx = nullptr, *sy = nullptr, *sz = nullptr;
-    unsigned char *pr = nullptr;
+    typename Vec4<T>::type *sp = nullptr;
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
     int bits = 1;
@@ -197,23 +215,21 @@ hv_status particle_densities_at(hv_ctx *c, int N, int protons, const T *px, cons
     HV_CUDA(cudaMallocAsync((void **)&idx, sizeof(int) * N, s));
     HV_CUDA(cudaMallocAsync((void **)&idx2, sizeof(int) * N, s));
     HV_CUDA(cudaMallocAsync((void **)&start, sizeof(int) * (ncells + 1), s));
-    HV_CUDA(cudaMallocAsync((void **)&sx, sizeof(T) * N, s));
-    HV_CUDA(cudaMallocAsync((void **)&sy, sizeof(T) * N, s));
-    HV_CUDA(cudaMallocAsync((void **)&sz, sizeof(T) * N, s));
-    HV_CUDA(cudaMallocAsync((void **)&pr, N, s));
+    HV_CUDA(cudaMallocAsync((void **)&sp, sizeof(typename Vec4<T>::type) * N, s));
     HV_CUDA(cudaMallocAsync(&tmp, tmp_bytes, s));
     k_cell_of<T><<<nb(N), kBlock, 0, s>>>(N, cl, px, py, pz, keys, idx);
     HV_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, idx, idx2, N, 0, bits, s));
     k_cell_ranges<<<nb(N + 1), kBlock, 0, s>>>(N, ncells, keys2, start);
-    k_sorted_positions<T><<<nb(N), kBlock, 0, s>>>(N, protons, idx2, px, py, pz, sx, sy, sz, pr);
+    k_sorted_positions<T><<<nb(N), kBlock, 0, s>>>(N, protons, idx2, px, py, pz, sp);
     const T sr = T(sig);
     const T exp_term = T(1.0) / (T(2.0) * sr * sr), cutoff = T(16.0) * sr * sr;
+    const T exp2_term = T(-1.4426950408889634) * exp_term;  // -log2(e) / (2 sigma_r^2)
     const T term = (T(1.0) / c->params.part_per_nucleon) * (T(1.0) / std::pow(T(2.0) * T(kPi) * sr * sr, T(1.5)));
     const double reach = 4.0 * sig * (1.0 + 1e-5);
-    k_pair_densities<T><<<nb(N), kBlock, 0, s>>>(N, cl, edge, reach, exp_term, cutoff, term, idx2, start, sx, sy, sz, pr, dp_dev,
+    k_pair_densities<T><<<nb(N), kBlock, 0, s>>>(N, cl, edge, reach, exp_term, exp2_term, cutoff, term, idx2, start, sp, dp_dev,
                                                  dn_dev);
     HV_CUDA(cudaGetLastError());
-    void *bufs[] = {keys, keys2, idx, idx2, start, sx, sy, sz, pr, tmp};
+    void *bufs[] = {keys, keys2, idx, idx2, start, sp, tmp};
     for (void *p : bufs) HV_CUDA(cudaFreeAsync(p, s));
     return HV_OK;
 }
