@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-init", action="store_true", help="skip the initialisation legs (densities, loop)")
     ap.add_argument("--no-extrap", action="store_true", help="skip the other warm start's comparison run")
+    ap.add_argument("--no-sorted", action="store_true", help="skip the deterministic sorted-deposit runs")
     ap.add_argument("--batch-steps", type=int, default=16)
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--cpu-sample", action="store_true", help=argparse.SUPPRESS)
@@ -446,6 +447,36 @@ def batched(args, local, world=1, rank=0):
     return out
 
 
+def sorted_deposit_leg(args, w, prec, parts, local, K, W):
+    """The same workload with the deterministic sort-by-cell deposit
+    (HV_DEPOSIT_SORTED): its throughput over K steps, and whether two runs give
+    bit-identical D(t)."""
+    import numpy as np
+    import torch
+    from dataclasses import replace
+
+    import hv_b200 as hv
+    ws = replace(w, deposit_mode=hv.HV_DEPOSIT_SORTED)
+    dips, ms = [], None
+    for rep in range(2):
+        with hv.Session.from_workload(ws, prec, device=local) as s:
+            s.upload_particles(*parts)
+            s.run(W, hv.HV_PATH_FUSED)
+            st = torch.cuda.ExternalStream(s.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            o = s.run(K, hv.HV_PATH_FUSED)
+            e1.record(st)
+            e1.synchronize()
+            if rep == 0:
+                ms = e0.elapsed_time(e1)
+            dips.append(np.array(o["dipole"]))
+    return {"value": w.particles * K / (ms / 1e3), "ms_per_step": ms / K,
+            "deterministic": bool(np.array_equal(dips[0], dips[1])),
+            "note": "sort-by-cell deposit, nodes summed in particle-slot order; two runs compared bit for bit"}
+
+
 # ---------------------------------------------------------------- GPU arm
 def our_arm(args, world, rank, local):
     import numpy as np
@@ -562,6 +593,8 @@ def our_arm(args, world, rank, local):
     }
     if extrap:
         line["warm_start_previous" if other == hv.HV_WARM_PREVIOUS else "warm_start_extrapolate"] = extrap
+    if not args.no_sorted:
+        line["deposit_sorted"] = sorted_deposit_leg(args, w, prec, parts, local, K, W)
 
     if not args.no_e2e:
         pinned = [torch.from_numpy(p.copy()).pin_memory() for p in parts]

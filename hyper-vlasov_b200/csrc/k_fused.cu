@@ -121,6 +121,7 @@ struct PArgs {
     const T *F4;
     T *rho_raw;
     T h, fd, dp, dn;
+    int deposit;  // 1: atomic CIC deposit of x_{n+1} here; 0: the sorted deposit follows
     const int *ctl;
     double *obs;  // [kRing][blocks][6]
 };
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(kPBlock) k_particle_step(PArgs<T> a) {
         a.kx[i] = qx;
         a.ky[i] = qy;
         a.kz[i] = qz;
-        deposit_at<T>(a.g, a.rho_raw, off, px, py, pz);
+        if (a.deposit) deposit_at<T>(a.g, a.rho_raw, off, px, py, pz);
     }
     // deterministic block reduction of the six sums
     __shared__ double sh[6][kPBlock / 32];
@@ -354,7 +355,8 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     const Geom &g = c->geom;
     const hv_run_params &p = c->params;
     int *ctl = ctl_of(c);
-    HV_CUDA(cudaMemsetAsync(s.rho_raw, 0, sizeof(T) * 2 * g.G, c->stream));
+    const bool sorted = p.deposit_mode == HV_DEPOSIT_SORTED;
+    if (!sorted) HV_CUDA(cudaMemsetAsync(s.rho_raw, 0, sizeof(T) * 2 * g.G, c->stream));
     PArgs<T> a;
     a.g = g;
     a.protons = c->protons;
@@ -372,6 +374,7 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     const T zz = T(p.z), nn = T(p.n), e = T(p.eta_exc);
     a.dp = e * nn / (zz + nn);
     a.dn = e * zz / (zz + nn);
+    a.deposit = sorted ? 0 : 1;
     a.ctl = ctl;
     a.obs = f.obs_partials;
     if (c->total > 0) {
@@ -381,6 +384,13 @@ hv_status enqueue_phase_a(hv_ctx *c) {
         HV_CUDA(cudaMemsetAsync(f.obs_partials, 0, sizeof(double) * kRing * f.obs_blocks * 6, c->stream));
     }
     HV_CUDA(cudaGetLastError());
+    // deterministic mode: every node sums its particles in slot order
+    // (distribute_volumetric_particles_cic's single-thread order when the
+    // slots are not permuted)
+    if (sorted) {
+        ProfScope ps(c, HV_K_PARTICLE);
+        HV_TRY(launch_deposit_sorted<T>(c, s.x, s.y, s.z, s.rho_raw));
+    }
     {
         ProfScope ps(c, HV_K_SMOOTH);
         if (sizeof(T) == 4 && f.smooth.ok)
@@ -438,7 +448,10 @@ hv_status initial_typed(hv_ctx *c) {
     const Geom &g = c->geom;
     const hv_run_params &p = c->params;
     int *ctl = ctl_of(c);
-    HV_TRY(launch_deposit_atomic<T>(c, s.x, s.y, s.z, s.rho_raw));
+    if (p.deposit_mode == HV_DEPOSIT_SORTED)
+        HV_TRY(launch_deposit_sorted<T>(c, s.x, s.y, s.z, s.rho_raw));
+    else
+        HV_TRY(launch_deposit_atomic<T>(c, s.x, s.y, s.z, s.rho_raw));
     if (sizeof(T) == 4 && f.smooth.ok)
         HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho)));
     else

@@ -263,3 +263,47 @@ def test_fused_smoothing_matches_direct_sum(hv, wname):
     e_fast, e_direct = max_rel(fast, ref), max_rel(direct, ref)
     assert e_fast < 5e-6
     assert e_fast <= 2 * e_direct + 1e-7
+
+
+def test_fused_f32_104k_dipole_and_spectrum_match_double_oracle(hv):
+    """208Pb with 104,000 test particles on 64^3 at h = 0.5 fm, dt 0.25 fm/c:
+    the FP32 fused path (default solve) against the FP64 oracle over 120
+    steps -- D(t) within 1e-3 of the oracle's largest |D|, and the strength
+    function S(E) of the two D(t) series (detrended, cos^2-windowed FFT as the
+    reference's post-processing, scripts/programs.py:82-122) within 1e-3 of
+    the oracle's largest |S|."""
+    import os
+    from hv_b200.spectrum import energy_spectrum
+    w = hv.PB208_104K
+    steps = 120
+    p32 = hv.workload_particles(w, np.float32)
+    from hv_oracle import Oracle
+    o = Oracle(np.float64)
+    o.set_threads(os.cpu_count() or 4)
+    a = [p.astype(np.float64) for p in p32]
+    obs_o, _ = o.simulate(w.world_tuple(), _oracle_runspec(w), w.protons, w.neutrons, *a, steps)
+    obs, _ = _fused(hv, w, steps, hv.HV_F32, p32)
+    assert not np.any(obs["flags"] & 1)
+    assert max_rel(obs["dipole"], obs_o["dipole"]) <= 1e-3
+    t_f = steps * w.dt
+    eo, so = energy_spectrum(obs_o["t"], obs_o["zcm_p"], obs_o["zcm_n"], w.Z, w.N, t_f, w.dt, w.eta)
+    eg, sg = energy_spectrum(obs["t"], obs["zcm_p"], obs["zcm_n"], w.Z, w.N, t_f, w.dt, w.eta)
+    assert np.allclose(eg, eo)
+    assert max_rel(sg, so) <= 1e-3
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_fused_sorted_deposit_is_deterministic(hv, prec):
+    """HV_DEPOSIT_SORTED on the fused path: every node sums its particles in
+    slot order, so two runs give bit-identical D(t) and particles (the atomic
+    deposit's summation order varies run to run); the two modes agree to the
+    float rounding of the deposit."""
+    dt = np.float32 if prec == "f32" else np.float64
+    P = hv.HV_F32 if prec == "f32" else hv.HV_F64
+    w = replace(hv.CA40_SMALL, deposit_mode=hv.HV_DEPOSIT_SORTED)
+    p = hv.workload_particles(w, dt)
+    runs = [_fused(hv, w, 30, P, p) for _ in range(2)]
+    assert np.array_equal(runs[0][0]["dipole"], runs[1][0]["dipole"])
+    assert all(np.array_equal(a, b) for a, b in zip(runs[0][1], runs[1][1]))
+    obs_a, _ = _fused(hv, replace(w, deposit_mode=hv.HV_DEPOSIT_ATOMIC), 30, P, p)
+    assert max_rel(runs[0][0]["dipole"], obs_a["dipole"]) < (1e-5 if prec == "f32" else 1e-10)
