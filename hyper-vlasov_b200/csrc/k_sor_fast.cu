@@ -63,7 +63,6 @@ struct SorArgs {
     int nx, ny, nz, nz2, P, R, bxn, byn, nblocks, src_smem, vec4;
     int nq_shift;           // log2(nz2 / 4) when a power of two, else -1
     u64 *tmirror;           // tagged mirror [x][colour][y][nz2]: value bits | half-sweep << 32
-    S hx2i, hy2i, hz2i, inv_diag, omega;
     S cx, cy, cz, cself;    // omega h^-2 / diag per axis, 1 - omega: the update's coefficients
     double dhx2i, dhy2i, dhz2i, ddiag, src_c;
     double src_scale;       // omega / diag: the residual is stored pre-scaled
@@ -1231,11 +1230,6 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.dhy2i = 1.0 / (dy * dy);
     a.dhz2i = 1.0 / (dz * dz);
     a.ddiag = 2.0 * (a.dhx2i + a.dhy2i + a.dhz2i);
-    a.hx2i = (S)a.dhx2i;
-    a.hy2i = (S)a.dhy2i;
-    a.hz2i = (S)a.dhz2i;
-    a.inv_diag = (S)(1.0 / a.ddiag);
-    a.omega = (S)sp.omega;
     a.cx = (S)(sp.omega * a.dhx2i / a.ddiag);
     a.cy = (S)(sp.omega * a.dhy2i / a.ddiag);
     a.cz = (S)(sp.omega * a.dhz2i / a.ddiag);
