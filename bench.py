@@ -18,6 +18,17 @@ Our arm (default) prints one JSON line with:
   kernels      per-kernel device time, share and algorithmic GB/s
   plain_f64    the plain FP64 drop-in (one kernel per reference routine,
                host-tested SOR) on the same workload, and the D(t) agreement
+  warm_start_previous
+               the same steps with each SOR started from the previous step's
+               phi (the reference's guess) instead of 2 phi_n - phi_(n-1)
+  deposit_sorted
+               the deterministic sort-by-cell deposit: throughput and whether
+               two runs give bit-identical D(t)
+  adjoint      gradient of the D(t)-spectrum objective: cost against a forward run
+  particle_densities, initialisation
+               the Woods-Saxon initialisation loop and its per-particle
+               densities on the device, against the reference's routines
+  batched      64 independent runs advanced together (sharded over ranks)
   cpu_baseline the reference's own routines on the host cores (rank 0, N=1)
 
 --impl reference times the reference's CPU step routines (compiled from its
