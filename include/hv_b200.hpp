@@ -74,6 +74,16 @@ struct Skyrme {
     T A, B, C, gamma;
 };
 
+template <typename T>
+struct WoodsSaxon {
+    T V0, R12, a;
+};
+
+template <typename T>
+struct Fermi {
+    T epsilon_p, epsilon_n;
+};
+
 constexpr int PROTONS = 0;   // include/sim_structs.hpp:28
 constexpr int NEUTRONS = 1;  // include/sim_structs.hpp:29
 
@@ -376,6 +386,138 @@ void gpu_simulate(const char *output_directory, TestParticles<T> *part, const Sk
             std::fprintf(stats, "%e %e %e %e %e\n", (double)(T(s) * T(p.dt)), rows[s].rms_p, rows[s].rms_n,
                          rows[s].zcm_p, rows[s].zcm_n);
     std::fclose(stats);
+}
+
+// ---- the initialisation -------------------------------------------------
+
+namespace detail {
+
+// A context holding only particles (the routines below use no grid).
+template <typename T>
+hv_ctx *particle_context(int protons, int neutrons, const hv_run_params &p) {
+    World<T> w;
+    for (int a = 0; a < 3; a++) {
+        w.n[a] = 8;
+        w.d_max[a] = T(1);
+    }
+    return context(w, protons, neutrons, p);
+}
+
+template <typename T>
+hv_run_params init_params(const Parameters<T> &param, const Skyrme<T> *skm) {
+    hv_run_params p = base_params();
+    p.z = param.z;
+    p.n = param.n;
+    p.part_per_nucleon = param.part_per_nucleon;
+    p.sigma_r = (double)param.sigma_r;
+    if (skm) p.skyrme = {(double)skm->A, (double)skm->B, (double)skm->C, (double)skm->gamma};
+    return p;
+}
+
+template <typename T>
+void to_ws(const WoodsSaxon<T> *ws, hv_woods_saxon *o) {
+    for (int q = 0; q < 2; q++) o[q] = {(double)ws[q].V0, (double)ws[q].R12, (double)ws[q].a};
+}
+
+template <typename T>
+void from_ws(const hv_woods_saxon *o, WoodsSaxon<T> *ws) {
+    for (int q = 0; q < 2; q++) {
+        ws[q].V0 = T(o[q].V0);
+        ws[q].R12 = T(o[q].R12);
+        ws[q].a = T(o[q].a);
+    }
+}
+
+}  // namespace detail
+
+// include/tools.hpp:170-203: part->density_p / density_n from the positions
+template <typename T>
+void compute_particle_densities(TestParticles<T> *part, const Parameters<T> &param) {
+    hv_ctx *c = detail::particle_context<T>(part->protons, part->neutrons, detail::init_params<T>(param, nullptr));
+    detail::check(hv_upload_particles(c, part->x, part->y, part->z, nullptr, nullptr, nullptr), "upload");
+    detail::check(hv_particle_densities(c, part->density_p, part->density_n), "hv_particle_densities");
+}
+
+// include/tools.hpp:226-232: part->energy
+template <typename T>
+void compute_particle_energies(TestParticles<T> *part, const WoodsSaxon<T> *ws, const Parameters<T> &param) {
+    hv_ctx *c = detail::particle_context<T>(part->protons, part->neutrons, detail::init_params<T>(param, nullptr));
+    detail::check(hv_upload_particles(c, part->x, part->y, part->z, part->kx, part->ky, part->kz), "upload");
+    hv_woods_saxon h[2];
+    detail::to_ws(ws, h);
+    detail::check(hv_particle_energies(c, h, (double)param.sigma_k, part->energy), "hv_particle_energies");
+}
+
+// include/fit_algorithm.hpp:95-137: the Woods-Saxon fit of each species, from
+// ws (in/out).  The densities are recomputed from the positions, as the
+// loop's preceding compute_particle_densities gives them; the fit restates
+// GSL's driver as Levenberg-Marquardt (hv_fit_woods_saxon).  param supplies
+// Z, N, part_per_nucleon and sigma_r (the reference's signature has none:
+// its densities come with the particles).
+template <typename T>
+void minim_woods_saxon(TestParticles<T> *part, WoodsSaxon<T> *ws, Skyrme<T> skm, const Parameters<T> &param) {
+    hv_ctx *c = detail::particle_context<T>(part->protons, part->neutrons, detail::init_params<T>(param, &skm));
+    detail::check(hv_upload_particles(c, part->x, part->y, part->z, nullptr, nullptr, nullptr), "upload");
+    hv_woods_saxon h[2];
+    detail::to_ws(ws, h);
+    detail::check(hv_fit_woods_saxon(c, nullptr, h, nullptr, nullptr), "hv_fit_woods_saxon");
+    detail::from_ws(h, ws);
+}
+
+// include/physics.hpp:34-97: allocates part (as create_particles,
+// include/init.hpp:133-157: free with the reference's free_particles) and
+// fills it with the loop's final particles, their densities and energies;
+// ws and fermi_levels receive the final parameters.  The candidates are drawn
+// from rand() in the reference's order, so after the same srand() the run is
+// the reference's (with the fit restated, GSL being absent).  Prints the
+// reference's per-pass lines and its warning when the loop does not converge.
+template <typename T>
+void initialize_particles(TestParticles<T> *part, WoodsSaxon<T> *ws, const Skyrme<T> &skm, Fermi<T> *fermi_levels,
+                          const Parameters<T> &param) {
+    const int total_p = param.z * param.part_per_nucleon, total_n = param.n * param.part_per_nucleon;
+    const int total = total_p + total_n;
+    hv_ctx *c = detail::particle_context<T>(total_p, total_n, detail::init_params<T>(param, &skm));
+    hv_woods_saxon h[2];
+    detail::to_ws(ws, h);
+    hv_fermi f = {(double)fermi_levels->epsilon_p, (double)fermi_levels->epsilon_n};
+    hv_init_params ip;
+    hv_init_params_default(&ip);
+    ip.sigma_k = (double)param.sigma_k;
+    ip.r_max = (double)param.r_max;
+    ip.max_test_part = param.max_test_part;
+    ip.rng = HV_RNG_LIBC;
+    hv_init_report rep;
+    std::vector<hv_init_row> rows(32);
+    detail::check(hv_initialize_particles(c, nullptr, h, &f, &ip, &rep, rows.data()), "hv_initialize_particles");
+    for (int it = 0; it < rep.iterations; it++) {  // include/physics.hpp:84-90
+        const hv_init_row &r = rows[it];
+        std::printf("---------------------------\n");
+        std::printf("EQUAL P %i EQUAL N %i\n", r.equal_p, r.equal_n);
+        for (int q = 0; q < 2; q++) std::printf("V0 %0.2lf R12 %0.2lf a %0.2lf\n", r.ws[q].V0, r.ws[q].R12, r.ws[q].a);
+        std::printf("FERMI P %0.2lf FERMI N %0.2lf\n", r.epsilon_p, r.epsilon_n);
+        std::printf("DELTA EPSILON %0.2lf\nITERATION %i\n", r.delta_epsilon, it + 1);
+    }
+    if (!rep.converged) std::fprintf(stderr, "INITIALIZATION DID NOT CONVERGE!\n");
+    part->protons = total_p;
+    part->neutrons = total_n;
+    T **arrays[12] = {&part->x, &part->y, &part->z, &part->kx, &part->ky, &part->kz,
+                      &part->fx, &part->fy, &part->fz, &part->energy, &part->density_p, &part->density_n};
+    for (T **a : arrays) {
+        *a = (T *)std::malloc((size_t)(total > 0 ? total : 1) * sizeof(T));
+        if (!*a) {
+            std::fprintf(stderr, "ERROR ALLOCATING MEMORY!\n");
+            std::exit(1);
+        }
+    }
+    detail::check(hv_download_particles(c, part->x, part->y, part->z, part->kx, part->ky, part->kz), "download");
+    detail::check(hv_particle_densities(c, part->density_p, part->density_n), "hv_particle_densities");
+    detail::check(hv_particle_energies(c, h, (double)param.sigma_k, part->energy), "hv_particle_energies");
+    std::memset(part->fx, 0, sizeof(T) * total);
+    std::memset(part->fy, 0, sizeof(T) * total);
+    std::memset(part->fz, 0, sizeof(T) * total);
+    detail::from_ws(h, ws);
+    fermi_levels->epsilon_p = T(f.epsilon_p);
+    fermi_levels->epsilon_n = T(f.epsilon_n);
 }
 
 }  // namespace hvb200

@@ -15,10 +15,13 @@ SRC = os.path.join(ROOT, "tests", "cpp", "dropin_main.cpp")
 LIBDIR = os.path.join(ROOT, "hyper-vlasov_b200", "hv_b200", "lib")
 
 
-def build(tmp):
-    exe = os.path.join(tmp, "dropin_main")
+INIT_SRC = os.path.join(ROOT, "tests", "cpp", "init_main.cpp")
+
+
+def build(tmp, src=SRC):
+    exe = os.path.join(tmp, os.path.splitext(os.path.basename(src))[0])
     gxx = shutil.which("g++") or "/usr/bin/g++"
-    cmd = [gxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), SRC, "-o", exe,
+    cmd = [gxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"), src, "-o", exe,
            "-L", LIBDIR, "-lhv_b200", f"-Wl,-rpath,{LIBDIR}"]
     env = dict(os.environ)
     env.pop("CXX", None)
@@ -30,6 +33,35 @@ def build(tmp):
 def test_dropin_header_compiles_and_links(hv, tmp_path):
     exe = build(str(tmp_path))
     assert os.path.exists(exe)
+    assert os.path.exists(build(str(tmp_path), INIT_SRC))
+
+
+@pytest.mark.gpu
+def test_dropin_initialize_particles_matches_the_reference_loop(hv, golden, tmp_path):
+    """hvb200::initialize_particles after srand(128), with the reference's
+    call shape, against the golden run of the reference's own loop (its fit
+    restated): the same particles to 1e-12, Woods-Saxon parameters and Fermi
+    levels to 1e-9, densities and energies of the final particles."""
+    g = golden("init_ca40_f64.npz")
+    exe = build(str(tmp_path), INIT_SRC)
+    out = os.path.join(str(tmp_path), "init.bin")
+    ws0, fe0, sk = g["ws0"], g["fermi0"], g["skyrme"]
+    args = [exe, out] + [str(v) for v in (int(g["Z"]), int(g["N"]), int(g["ppn"]))] + \
+        [repr(float(g["sigma_k"])), repr(float(g["sigma_r"])), repr(float(g["r_max"])), str(int(g["max_test_part"])),
+         str(int(g["seed"]))] + [repr(float(v)) for v in sk] + [repr(float(v)) for v in ws0.ravel()] + \
+        [repr(float(v)) for v in fe0]
+    r = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.count("ITERATION") == int(g["passes"])
+    data = np.fromfile(out, dtype=np.float64)
+    total = (int(g["Z"]) + int(g["N"])) * int(g["ppn"])
+    assert data.size == 8 + 9 * total
+    assert np.allclose(data[:6], g["ws"].ravel(), rtol=1e-9, atol=0)
+    assert np.allclose(data[6:8], g["fermi"], rtol=1e-9, atol=0)
+    arrs = data[8:].reshape(9, total)
+    for a, k in zip(arrs, ("x", "y", "z", "kx", "ky", "kz", "density_p", "density_n", "energy")):
+        tol = 1e-12 if k in ("x", "y", "z", "kx", "ky", "kz") else 1e-9
+        assert np.max(np.abs(a - g[k])) <= tol * np.abs(g[k]).max(), k
 
 
 @pytest.mark.gpu
