@@ -621,6 +621,13 @@ def our_arm(args, world, rank, local):
                        "d2h_bytes_per_step": (6 * w.particles * es + obs_e.nbytes) / K,
                        "includes": "context creation, upload, initial solve, K steps, download (hv_simulate)"}
 
+    # the last leg with collectives, before the legs that rank 0 runs alone (so
+    # that no rank waits on those at a barrier)
+    if not args.no_batch:
+        bl = batched(args, local, world, rank)  # every rank takes part (its share of the runs)
+        if rank == 0:
+            line["batched"] = bl
+
     if not args.no_plain and rank == 0:
         # the plain FP64 drop-in: per-routine kernels, SOR tested on the host
         p64 = [p.astype(np.float64) for p in parts]
@@ -651,10 +658,6 @@ def our_arm(args, world, rank, local):
     if not args.no_init and rank == 0:
         line["particle_densities"] = particle_densities_cost(args, local, world)
         line["initialisation"] = initialisation_cost(args, local, world)
-    if not args.no_batch:
-        bl = batched(args, local, world, rank)  # every rank takes part (its share of the runs)
-        if rank == 0:
-            line["batched"] = bl
 
     if not args.no_cpu and rank == 0 and world == 1:
         try:
