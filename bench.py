@@ -20,7 +20,7 @@ Our arm (default) prints one JSON line with:
                host-tested SOR) on the same workload, and the D(t) agreement
   warm_start_previous
                the same steps with each SOR started from the previous step's
-               phi (the reference's guess) instead of 2 phi_n - phi_(n-1)
+               phi (the reference's guess) instead of 3 phi_n - 3 phi_(n-1) + phi_(n-2)
   deposit_sorted
                the deterministic sort-by-cell deposit: throughput and whether
                two runs give bit-identical D(t)
@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="208Pb-2.08M-128^3")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
-    ap.add_argument("--warm-start", choices=["previous", "extrapolate"], default="extrapolate")
+    ap.add_argument("--warm-start", choices=["previous", "extrapolate", "quadratic"], default="quadratic")
     ap.add_argument("--sor-exchange", choices=["auto", "flags"], default="auto")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -498,7 +498,8 @@ def our_arm(args, world, rank, local):
     prec = hv.HV_F32 if args.precision == "f32" else hv.HV_F64
     dt = np.float32 if prec == hv.HV_F32 else np.float64
     K, W = args.steps, max(3, args.warmup)
-    warm_mode = hv.HV_WARM_EXTRAPOLATE if args.warm_start == "extrapolate" else hv.HV_WARM_PREVIOUS
+    warm_mode = {"previous": hv.HV_WARM_PREVIOUS, "extrapolate": hv.HV_WARM_EXTRAPOLATE,
+                 "quadratic": hv.HV_WARM_QUADRATIC}[args.warm_start]
     parts = hv.workload_particles(w, dt)
     torch.cuda.set_device(local)
 
@@ -564,7 +565,7 @@ def our_arm(args, world, rank, local):
     # the same K steps from the other initial guess of the solve (the
     # reference's: the previous step's phi), same stopping rule, for comparison
     extrap = None
-    other = hv.HV_WARM_PREVIOUS if warm_mode == hv.HV_WARM_EXTRAPOLATE else hv.HV_WARM_EXTRAPOLATE
+    other = hv.HV_WARM_PREVIOUS if warm_mode != hv.HV_WARM_PREVIOUS else hv.HV_WARM_QUADRATIC
     if not args.no_extrap:
         with hv.Session.from_workload(w, prec, device=local) as sx:
             sx.set_fast_options(sor_warm_start=other)
@@ -584,7 +585,7 @@ def our_arm(args, world, rank, local):
                   "dipole_max_rel_diff_vs_headline": float(np.max(np.abs(obs_x["dipole"] - obs["dipole"])) / dref)
                   if dref > 0 else None,
                   "note": ("SOR started from the previous step's phi (the reference's guess)"
-                           if other == hv.HV_WARM_PREVIOUS else "SOR started from 2 phi_n - phi_(n-1)") +
+                           if other == hv.HV_WARM_PREVIOUS else "SOR started from 3 phi_n - 3 phi_(n-1) + phi_(n-2)") +
                           ", same stopping rule"}
 
     line = {
@@ -603,7 +604,7 @@ def our_arm(args, world, rank, local):
         "clocks": clk.summary(),
     }
     if extrap:
-        line["warm_start_previous" if other == hv.HV_WARM_PREVIOUS else "warm_start_extrapolate"] = extrap
+        line["warm_start_previous" if other == hv.HV_WARM_PREVIOUS else "warm_start_quadratic"] = extrap
     if not args.no_sorted:
         line["deposit_sorted"] = sorted_deposit_leg(args, w, prec, parts, local, K, W)
 

@@ -729,7 +729,7 @@ hv_status hv_observe(hv_ctx *c, hv_observables *out) {
 
 void hv_fast_options_default(hv_fast_options *o) {
     if (!o) return;
-    o->sor_warm_start = HV_WARM_EXTRAPOLATE;
+    o->sor_warm_start = HV_WARM_QUADRATIC;
     o->sor_inner_min = 2;
     o->sor_inner_max = 256;
     o->sort_every = 16;
@@ -739,7 +739,9 @@ void hv_fast_options_default(hv_fast_options *o) {
 
 hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
     if (!c || !o) return HV_ERR_BAD_ARG;
-    if (o->sor_warm_start != HV_WARM_PREVIOUS && o->sor_warm_start != HV_WARM_EXTRAPOLATE) return HV_ERR_BAD_ARG;
+    if (o->sor_warm_start != HV_WARM_PREVIOUS && o->sor_warm_start != HV_WARM_EXTRAPOLATE &&
+        o->sor_warm_start != HV_WARM_QUADRATIC)
+        return HV_ERR_BAD_ARG;
     if (o->sor_inner_min < 1 || o->sor_inner_max < o->sor_inner_min || o->sor_inner_max > 4096) return HV_ERR_BAD_ARG;
     if (o->sort_every < 0 || o->graph_steps < 0 || o->graph_steps > 64) return HV_ERR_BAD_ARG;
     if (o->sor_exchange != HV_SOR_EXCHANGE_AUTO && o->sor_exchange != HV_SOR_EXCHANGE_FLAGS) return HV_ERR_BAD_ARG;

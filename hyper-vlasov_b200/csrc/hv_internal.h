@@ -118,6 +118,7 @@ struct Fused {
     bool ready = false;
     double *phi64 = nullptr;      // Coulomb potential (double for every precision)
     double *phi64_prev = nullptr; // previous step's phi (extrapolated warm start)
+    double *phi64_prev2 = nullptr; // the step before's (quadratic extrapolation)
     void *F4 = nullptr;           // interleaved forces, 4 x T per node
     double *obs_partials = nullptr;  // per-step observable partials
     int obs_blocks = 0;

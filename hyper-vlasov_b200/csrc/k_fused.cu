@@ -655,8 +655,10 @@ hv_status fused_prepare(hv_ctx *c) {
     const size_t es = c->prec == HV_F64 ? 8 : 4;
     HV_CUDA(cudaMalloc((void **)&f.phi64, sizeof(double) * g.G));
     HV_CUDA(cudaMalloc((void **)&f.phi64_prev, sizeof(double) * g.G));
+    HV_CUDA(cudaMalloc((void **)&f.phi64_prev2, sizeof(double) * g.G));
     HV_CUDA(cudaMemsetAsync(f.phi64, 0, sizeof(double) * g.G, c->stream));
     HV_CUDA(cudaMemsetAsync(f.phi64_prev, 0, sizeof(double) * g.G, c->stream));
+    HV_CUDA(cudaMemsetAsync(f.phi64_prev2, 0, sizeof(double) * g.G, c->stream));
     HV_CUDA(cudaMalloc(&f.F4, es * 4 * 2 * g.G));
     f.obs_blocks = 4 * c->sm_count;
     HV_CUDA(cudaMalloc((void **)&f.obs_partials, sizeof(double) * kRing * f.obs_blocks * 6));
@@ -678,7 +680,7 @@ hv_status fused_prepare(hv_ctx *c) {
 hv_status fused_release(hv_ctx *c) {
     Fused &f = c->fused;
     if (f.graph) cudaGraphExecDestroy(f.graph);
-    void *ptrs[] = {f.phi64, f.phi64_prev, f.F4, f.obs_partials, f.obs_rows_dev, f.sor_its};
+    void *ptrs[] = {f.phi64, f.phi64_prev, f.phi64_prev2, f.F4, f.obs_partials, f.obs_rows_dev, f.sor_its};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     sor_fast_release(c);

@@ -67,9 +67,10 @@ struct SorArgs {
     double dhx2i, dhy2i, dhz2i, ddiag, src_c;
     double src_scale;       // omega / diag: the residual is stored pre-scaled
     double tol;
-    int max_iter, criterion, inner_min, inner_max, extrapolate;
+    int max_iter, criterion, inner_min, inner_max;
+    int extrapolate;        // initial guess: 0 previous phi, else extrapolation of this order (1, 2)
     const T *rho;
-    double *phi64, *phi64_prev;
+    double *phi64, *phi64_prev, *phi64_prev2;
     S *delta, *src;         // global mirrors, [x][colour][y][nz2]
     double *partials;       // [nblocks][4]: rr, bb, max|ddelta|, -
     unsigned *phase;        // [nblocks]
@@ -855,15 +856,22 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
                 else a.delta[B.mirror(x0 + p, c, y0) + e] = S(0);
             }
     const int step = a.ctl[0];
-    const bool extrap = a.extrapolate && a.ctl[2];
+    // initial guess from the phi of earlier steps (ctl[2]: how many are held)
+    const int hist = a.extrapolate ? a.ctl[2] : 0;
     if (a.extrapolate) {
         for (int e = tid; e < np * nr * nz; e += nth) {
             int k = e % nz, l = e / nz, j = l % nr, p = l / nr;
             int x = x0 + p, y = y0 + j;
             if (y < 1 || y > ny - 2 || k < 1 || k > nz - 2) continue;
             long long id = x * sxy + (long long)y * nz + k;
-            double cur = a.phi64[id];
-            if (extrap) a.phi64[id] = 2.0 * cur - a.phi64_prev[id];
+            // polynomial extrapolation in time of the highest order the history
+            // allows: 2 p0 - p1 (linear), 3 (p0 - p1) + p2 (quadratic).  A cubic
+            // guess measured worse: it amplifies the step-to-step particle noise.
+            const double cur = a.phi64[id], prev = a.phi64_prev[id];
+            const int ord = min(a.extrapolate, hist);
+            if (ord == 2) a.phi64[id] = 3.0 * (cur - prev) + a.phi64_prev2[id];
+            else if (ord == 1) a.phi64[id] = 2.0 * cur - prev;
+            if (a.extrapolate >= 2) a.phi64_prev2[id] = prev;
             a.phi64_prev[id] = cur;
         }
     }
@@ -1052,7 +1060,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         a.status[3] = cycles;
         a.metric[0] = a.criterion == HV_SOR_REL_RESIDUAL ? rel : maxd;
         a.ctl[1] = max(m, a.inner_min);
-        if (a.extrapolate) a.ctl[2] = 1;
+        if (a.extrapolate) a.ctl[2] = min(a.ctl[2] + 1, 2);
         if (a.its_ring) a.its_ring[step % a.ring] = converged ? its : -its;
     }
 }
@@ -1241,10 +1249,12 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.criterion = sp.criterion;
     a.inner_min = c->fast.sor_inner_min;
     a.inner_max = c->fast.sor_inner_max;
-    a.extrapolate = c->fast.sor_warm_start == HV_WARM_EXTRAPOLATE;
+    a.extrapolate = c->fast.sor_warm_start == HV_WARM_EXTRAPOLATE ? 1
+                    : c->fast.sor_warm_start == HV_WARM_QUADRATIC ? 2 : 0;
     a.rho = rho;
     a.phi64 = c->fused.phi64;
     a.phi64_prev = c->fused.phi64_prev;
+    a.phi64_prev2 = c->fused.phi64_prev2;
     a.delta = reinterpret_cast<S *>(f.delta);
     a.tmirror = reinterpret_cast<u64 *>(f.delta);
     a.src = reinterpret_cast<S *>(f.src);

@@ -70,6 +70,7 @@ class hv_fast_options(C.Structure):
 
 HV_WARM_PREVIOUS = 0
 HV_WARM_EXTRAPOLATE = 1
+HV_WARM_QUADRATIC = 2
 HV_SOR_EXCHANGE_AUTO = 0
 HV_SOR_EXCHANGE_FLAGS = 1
 

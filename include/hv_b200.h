@@ -285,15 +285,17 @@ HV_API hv_status hv_observe_noalloc(const hv_world *world, int protons, int neut
 
 /* ---- fused-path options ------------------------------------------------ */
 
-/* SOR starting guess of each step's solve in the fused path (the plain path
+ /* SOR starting guess of each step's solve in the fused path (the plain path
  * always starts from the previous step's phi, as the reference does). */
 typedef enum hv_warm_start {
     HV_WARM_PREVIOUS = 0,    /* the previous step's phi, as the reference does  */
-    HV_WARM_EXTRAPOLATE = 1  /* 2 phi(t) - phi(t - dt) (the default): the same
-                                stopping rule from a closer guess, about half
-                                the iterations; the converged phi differs from
-                                the previous-guess solve within the tolerance
-                                (D(t) by ~1e-9 relative on 208Pb, 2.08 M)     */
+    HV_WARM_EXTRAPOLATE = 1, /* 2 phi(t) - phi(t - dt): the same stopping rule
+                                from a closer guess, about half the iterations */
+    HV_WARM_QUADRATIC = 2    /* 3 phi(t) - 3 phi(t - dt) + phi(t - 2 dt) (the
+                                default): a quarter of the linear guess's
+                                iterations on 208Pb / 2.08 M; the converged phi
+                                differs from the previous-guess solve within
+                                the tolerance (D(t) by ~6e-9 relative)         */
 } hv_warm_start;
 
 /* How the blocks of the fused SOR exchange boundary corrections. */
@@ -313,7 +315,7 @@ typedef struct hv_fast_options {
     int sor_exchange;     /* hv_sor_exchange                                    */
 } hv_fast_options;
 
-/* Defaults: HV_WARM_EXTRAPOLATE, inner 2..256, sort every 16 steps, 8-step graphs,
+/* Defaults: HV_WARM_QUADRATIC, inner 2..256, sort every 16 steps, 8-step graphs,
  * HV_SOR_EXCHANGE_AUTO. */
 HV_API void hv_fast_options_default(hv_fast_options *o);
 HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);

@@ -106,6 +106,12 @@ def test_extrapolated_warm_start_saves_iterations(hv):
                       sor_inner_max=8)
     assert obs_b["sor_iterations"][10:].sum() < obs_a["sor_iterations"][10:].sum()
     assert max_rel(obs_b["dipole"], obs_a["dipole"]) < 1e-3
+    # the quadratic guess 3 phi_n - 3 phi_(n-1) + phi_(n-2) (the default)
+    obs_c, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_QUADRATIC, sor_inner_min=1,
+                      sor_inner_max=8)
+    assert obs_c["sor_iterations"][10:].sum() < obs_b["sor_iterations"][10:].sum()
+    assert max_rel(obs_c["dipole"], obs_a["dipole"]) < 1e-3
+    assert not np.any(obs_c["flags"] & 1)
 
 
 def test_fused_state_and_fields_match_oracle_on_final_positions(hv):
