@@ -730,7 +730,7 @@ hv_status hv_observe(hv_ctx *c, hv_observables *out) {
 void hv_fast_options_default(hv_fast_options *o) {
     if (!o) return;
     o->sor_warm_start = HV_WARM_QUADRATIC;
-    o->sor_inner_min = 2;
+    o->sor_inner_min = 8;
     o->sor_inner_max = 256;
     o->sort_every = 16;
     o->graph_steps = 8;

@@ -93,6 +93,7 @@ struct SorFast {
     bool tables = false;       // shared memory also holds the tagged sweeps' row tables
     void *delta = nullptr;     // SOR correction, colour-split layout
     void *src = nullptr;       // residual source, colour-split layout
+    double *resid = nullptr;   // FP64 residual of phi per grid node, carried between checks
     double *partials = nullptr;
     unsigned *phase = nullptr; // per-block publish counters
     unsigned *bar = nullptr;   // [0] arrivals, [1] generation
@@ -129,7 +130,7 @@ struct Fused {
     int graph_len = 0;
     bool prev_valid = false;      // phi64_prev holds the previous step's phi
     bool f4_current = false;      // F4 holds the forces of the current positions
-    int m_hint = 8;
+    int m_hint = 8;               // iterations of the previous SOR solve (seeds the first cycle)
     SorFast sor;
     SmoothFast smooth;
 };

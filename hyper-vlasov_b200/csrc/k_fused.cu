@@ -20,7 +20,7 @@ namespace hv {
 hv_status sor_fast_plan(hv_ctx *c);
 void sor_fast_release(hv_ctx *c);
 template <typename T>
-hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring);
+hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, bool step_solve);
 hv_status smooth_fast_plan(hv_ctx *c);
 void smooth_fast_release(hv_ctx *c);
 hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho);
@@ -432,7 +432,7 @@ hv_status enqueue_step(hv_ctx *c) {
     HV_TRY(enqueue_phase_a<T>(c));
     {
         ProfScope ps(c, HV_K_SOR);
-        HV_TRY(sor_fast_launch<T>(c, st<T>(c).rho, ctl_of(c), c->fused.sor_its, kRing));
+        HV_TRY(sor_fast_launch<T>(c, st<T>(c).rho, ctl_of(c), c->fused.sor_its, kRing, true));
     }
     return enqueue_phase_c<T>(c);
 }
@@ -468,7 +468,8 @@ hv_status initial_typed(hv_ctx *c) {
     }
     int h_ctl[3] = {c->step_index, f.m_hint, 0};
     HV_CUDA(cudaMemcpyAsync(ctl, h_ctl, sizeof(int) * 3, cudaMemcpyHostToDevice, c->stream));
-    HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, nullptr, kRing));
+    // from phi = 0: neither extrapolated nor recorded as an earlier solution
+    HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, nullptr, kRing, false));
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
     k_forces_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64, reinterpret_cast<T *>(f.F4));

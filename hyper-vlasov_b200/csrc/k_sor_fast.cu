@@ -71,13 +71,14 @@ struct SorArgs {
     int extrapolate;        // initial guess: 0 previous phi, else extrapolation of this order (1, 2)
     const T *rho;
     double *phi64, *phi64_prev, *phi64_prev2;
+    double *resid;          // FP64 residual of phi per node, carried between checks
     S *delta, *src;         // global mirrors, [x][colour][y][nz2]
     double *partials;       // [nblocks][4]: rr, bb, max|ddelta|, -
     unsigned *phase;        // [nblocks]
     unsigned *bar;          // [0] arrivals, [1] generation
     int *status;            // [0] error, [1] iterations, [2] converged, [3] cycles
     double *metric;
-    int *ctl;               // [0] step counter, [1] m hint, [2] previous-phi valid
+    int *ctl;               // [0] step counter, [1] iterations of the previous solve, [2] phi history held
     int *its_ring;          // per-step iterations, indexed by step % ring
     int ring;
     // several solves in one launch: block -> instance, first block of an
@@ -462,6 +463,8 @@ __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cas
 // (off the block's perimeter), which read only this block's shared memory.
 // The fetch's L2 round trip is thus spent under the inner rows' updates.
 constexpr int kGhostThreads = 256;
+// rows of the residual check whose loads one thread issues together
+constexpr int kCheckRows = 2;
 
 // Shared-memory tables behind delta | src, sized by the plan's P x R block.
 struct Staged {
@@ -739,7 +742,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     const int r4_start = nq > 0 ? tid / nq : 0;
     const int q_own = (nq > 0 && r4_start < rows_step4) ? tid % nq : nq;
     const int j4_start = r4_start % nr, p4_start = r4_start / nr, dj4 = rows_step4 % nr, dp4 = rows_step4 / nr;
-    // residual and fold: thread -> z position k_own, rows rz_start, +zrows_step
+    // residual checks: thread -> z position k_own, rows rz_start, +zrows_step
     const int zrows_step = max(1, nth / nz);
     const int rz_start = tid / nz;
     const int k_own = rz_start < zrows_step ? tid % nz : nz;
@@ -763,37 +766,63 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     [[maybe_unused]] GhostQuad ghost[kStaged ? kGhost : 1];
     if constexpr (kStaged) {
         __shared__ int s_nf, s_ng;
-        if (tid == 0) {
+        if (tid < 32) {
             // Perimeter rows and their ghost rows, and (in `order`) the inner
             // rows, each listed by the parity of x + y first: a row's parity
             // fixes which end of its other-colour half-row a quad reads, so
-            // warps whose rows share it take one path.
+            // warps whose rows share it take one path.  Warp 0 lists 32 rows
+            // at a time; ballots and a scan of the ghost counts give each
+            // lane its slots, in row order.
+            const unsigned below = (1u << tid) - 1u;
             int nf = 0, ng = 0, ni = 0;
-            for (int l = 0; l < 2 * np * nr; l++) {
-                const int par = l / (np * nr), lr = l - par * np * nr;
-                const int p = lr / nr, j = lr - p * nr, x = x0 + p, y = y0 + j;
-                if (((x + y) & 1) != par) continue;
-                if (!(p == 0 || p + 1 == np || j == 0 || j + 1 == nr)) {
-                    order[ni++] = (unsigned)p << 16 | (unsigned)j;
-                    continue;
+            for (int base = 0; base < 2 * np * nr; base += 32) {
+                const int l = base + tid;
+                int p = 0, j = 0, x = 0, y = 0;
+                bool sel = false, perim = false;
+                if (l < 2 * np * nr) {
+                    const int par = l / (np * nr), lr = l - par * np * nr;
+                    p = lr / nr;
+                    j = lr - p * nr;
+                    x = x0 + p;
+                    y = y0 + j;
+                    sel = ((x + y) & 1) == par;
+                    perim = p == 0 || p + 1 == np || j == 0 || j + 1 == nr;
                 }
-                const bool active = y >= 1 && y <= ny - 2;
-                unsigned gi[4] = {0xffffu, 0xffffu, 0xffffu, 0xffffu};
+                const bool is_in = sel && !perim, is_f = sel && perim;
+                const bool active = is_f && y >= 1 && y <= ny - 2;
                 const bool need[4] = {active && p == 0 && x - 1 >= 1, active && p + 1 == np && x + 1 <= a.nx - 2,
                                       active && j == 0 && y - 1 >= 1, active && j + 1 == nr && y + 1 <= ny - 2};
-                const int sx[4] = {x - 1, x + 1, x, x}, sy[4] = {y, y, y - 1, y + 1};
-                for (int d = 0; d < 4; d++)
-                    if (need[d]) {
-                        st.gsrc[ng] = (unsigned)(((2ll * sx[d]) * ny + sy[d]) * nz2);
-                        gi[d] = (unsigned)ng++;
-                    }
-                st.ftab[nf] = (unsigned)p << 16 | (unsigned)j;
-                st.fgi[2 * nf] = gi[0] | gi[1] << 16;
-                st.fgi[2 * nf + 1] = gi[2] | gi[3] << 16;
-                nf++;
+                const int cnt = (int)need[0] + (int)need[1] + (int)need[2] + (int)need[3];
+                int inc = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (tid >= o) inc += v;
+                }
+                const unsigned bi = __ballot_sync(0xffffffffu, is_in), bf = __ballot_sync(0xffffffffu, is_f);
+                if (is_in) order[ni + __popc(bi & below)] = (unsigned)p << 16 | (unsigned)j;
+                if (is_f) {
+                    int g = ng + inc - cnt;
+                    unsigned gi[4] = {0xffffu, 0xffffu, 0xffffu, 0xffffu};
+                    const int sx[4] = {x - 1, x + 1, x, x}, sy[4] = {y, y, y - 1, y + 1};
+                    for (int d = 0; d < 4; d++)
+                        if (need[d]) {
+                            st.gsrc[g] = (unsigned)(((2ll * sx[d]) * ny + sy[d]) * nz2);
+                            gi[d] = (unsigned)g++;
+                        }
+                    const int f = nf + __popc(bf & below);
+                    st.ftab[f] = (unsigned)p << 16 | (unsigned)j;
+                    st.fgi[2 * f] = gi[0] | gi[1] << 16;
+                    st.fgi[2 * f + 1] = gi[2] | gi[3] << 16;
+                }
+                ni += __popc(bi);
+                nf += __popc(bf);
+                ng += __shfl_sync(0xffffffffu, inc, 31);
             }
-            s_nf = nf;
-            s_ng = ng;
+            if (tid == 0) {
+                s_nf = nf;
+                s_ng = ng;
+            }
         }
         __syncthreads();
         const int nq = nz2 / 4, nfq = s_nf * nq, ngq = s_ng * nq;
@@ -859,24 +888,45 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     // initial guess from the phi of earlier steps (ctl[2]: how many are held)
     const int hist = a.extrapolate ? a.ctl[2] : 0;
     if (a.extrapolate) {
-        for (int e = tid; e < np * nr * nz; e += nth) {
-            int k = e % nz, l = e / nz, j = l % nr, p = l / nr;
-            int x = x0 + p, y = y0 + j;
-            if (y < 1 || y > ny - 2 || k < 1 || k > nz - 2) continue;
-            long long id = x * sxy + (long long)y * nz + k;
-            // polynomial extrapolation in time of the highest order the history
-            // allows: 2 p0 - p1 (linear), 3 (p0 - p1) + p2 (quadratic).  A cubic
-            // guess measured worse: it amplifies the step-to-step particle noise.
-            const double cur = a.phi64[id], prev = a.phi64_prev[id];
-            const int ord = min(a.extrapolate, hist);
-            if (ord == 2) a.phi64[id] = 3.0 * (cur - prev) + a.phi64_prev2[id];
-            else if (ord == 1) a.phi64[id] = 2.0 * cur - prev;
-            if (a.extrapolate >= 2) a.phi64_prev2[id] = prev;
-            a.phi64_prev[id] = cur;
+        // polynomial extrapolation in time of the highest order the history
+        // allows: 2 p0 - p1 (linear), 3 (p0 - p1) + p2 (quadratic).  A cubic
+        // guess measured worse: it amplifies the step-to-step particle noise.
+        // Four nodes per thread at a time, their loads ahead of the stores.
+        const int ord = min(a.extrapolate, hist), ne = np * nr * nz;
+        constexpr int kU = 4;
+        for (int e0 = tid; e0 < ne; e0 += kU * nth) {
+            long long idv[kU];
+            double cur[kU], prev[kU], prev2[kU];
+            bool ok[kU];
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                const int e = e0 + u * nth, k = e % nz, l = e / nz, j = l % nr, p = l / nr;
+                const int y = y0 + j;
+                ok[u] = e < ne && y >= 1 && y <= ny - 2 && k >= 1 && k <= nz - 2;
+                idv[u] = (x0 + p) * sxy + (long long)y * nz + k;
+                cur[u] = prev[u] = prev2[u] = 0.0;
+                if (ok[u]) {
+                    cur[u] = a.phi64[idv[u]];
+                    prev[u] = a.phi64_prev[idv[u]];
+                    if (ord == 2) prev2[u] = a.phi64_prev2[idv[u]];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; u++) {
+                if (!ok[u]) continue;
+                if (ord == 2) a.phi64[idv[u]] = 3.0 * (cur[u] - prev[u]) + prev2[u];
+                else if (ord == 1) a.phi64[idv[u]] = 2.0 * cur[u] - prev[u];
+                if (a.extrapolate >= 2) a.phi64_prev2[idv[u]] = prev[u];
+                a.phi64_prev[idv[u]] = cur[u];
+            }
         }
     }
 
-    int its = 0, m_prev = 0, cycles = 0, m = max(a.inner_min, min(a.inner_max, a.ctl[1]));
+    // first cycle: 7/8 of the previous solve's iteration count (ctl[1]), so
+    // that a solve like the last one takes one long cycle and a short
+    // correction, three residual checks in all; the cycles after it follow the
+    // observed rate, clamped to [inner_min, inner_max]
+    int its = 0, m_prev = 0, cycles = 0, m = max(1, min(a.inner_max, (7 * a.ctl[1]) / 8));
     double rel_prev = -1.0, rel = 0.0, maxd = 0.0;
     bool converged = false;
     S last_max = S(0);
@@ -889,47 +939,120 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         // delta of every block is final in global memory after this barrier
         if (!grid_barrier(a.bar, a.nblocks, err)) return;
 
-        // ---- double residual of phi + delta on own interior nodes -------
-        double rr = 0.0, bb = 0.0;
+        // ---- FP64 residual of phi + delta on own interior nodes ----------
+        // The first check of a solve evaluates b + L phi from phi's stencil
+        // (delta is zero there).  Later ones carry it: the residual of
+        // phi + delta is r + L delta, with r the FP64 residual kept per node
+        // since the last check and delta read as floats (exact in double), so
+        // no block reads another block's phi and phi += delta folds in the
+        // same pass.  The source of the next cycle is the new residual,
+        // pre-scaled.
+        double rr = 0.0;
         const int k = k_own;
-        for (int l = rz_start, j = jz_start, p = pz_start; k >= 1 && k <= nz - 2 && l < np * nr;
-             l += zrows_step, j += djz, p += dpz) {
-            if (j >= nr) {
-                j -= nr;
-                p++;
+        const bool kin = k >= 1 && k <= nz - 2;
+        if (its == 0) {
+            double bb = 0.0;
+            // kCheckRows rows at a time: their stencil loads go out together
+            for (int l = rz_start; kin && l < np * nr; l += kCheckRows * zrows_step) {
+                long long idr[kCheckRows];
+                double v[kCheckRows][7];
+                T rh[kCheckRows];
+                bool okr[kCheckRows];
+#pragma unroll
+                for (int u = 0; u < kCheckRows; u++) {
+                    const int lu = l + u * zrows_step;
+                    const int p = lu / nr, j = lu - p * nr, y = y0 + j;
+                    okr[u] = lu < np * nr && y >= 1 && y <= ny - 2;
+                    const long long id = (x0 + p) * sxy + (long long)y * nz + k;
+                    idr[u] = id;
+                    rh[u] = T(0);
+#pragma unroll
+                    for (int q = 0; q < 7; q++) v[u][q] = 0.0;
+                    if (okr[u]) {
+                        v[u][0] = __ldcg(a.phi64 + id);
+                        v[u][1] = __ldcg(a.phi64 + id - sxy);
+                        v[u][2] = __ldcg(a.phi64 + id + sxy);
+                        v[u][3] = __ldcg(a.phi64 + id - nz);
+                        v[u][4] = __ldcg(a.phi64 + id + nz);
+                        v[u][5] = __ldcg(a.phi64 + id - 1);
+                        v[u][6] = __ldcg(a.phi64 + id + 1);
+                        rh[u] = __ldg(a.rho + id);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kCheckRows; u++) {
+                    if (!okr[u]) continue;
+                    const int lu = l + u * zrows_step;
+                    const int p = lu / nr, j = lu - p * nr, x = x0 + p, y = y0 + j;
+                    const double bv = a.src_c * (double)rh[u];
+                    const double r = bv + (v[u][2] + v[u][1]) * a.dhx2i + (v[u][4] + v[u][3]) * a.dhy2i +
+                                     (v[u][6] + v[u][5]) * a.dhz2i - a.ddiag * v[u][0];
+                    a.resid[idr[u]] = r;
+                    rr += r * r;
+                    bb += bv * bv;
+                    const int kh = k >> 1, c0 = (x + y + k) & 1;
+                    if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)(r * a.src_scale);
+                    else a.src[B.mirror(x, c0, y) + kh] = (S)(r * a.src_scale);
+                }
             }
-            const int x = x0 + p, y = y0 + j;
-            if (y < 1 || y > ny - 2) continue;
-            const long long id = x * sxy + (long long)y * nz + k;
-            const int kh = k >> 1, c0 = (x + y + k) & 1, c1 = c0 ^ 1;
-            // own values from shared memory, other blocks' from their mirrors
-            // (zero on the Dirichlet planes and rows)
-            double dc = (double)SD(p, c0, j, kh);
-            double dzm = (double)SD(p, c1, j, (k - 1) >> 1), dzp = (double)SD(p, c1, j, (k + 1) >> 1);
-            double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh) : mirror_value<kTag>(a, B.mirror(x - 1, c1, y) + kh);
-            double dxp =
-                p + 1 < np ? (double)SD(p + 1, c1, j, kh) : mirror_value<kTag>(a, B.mirror(x + 1, c1, y) + kh);
-            double dym = j > 0 ? (double)SD(p, c1, j - 1, kh) : mirror_value<kTag>(a, B.mirror(x, c1, y - 1) + kh);
-            double dyp =
-                j + 1 < nr ? (double)SD(p, c1, j + 1, kh) : mirror_value<kTag>(a, B.mirror(x, c1, y + 1) + kh);
-            double pc = __ldcg(a.phi64 + id) + dc;
-            double pxm = __ldcg(a.phi64 + id - sxy) + dxm;
-            double pxp = __ldcg(a.phi64 + id + sxy) + dxp;
-            double pym = __ldcg(a.phi64 + id - nz) + dym;
-            double pyp = __ldcg(a.phi64 + id + nz) + dyp;
-            double pzm = __ldcg(a.phi64 + id - 1) + dzm;
-            double pzp = __ldcg(a.phi64 + id + 1) + dzp;
-            double bv = a.src_c * (double)__ldg(a.rho + id);
-            double r = bv + (pxp + pxm) * a.dhx2i + (pyp + pym) * a.dhy2i + (pzp + pzm) * a.dhz2i - a.ddiag * pc;
-            rr += r * r;
-            bb += bv * bv;
-            if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)(r * a.src_scale);
-            else a.src[B.mirror(x, c0, y) + kh] = (S)(r * a.src_scale);
-        }
-        block_sum2(rr, bb);
-        if (tid == 0) {
-            a.partials[4 * b + 0] = rr;
-            a.partials[4 * b + 1] = bb;
+            block_sum2(rr, bb);
+            if (tid == 0) {
+                a.partials[4 * b + 0] = rr;
+                a.partials[4 * b + 1] = bb;  // kept for the later checks
+            }
+        } else {
+            // kCheckRows rows at a time: their loads go out before any store
+            for (int l = rz_start; kin && l < np * nr; l += kCheckRows * zrows_step) {
+                long long idr[kCheckRows];
+                double rv[kCheckRows], pv[kCheckRows];
+                S mv[kCheckRows][4];
+                int pr[kCheckRows], jr[kCheckRows];
+                bool okr[kCheckRows];
+#pragma unroll
+                for (int u = 0; u < kCheckRows; u++) {
+                    const int lu = l + u * zrows_step;
+                    const int p = lu / nr, j = lu - p * nr, x = x0 + p, y = y0 + j;
+                    pr[u] = p;
+                    jr[u] = j;
+                    okr[u] = lu < np * nr && y >= 1 && y <= ny - 2;
+                    idr[u] = x * sxy + (long long)y * nz + k;
+                    rv[u] = pv[u] = 0.0;
+                    mv[u][0] = mv[u][1] = mv[u][2] = mv[u][3] = S(0);
+                    if (okr[u]) {
+                        rv[u] = a.resid[idr[u]];
+                        pv[u] = __ldcg(a.phi64 + idr[u]);
+                        // other blocks' delta from their mirrors (zero on the
+                        // Dirichlet planes and rows)
+                        const int kh = k >> 1, c1 = ((x + y + k) & 1) ^ 1;
+                        if (p == 0) mv[u][0] = (S)mirror_value<kTag>(a, B.mirror(x - 1, c1, y) + kh);
+                        if (p + 1 == np) mv[u][1] = (S)mirror_value<kTag>(a, B.mirror(x + 1, c1, y) + kh);
+                        if (j == 0) mv[u][2] = (S)mirror_value<kTag>(a, B.mirror(x, c1, y - 1) + kh);
+                        if (j + 1 == nr) mv[u][3] = (S)mirror_value<kTag>(a, B.mirror(x, c1, y + 1) + kh);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kCheckRows; u++) {
+                    if (!okr[u]) continue;
+                    const int p = pr[u], j = jr[u], x = x0 + p, y = y0 + j;
+                    const int kh = k >> 1, c0 = (x + y + k) & 1, c1 = c0 ^ 1;
+                    const double dc = (double)SD(p, c0, j, kh);
+                    const double dzm = (double)SD(p, c1, j, (k - 1) >> 1), dzp = (double)SD(p, c1, j, (k + 1) >> 1);
+                    const double dxm = p > 0 ? (double)SD(p - 1, c1, j, kh) : (double)mv[u][0];
+                    const double dxp = p + 1 < np ? (double)SD(p + 1, c1, j, kh) : (double)mv[u][1];
+                    const double dym = j > 0 ? (double)SD(p, c1, j - 1, kh) : (double)mv[u][2];
+                    const double dyp = j + 1 < nr ? (double)SD(p, c1, j + 1, kh) : (double)mv[u][3];
+                    const double r = rv[u] + (dxp + dxm) * a.dhx2i + (dyp + dym) * a.dhy2i + (dzp + dzm) * a.dhz2i -
+                                     a.ddiag * dc;
+                    a.resid[idr[u]] = r;
+                    a.phi64[idr[u]] = pv[u] + dc;
+                    rr += r * r;
+                    if (ss) ss[((p * 2 + c0) * nr + j) * nz2 + kh] = (S)(r * a.src_scale);
+                    else a.src[B.mirror(x, c0, y) + kh] = (S)(r * a.src_scale);
+                }
+            }
+            double none = 0.0;
+            block_sum2(rr, none);
+            if (tid == 0) a.partials[4 * b + 0] = rr;
         }
         if (!grid_barrier(a.bar, a.nblocks, err)) return;
 
@@ -957,19 +1080,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         maxd = s_tot[2];
         cycles++;
 
-        // ---- fold: phi += delta, delta = 0 -------------------------------
-        for (int l = rz_start, j = jz_start, p = pz_start; k >= 1 && k <= nz - 2 && l < np * nr;
-             l += zrows_step, j += djz, p += dpz) {
-            if (j >= nr) {
-                j -= nr;
-                p++;
-            }
-            const int x = x0 + p, y = y0 + j;
-            if (y < 1 || y > ny - 2) continue;
-            const long long id = x * sxy + (long long)y * nz + k;
-            a.phi64[id] += (double)SD(p, (x + y + k) & 1, j, k >> 1);
-        }
-        __syncthreads();
+        // ---- the next cycle starts from delta = 0 -------------------------
         for (int e = tid; e < own; e += nth) sd[e] = S(0);
         if constexpr (!kTag)
             for (int p = 0; p < np; p++)
@@ -1059,7 +1170,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         a.status[2] = converged ? 1 : 0;
         a.status[3] = cycles;
         a.metric[0] = a.criterion == HV_SOR_REL_RESIDUAL ? rel : maxd;
-        a.ctl[1] = max(m, a.inner_min);
+        a.ctl[1] = max(its, 1);
         if (a.extrapolate) a.ctl[2] = min(a.ctl[2] + 1, 2);
         if (a.its_ring) a.its_ring[step % a.ring] = converged ? its : -its;
     }
@@ -1179,6 +1290,7 @@ static hv_status plan_for(hv_ctx *c, int max_blocks) {
     const size_t n = (size_t)g.nx * 2 * g.ny * nz2;
     HV_CUDA(cudaMalloc(&f.delta, n * 8));
     HV_CUDA(cudaMalloc(&f.src, n * sizeof(S)));
+    HV_CUDA(cudaMalloc((void **)&f.resid, sizeof(double) * g.G));
     HV_CUDA(cudaMemsetAsync(f.delta, 0, n * 8, c->stream));
     HV_CUDA(cudaMemsetAsync(f.src, 0, n * sizeof(S), c->stream));
     HV_CUDA(cudaMalloc((void **)&f.partials, sizeof(double) * 4 * f.nblocks));
@@ -1198,7 +1310,7 @@ hv_status sor_fast_plan(hv_ctx *c) {
 
 void sor_fast_release(hv_ctx *c) {
     SorFast &f = c->fused.sor;
-    void *ptrs[] = {f.delta, f.src, f.partials, f.phase, f.status, f.metric};
+    void *ptrs[] = {f.delta, f.src, f.resid, f.partials, f.phase, f.status, f.metric};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     f = SorFast();
@@ -1255,6 +1367,7 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.phi64 = c->fused.phi64;
     a.phi64_prev = c->fused.phi64_prev;
     a.phi64_prev2 = c->fused.phi64_prev2;
+    a.resid = f.resid;
     a.delta = reinterpret_cast<S *>(f.delta);
     a.tmirror = reinterpret_cast<u64 *>(f.delta);
     a.src = reinterpret_cast<S *>(f.src);
@@ -1296,13 +1409,17 @@ static const void *sor_kernel(int form) {
     else return (const void *)k_sor_fast<T, T, false, 0, 0, 0>;
 }
 
+// step_solve false: a solve whose starting phi is not a converged solution
+// (the initial solve from phi = 0) starts from that phi and leaves the history
+// of earlier solutions untouched.
 template <typename T>
-hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring) {
+hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, bool step_solve) {
     SorFast &f = c->fused.sor;
     HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
     HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, c->stream));
     SorArgs<T, T> a;
     const int form = sor_fast_args<T>(c, rho, ctl, its_ring, ring, a);
+    if (!step_solve) a.extrapolate = 0;
     void *args[] = {&a};
     HV_CUDA(cudaLaunchCooperativeKernel(sor_kernel<T, false>(form), dim3(f.nblocks), dim3(f.threads), args, f.smem,
                                         c->stream));
@@ -1377,7 +1494,7 @@ void sor_wave_release(SorWave &w) {
     w = SorWave();
 }
 
-template hv_status sor_fast_launch<float>(hv_ctx *, const float *, int *, int *, int);
-template hv_status sor_fast_launch<double>(hv_ctx *, const double *, int *, int *, int);
+template hv_status sor_fast_launch<float>(hv_ctx *, const float *, int *, int *, int, bool);
+template hv_status sor_fast_launch<double>(hv_ctx *, const double *, int *, int *, int, bool);
 
 }  // namespace hv

@@ -309,13 +309,16 @@ typedef enum hv_sor_exchange {
 typedef struct hv_fast_options {
     int sor_warm_start;   /* hv_warm_start                                      */
     int sor_inner_min;    /* red+black iterations between two FP64 residual     */
-    int sor_inner_max;    /*   checks: adaptive, clamped to [min, max]          */
+    int sor_inner_max;    /*   checks: the first cycle of a solve runs 7/8 of the
+                             previous solve's iterations (at most max), the
+                             later ones follow the observed rate, clamped to
+                             [min, max]                                        */
     int sort_every;       /* re-sort particle slots by cell every n steps (0 = off) */
     int graph_steps;      /* steps captured per CUDA graph launch (0 = no graph) */
     int sor_exchange;     /* hv_sor_exchange                                    */
 } hv_fast_options;
 
-/* Defaults: HV_WARM_QUADRATIC, inner 2..256, sort every 16 steps, 8-step graphs,
+/* Defaults: HV_WARM_QUADRATIC, inner 8..256, sort every 16 steps, 8-step graphs,
  * HV_SOR_EXCHANGE_AUTO. */
 HV_API void hv_fast_options_default(hv_fast_options *o);
 HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);

@@ -114,6 +114,28 @@ def test_extrapolated_warm_start_saves_iterations(hv):
     assert not np.any(obs_c["flags"] & 1)
 
 
+def test_first_steps_after_the_fused_initial_solve_start_from_solutions(hv):
+    """hv_run on the fused path with no earlier solve runs the initial solve
+    itself, from phi = 0.  That starting phi must not enter the history that
+    the extrapolated guesses are built from: the first steps then need no more
+    iterations than from the previous phi (a zero in the history made steps 1
+    and 2 start from 2 phi_0 and ~0 and cost as much as the initial solve)."""
+    w = hv.CA40_SMALL
+    p32 = hv.workload_particles(w, np.float32)
+    its = {}
+    for ws in (hv.HV_WARM_PREVIOUS, hv.HV_WARM_QUADRATIC):
+        with hv.Session.from_workload(w, hv.HV_F32) as s:
+            s.set_fast_options(sor_warm_start=ws, sor_inner_min=1, sor_inner_max=8)
+            s.upload_particles(*p32)
+            its[ws] = s.run(6, hv.HV_PATH_FUSED)["sor_iterations"].astype(np.int64)
+    prev, quad = its[hv.HV_WARM_PREVIOUS], its[hv.HV_WARM_QUADRATIC]
+    # step 0 starts from the initial solution under both guesses
+    assert abs(int(quad[0]) - int(prev[0])) <= 8, (quad, prev)
+    # later steps extrapolate from converged solutions only
+    assert np.all(quad[1:] <= prev[1:] + 8), (quad, prev)
+    assert quad[1:].sum() < prev[1:].sum(), (quad, prev)
+
+
 def test_fused_state_and_fields_match_oracle_on_final_positions(hv):
     """After a fused run the plain buffers describe the final state: density,
     potential and forces of the final positions (computed by the oracle from
