@@ -112,6 +112,14 @@ struct SmoothFast {
     size_t smem = 0;
     int per = 0;               // R = max(A, B, W): the kernel instantiation
     int xsplit = 1;            // x segments per column tile (the plan's choice)
+    // FFT form (power-of-two axes up to 128): the circular convolution by the
+    // stencil's spectrum, exact while no density lies within (A, B, W) of a face
+    bool fft = false;
+    void *fwork = nullptr;     // nx ny nz complex floats: both species' transform
+    float *khat = nullptr;     // nx ny nz: the stencil's spectrum x term / (nx ny nz)
+    void *tw = nullptr;        // 64 complex twiddles exp(-2 pi i m / 128)
+    int *edge = nullptr;       // [nx]: density found within the stencil of a face
+    double fft_term = 0.0;     // the term folded into khat
 };
 
 // Fast-path (fused) buffers.

@@ -19,9 +19,11 @@
 //
 // Used when the tap table passes the symmetry and contiguity checks in
 // smooth_fast_plan (all cubic grids); otherwise the direct kernel runs.
+#include <algorithm>
 #include <cmath>
 #include <set>
 #include <tuple>
+#include <vector>
 
 #include "hv_internal.h"
 
@@ -44,6 +46,8 @@ struct MarchArgs {
     int wt[(kMaxR + 1) * (kMaxR + 1)];        // w(|a|, |b|) at |a| (kMaxR + 1) + |b| (-1: none)
     const float *src;                         // 2G
     float *dst;                               // 2G
+    const int *edge;                          // [nx] edge flags of the FFT form: run only if
+                                              // one is set (null: always run)
 };
 
 // Plane xi of the block's rho tile (y halo B, z halo W; zero outside the
@@ -79,6 +83,18 @@ __global__ void __launch_bounds__(kMThreads) k_smooth_march(const __grid_constan
     extern __shared__ __align__(16) float sm[];
     constexpr int rows = kMBY + 2 * R, cols = kMBK + 2 * R;
     constexpr int kPer = (rows * cols + kMThreads - 1) / kMThreads;
+    if (a.edge) {
+        // after the FFT form: needed only where it is not exact
+        __shared__ int s_any;
+        if (threadIdx.x < 32) {
+            int v = 0;
+            for (int i = threadIdx.x; i < a.nx; i += 32) v |= a.edge[i];
+            v = __any_sync(0xffffffffu, v);
+            if (threadIdx.x == 0) s_any = v;
+        }
+        __syncthreads();
+        if (!s_any) return;
+    }
     const int A = a.A, ring = 2 * A + 1;
     float *s_rho = sm;                               // rows x cols
     float *s_z = s_rho + rows * cols;                // (R + 1) x rows x kMBK
@@ -190,6 +206,161 @@ const void *march_kernel(int r) {
     }
 }
 
+// ---- FFT form --------------------------------------------------------------
+//
+// The smoothing is a convolution by a fixed symmetric stencil, so on a grid of
+// power-of-two axes it is also a pointwise product in Fourier space.  The
+// circular convolution equals the reference's truncated sum when no density
+// lies within the stencil's half-widths (A, B, W) of a face: the only wrapped
+// inputs come from those edge slabs.  The first pass flags any density there;
+// the march kernel then runs (and overwrites the result) only when a flag is
+// set.  Both species go through one complex transform, rho_p + i rho_n: the
+// stencil's spectrum is real (the stencil is even), so the product keeps them
+// apart.  Three passes over a complex work grid:
+//   1. per x plane: load both species, flag the edge slabs, 2D transform along
+//      z then y in shared memory (radix 2, decimation in time from a
+//      bit-reversed load);
+//   2. per y: transform along x, multiply by the spectrum, inverse along x
+//      (decimation in frequency, stored back from bit-reversed order);
+//   3. per x plane: inverse along z and y, both species stored, clamped at 0.
+constexpr int kFThreads = 1024;
+constexpr int kFMaxN = 128;        // longest axis of the FFT form
+constexpr int kFMaxPlane = 16384;  // complex elements of a plane or column slab (128 KB)
+
+struct FftArgs {
+    int nx, ny, nz, lx, ly, lz;  // axis lengths and their log2
+    int A, B, W;                 // stencil half-widths: the edge slabs
+    long long G;
+    const float *src;            // 2G: protons, neutrons
+    float *dst;                  // 2G
+    float2 *work;                // G complex
+    const float *khat;           // G: spectrum x term / G
+    const float2 *tw;            // kFMaxN / 2 twiddles exp(-2 pi i m / kFMaxN)
+    int *edge;                   // [nx]
+    float post;                  // current term / the term folded into khat
+};
+
+__device__ __forceinline__ int bit_reverse(int v, int l) { return (int)(__brev((unsigned)v) >> (32 - l)); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// Radix-2 stages over `lines` transforms of length n = 2^l (l >= 1) in shared
+// memory, element m of line q at s[q * qs + m * ms].  kDit: bit-reversed input,
+// natural output (decimation in time); otherwise natural input, bit-reversed
+// output (decimation in frequency).  inv: conjugate twiddles (no 1/n; the
+// spectrum carries it).  Rows (ms = 1) give consecutive threads consecutive
+// butterflies of a line; columns give them consecutive lines, so a warp's
+// accesses are contiguous either way.
+template <bool kDit>
+__device__ void fft_stages(float2 *s, int n, int l, int lines, int qs, int ms, const float2 *tw, bool inv) {
+    const int half = n >> 1, total = lines * half, tstep = kFMaxN / n;
+    for (int st = 0; st < l; st++) {
+        const int h = kDit ? (1 << st) : (half >> st);
+        const int wstep = (half / h) * tstep;
+        for (int t = threadIdx.x; t < total; t += blockDim.x) {
+            int q, j;
+            if (ms == 1) {
+                j = t & (half - 1);
+                q = t >> (l - 1);
+            } else {
+                q = t % lines;
+                j = t / lines;
+            }
+            const int k = j & (h - 1), i = ((j - k) << 1) + k;
+            float2 w = tw[k * wstep];
+            if (inv) w.y = -w.y;
+            float2 *p0 = s + q * qs + i * ms, *p1 = p0 + h * ms;
+            const float2 u = *p0, v = *p1;
+            if (kDit) {
+                const float2 vw = cmul(v, w);
+                *p0 = make_float2(u.x + vw.x, u.y + vw.y);
+                *p1 = make_float2(u.x - vw.x, u.y - vw.y);
+            } else {
+                *p0 = make_float2(u.x + v.x, u.y + v.y);
+                *p1 = cmul(make_float2(u.x - v.x, u.y - v.y), w);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kFThreads) k_fft_plane_fwd(const __grid_constant__ FftArgs a) {
+    extern __shared__ __align__(16) float2 fs[];  // ny x nz
+    __shared__ float2 stw[kFMaxN / 2];
+    const int x = blockIdx.x, tid = threadIdx.x, P = a.ny * a.nz;
+    if (tid < kFMaxN / 2) stw[tid] = a.tw[tid];
+    const float *sp = a.src + (long long)x * P, *sn = sp + a.G;
+    const bool xedge = x < a.A || x >= a.nx - a.A;
+    int edge = 0;
+    for (int e = tid; e < P; e += kFThreads) {
+        const int y = e >> a.lz, z = e & (a.nz - 1);
+        const float rp = __ldg(sp + e), rn = __ldg(sn + e);
+        if ((rp != 0.0f || rn != 0.0f) && (xedge || y < a.B || y >= a.ny - a.B || z < a.W || z >= a.nz - a.W))
+            edge = 1;
+        fs[(bit_reverse(y, a.ly) << a.lz) + bit_reverse(z, a.lz)] = make_float2(rp, rn);
+    }
+    edge = __syncthreads_or(edge);
+    if (tid == 0) a.edge[x] = edge;
+    fft_stages<true>(fs, a.nz, a.lz, a.ny, a.nz, 1, stw, false);
+    fft_stages<true>(fs, a.ny, a.ly, a.nz, 1, a.nz, stw, false);
+    float2 *out = a.work + (long long)x * P;
+    for (int e = tid; e < P; e += kFThreads) out[e] = fs[e];
+}
+
+__global__ void __launch_bounds__(kFThreads) k_fft_columns(const __grid_constant__ FftArgs a) {
+    extern __shared__ __align__(16) float2 fs[];  // nx x nz
+    __shared__ float2 stw[kFMaxN / 2];
+    const int y = blockIdx.x, tid = threadIdx.x, P = a.ny * a.nz, L = a.nx * a.nz;
+    if (tid < kFMaxN / 2) stw[tid] = a.tw[tid];
+    for (int e = tid; e < L; e += kFThreads) {
+        const int x = e >> a.lz, z = e & (a.nz - 1);
+        fs[(bit_reverse(x, a.lx) << a.lz) + z] = a.work[(long long)x * P + y * a.nz + z];
+    }
+    __syncthreads();
+    fft_stages<true>(fs, a.nx, a.lx, a.nz, 1, a.nz, stw, false);
+    for (int e = tid; e < L; e += kFThreads) {
+        const int x = e >> a.lz, z = e & (a.nz - 1);
+        const float kh = __ldg(a.khat + (long long)x * P + y * a.nz + z);
+        fs[e] = make_float2(fs[e].x * kh, fs[e].y * kh);
+    }
+    __syncthreads();
+    fft_stages<false>(fs, a.nx, a.lx, a.nz, 1, a.nz, stw, true);
+    for (int e = tid; e < L; e += kFThreads) {
+        const int x = e >> a.lz, z = e & (a.nz - 1);
+        a.work[(long long)x * P + y * a.nz + z] = fs[(bit_reverse(x, a.lx) << a.lz) + z];
+    }
+}
+
+__global__ void __launch_bounds__(kFThreads) k_fft_plane_inv(const __grid_constant__ FftArgs a) {
+    extern __shared__ __align__(16) float2 fs[];  // ny x nz
+    __shared__ float2 stw[kFMaxN / 2];
+    const int x = blockIdx.x, tid = threadIdx.x, P = a.ny * a.nz;
+    if (tid < kFMaxN / 2) stw[tid] = a.tw[tid];
+    const float2 *in = a.work + (long long)x * P;
+    for (int e = tid; e < P; e += kFThreads) fs[e] = in[e];
+    __syncthreads();
+    fft_stages<false>(fs, a.nz, a.lz, a.ny, a.nz, 1, stw, true);
+    fft_stages<false>(fs, a.ny, a.ly, a.nz, 1, a.nz, stw, true);
+    float *dp = a.dst + (long long)x * P, *dn = dp + a.G;
+    for (int e = tid; e < P; e += kFThreads) {
+        const int y = e >> a.lz, z = e & (a.nz - 1);
+        const float2 v = fs[(bit_reverse(y, a.ly) << a.lz) + bit_reverse(z, a.lz)];
+        // the exact sum is non-negative; the transform's rounding (~1e-7 of
+        // the maximum) must not leave negative densities, where the Skyrme
+        // term rho^gamma has no value
+        dp[e] = fmaxf(v.x * a.post, 0.0f);
+        dn[e] = fmaxf(v.y * a.post, 0.0f);
+    }
+}
+
+int log2_exact(int n) {
+    int l = 0;
+    while ((1 << l) < n) l++;
+    return (1 << l) == n ? l : -1;
+}
+
 }  // namespace
 
 // Builds the decomposition from the tap table, or leaves ok = false when the
@@ -283,10 +454,94 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     f.B = B;
     f.W = W;
     f.ok = true;
+
+    // FFT form: power-of-two axes of 2..128 whose planes fit in shared memory
+    const Geom &gg = c->geom;
+    const int lx = log2_exact(gg.nx), ly = log2_exact(gg.ny), lz = log2_exact(gg.nz);
+    if (lx < 1 || ly < 1 || lz < 1 || gg.nx > kFMaxN || gg.ny > kFMaxN || gg.nz > kFMaxN ||
+        gg.ny * gg.nz > kFMaxPlane || gg.nx * gg.nz > kFMaxPlane)
+        return HV_OK;
+    // The stencil's spectrum, in double: with the taps symmetric per axis,
+    //   K(kx,ky,kz) = sum_a m_a g(a) cos(2 pi a kx / nx) Y_|a|(ky, kz),
+    //   Y_a(ky,kz)  = sum_{b <= bm(a)} m_b g(b) cos(2 pi b ky / ny) Z_w(a,b)(kz),
+    //   Z_w(kz)     = sum_{|c| <= w} g(c) cos(2 pi c kz / nz),
+    // m = 1 at 0 and 2 elsewhere; scaled by term / G (the inverse transform's 1/G).
+    const int nx = gg.nx, ny = gg.ny, nz = gg.nz, P = ny * nz;
+    std::vector<double> gxd(A + 1), gyd(B + 1), gzd(W + 1);
+    auto g1d = [&](int axis, int off) {
+        const int n = wd.n[axis], ctr = n / 2;
+        const double dm = wd.d_max[axis];
+        double d = dm * (2.0 * ctr / n - 1.0) - dm * (2.0 * (ctr + off) / n - 1.0);
+        return std::exp(-d * d * e);
+    };
+    for (int a = 0; a <= A; a++) gxd[a] = g1d(0, a);
+    for (int b = 0; b <= B; b++) gyd[b] = g1d(1, b);
+    for (int cz = 0; cz <= W; cz++) gzd[cz] = g1d(2, cz);
+    const double twopi = 2.0 * kPi;
+    std::vector<double> zw((size_t)(W + 1) * nz);
+    for (int kz = 0; kz < nz; kz++) {
+        double acc = gzd[0];
+        zw[kz] = acc;
+        for (int w = 1; w <= W; w++) {
+            acc += 2.0 * gzd[w] * std::cos(twopi * w * kz / nz);
+            zw[(size_t)w * nz + kz] = acc;
+        }
+    }
+    std::vector<double> ya((size_t)(A + 1) * P, 0.0);
+    for (int a = 0; a <= A; a++) {
+        if (f.bm[a] < 0) continue;
+        for (int b = 0; b <= f.bm[a]; b++) {
+            const int w = f.wt[a * (kMaxR + 1) + b];
+            const double mb = b ? 2.0 : 1.0;
+            for (int ky = 0; ky < ny; ky++) {
+                const double cy = mb * gyd[b] * std::cos(twopi * b * ky / ny);
+                double *row = &ya[(size_t)a * P + (size_t)ky * nz];
+                const double *zr = &zw[(size_t)w * nz];
+                for (int kz = 0; kz < nz; kz++) row[kz] += cy * zr[kz];
+            }
+        }
+    }
+    const hv_run_params &pr = c->params;
+    f.fft_term = (1.0 / pr.part_per_nucleon) * (1.0 / std::pow(2.0 * kPi * sig * sig, 1.5));
+    const double scale = f.fft_term / (double)gg.G;
+    std::vector<float> kh((size_t)gg.G);
+    std::vector<double> acc(P);
+    for (int kx = 0; kx <= nx / 2; kx++) {
+        std::fill(acc.begin(), acc.end(), 0.0);
+        for (int a = 0; a <= A; a++) {
+            if (f.bm[a] < 0) continue;
+            const double cx = (a ? 2.0 : 1.0) * gxd[a] * std::cos(twopi * a * kx / nx);
+            const double *yr = &ya[(size_t)a * P];
+            for (int q = 0; q < P; q++) acc[q] += cx * yr[q];
+        }
+        // K is even in kx: planes kx and nx - kx are equal
+        for (int q = 0; q < P; q++) kh[(size_t)kx * P + q] = (float)(acc[q] * scale);
+        if (kx > 0 && kx < nx - kx)
+            std::copy(kh.begin() + (size_t)kx * P, kh.begin() + (size_t)(kx + 1) * P, kh.begin() + (size_t)(nx - kx) * P);
+    }
+    std::vector<float2> tw(kFMaxN / 2);
+    for (int m = 0; m < kFMaxN / 2; m++)
+        tw[m] = make_float2((float)std::cos(twopi * m / kFMaxN), (float)-std::sin(twopi * m / kFMaxN));
+    HV_CUDA(cudaMalloc(&f.fwork, sizeof(float2) * gg.G));
+    HV_CUDA(cudaMalloc((void **)&f.khat, sizeof(float) * gg.G));
+    HV_CUDA(cudaMalloc(&f.tw, sizeof(float2) * tw.size()));
+    HV_CUDA(cudaMalloc((void **)&f.edge, sizeof(int) * nx));
+    HV_CUDA(cudaMemcpy(f.khat, kh.data(), sizeof(float) * gg.G, cudaMemcpyHostToDevice));
+    HV_CUDA(cudaMemcpy(f.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+    const size_t plane = sizeof(float2) * (size_t)std::max(P, nx * nz);
+    for (const void *k : {(const void *)k_fft_plane_fwd, (const void *)k_fft_columns, (const void *)k_fft_plane_inv})
+        HV_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+    f.fft = true;
     return HV_OK;
 }
 
-void smooth_fast_release(hv_ctx *c) { c->fused.smooth = SmoothFast(); }
+void smooth_fast_release(hv_ctx *c) {
+    SmoothFast &f = c->fused.smooth;
+    void *ptrs[] = {f.fwork, f.khat, f.tw, f.edge};
+    for (void *q : ptrs)
+        if (q) cudaFree(q);
+    f = SmoothFast();
+}
 
 hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
     const SmoothFast &f = c->fused.smooth;
@@ -302,7 +557,8 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
     a.W = f.W;
     a.xsplit = f.xsplit;
     const double sig = p.sigma_r;
-    a.term = (float)((1.0 / p.part_per_nucleon) * (1.0 / std::pow(2.0 * kPi * sig * sig, 1.5)));
+    const double term = (1.0 / p.part_per_nucleon) * (1.0 / std::pow(2.0 * kPi * sig * sig, 1.5));
+    a.term = (float)term;
     for (int i = 0; i <= kMaxR; i++) {
         a.gx[i] = f.gx[i];
         a.gy[i] = f.gy[i];
@@ -312,6 +568,33 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
     for (int i = 0; i < (kMaxR + 1) * (kMaxR + 1); i++) a.wt[i] = f.wt[i];
     a.src = rho_raw;
     a.dst = rho;
+    a.edge = nullptr;
+    if (f.fft && c->fast.smooth_fft) {
+        FftArgs q;
+        q.nx = g.nx;
+        q.ny = g.ny;
+        q.nz = g.nz;
+        q.lx = log2_exact(g.nx);
+        q.ly = log2_exact(g.ny);
+        q.lz = log2_exact(g.nz);
+        q.A = f.A;
+        q.B = f.B;
+        q.W = f.W;
+        q.G = g.G;
+        q.src = rho_raw;
+        q.dst = rho;
+        q.work = reinterpret_cast<float2 *>(f.fwork);
+        q.khat = f.khat;
+        q.tw = reinterpret_cast<const float2 *>(f.tw);
+        q.edge = f.edge;
+        q.post = (float)(term / f.fft_term);
+        const size_t plane = sizeof(float2) * (size_t)g.ny * g.nz, slab = sizeof(float2) * (size_t)g.nx * g.nz;
+        k_fft_plane_fwd<<<g.nx, kFThreads, plane, c->stream>>>(q);
+        k_fft_columns<<<g.ny, kFThreads, slab, c->stream>>>(q);
+        k_fft_plane_inv<<<g.nx, kFThreads, plane, c->stream>>>(q);
+        HV_CUDA(cudaGetLastError());
+        a.edge = f.edge;
+    }
     const int tz = (g.nz + kMBK - 1) / kMBK, ty = (g.ny + kMBY - 1) / kMBY;
     void *args[] = {&a};
     HV_CUDA(cudaLaunchKernel(march_kernel(f.per), dim3(2 * f.xsplit * ty * tz), dim3(kMThreads), args, f.smem,

@@ -122,7 +122,7 @@ class Session:
 
     def set_fast_options(self, **kw):
         """Updates fields of hv_fast_options (sor_warm_start, sor_inner_min,
-        sor_inner_max, sort_every, graph_steps)."""
+        sor_inner_max, sort_every, graph_steps, sor_exchange, smooth_fft)."""
         o = self.fast_options()
         for k, v in kw.items():
             if not hasattr(o, k):

@@ -316,10 +316,14 @@ typedef struct hv_fast_options {
     int sort_every;       /* re-sort particle slots by cell every n steps (0 = off) */
     int graph_steps;      /* steps captured per CUDA graph launch (0 = no graph) */
     int sor_exchange;     /* hv_sor_exchange                                    */
+    int smooth_fft;       /* 1: Gaussian smoothing as an FFT convolution where it
+                             is exact (power-of-two axes up to 128, no density
+                             within the stencil of a face; elsewhere the direct
+                             form runs); 0: always the direct form              */
 } hv_fast_options;
 
 /* Defaults: HV_WARM_QUADRATIC, inner 8..256, sort every 16 steps, 8-step graphs,
- * HV_SOR_EXCHANGE_AUTO. */
+ * HV_SOR_EXCHANGE_AUTO, smooth_fft 1. */
 HV_API void hv_fast_options_default(hv_fast_options *o);
 HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);
 HV_API hv_status hv_ctx_get_fast_options(const hv_ctx *ctx, hv_fast_options *o);

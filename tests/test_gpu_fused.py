@@ -136,6 +136,44 @@ def test_first_steps_after_the_fused_initial_solve_start_from_solutions(hv):
     assert quad[1:].sum() < prev[1:].sum(), (quad, prev)
 
 
+def _smoothed_after(hv, w, parts, steps, **opts):
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        s.set_fast_options(**opts)
+        s.upload_particles(*parts)
+        s.run(steps, hv.HV_PATH_FUSED)
+        return s.download_field(hv.HV_FIELD_DENSITY), s.download_field(hv.HV_FIELD_DENSITY_RAW)
+
+
+@pytest.mark.parametrize("wname", ["40Ca-4k-32^3", "208Pb-20.8k-128^3"])
+def test_fft_smoothing_matches_the_direct_form(hv, wname):
+    """The FFT convolution (power-of-two grids, no density near a face) gives
+    the direct march's smoothed density to float rounding: 1e-5 of the
+    maximum, the tolerance of the fused fields against the oracle."""
+    w = hv.WORKLOADS[wname]
+    p32 = hv.workload_particles(w, np.float32)
+    d_fft, raw_fft = _smoothed_after(hv, w, p32, 3, smooth_fft=1)
+    d_dir, raw_dir = _smoothed_after(hv, w, p32, 3, smooth_fft=0)
+    assert max_rel(raw_fft, raw_dir) < 1e-5  # same particles (atomic order aside)
+    assert max_rel(d_fft, d_dir) < 1e-5, max_rel(d_fft, d_dir)
+    # no negative densities from the transform's rounding (rho^gamma follows)
+    assert d_fft.min() >= 0.0
+
+
+def test_fft_smoothing_falls_back_with_density_at_a_face(hv):
+    """Particles within the stencil of a face would wrap around in the
+    circular convolution; the first FFT pass flags them and the direct form
+    recomputes the whole field, so both options agree."""
+    w = hv.CA40_SMALL
+    p32 = [a.copy() for a in hv.workload_particles(w, np.float32)]
+    lo = -float(w.n) * w.h / 2.0
+    # 40 protons moved next to the x = min face (inside the grid)
+    p32[0][:40] = lo + 0.6 * w.h
+    d_fft, raw_fft = _smoothed_after(hv, w, p32, 1, smooth_fft=1)
+    d_dir, raw_dir = _smoothed_after(hv, w, p32, 1, smooth_fft=0)
+    assert raw_fft.reshape(2, w.n, w.n, w.n)[0, :2].sum() > 0  # density in the x edge slab
+    assert max_rel(d_fft, d_dir) < 1e-6, max_rel(d_fft, d_dir)
+
+
 def test_fused_state_and_fields_match_oracle_on_final_positions(hv):
     """After a fused run the plain buffers describe the final state: density,
     potential and forces of the final positions (computed by the oracle from
