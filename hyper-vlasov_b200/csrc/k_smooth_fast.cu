@@ -246,43 +246,114 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Radix-2 stages over `lines` transforms of length n = 2^l (l >= 1) in shared
+// Stages over `lines` = 2^ll transforms of length n = 2^l (l >= 1) in shared
 // memory, element m of line q at s[q * qs + m * ms].  kDit: bit-reversed input,
 // natural output (decimation in time); otherwise natural input, bit-reversed
 // output (decimation in frequency).  inv: conjugate twiddles (no 1/n; the
-// spectrum carries it).  Rows (ms = 1) give consecutive threads consecutive
-// butterflies of a line; columns give them consecutive lines, so a warp's
-// accesses are contiguous either way.
-template <bool kDit>
-__device__ void fft_stages(float2 *s, int n, int l, int lines, int qs, int ms, const float2 *tw, bool inv) {
-    const int half = n >> 1, total = lines * half, tstep = kFMaxN / n;
-    for (int st = 0; st < l; st++) {
-        const int h = kDit ? (1 << st) : (half >> st);
-        const int wstep = (half / h) * tstep;
-        for (int t = threadIdx.x; t < total; t += blockDim.x) {
-            int q, j;
-            if (ms == 1) {
-                j = t & (half - 1);
-                q = t >> (l - 1);
-            } else {
-                q = t % lines;
-                j = t / lines;
-            }
-            const int k = j & (h - 1), i = ((j - k) << 1) + k;
-            float2 w = tw[k * wstep];
-            if (inv) w.y = -w.y;
-            float2 *p0 = s + q * qs + i * ms, *p1 = p0 + h * ms;
-            const float2 u = *p0, v = *p1;
-            if (kDit) {
-                const float2 vw = cmul(v, w);
-                *p0 = make_float2(u.x + vw.x, u.y + vw.y);
-                *p1 = make_float2(u.x - vw.x, u.y - vw.y);
-            } else {
-                *p0 = make_float2(u.x + v.x, u.y + v.y);
-                *p1 = cmul(make_float2(u.x - v.x, u.y - v.y), w);
-            }
+// spectrum carries it).  Two radix-2 stages at a time: a thread takes the four
+// elements i, i + h, i + 2h, i + 3h and applies both stages' butterflies in
+// registers, so a length-128 transform is one radix-2 pass and three radix-4
+// passes.  Rows (ms = 1) give consecutive threads consecutive butterflies of a
+// line; columns give them consecutive lines, so a warp's accesses are
+// contiguous either way.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// a W_4: a * (-i) forward, a * (+i) inverse
+__device__ __forceinline__ float2 cmul_w4(float2 a, bool inv) {
+    return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+__device__ __forceinline__ void fft_radix2(float2 *s, int l, int ll, int qs, int ms, const float2 *tw, int tstep,
+                                           int h, bool dit, bool inv) {
+    const int half = 1 << (l - 1), total = half << ll;
+    const int wstep = (half / h) * tstep;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int q, j;
+        if (ms == 1) {
+            j = t & (half - 1);
+            q = t >> (l - 1);
+        } else {
+            q = t & ((1 << ll) - 1);
+            j = t >> ll;
         }
-        __syncthreads();
+        const int k = j & (h - 1), i = ((j - k) << 1) + k;
+        float2 w = tw[k * wstep];
+        if (inv) w.y = -w.y;
+        float2 *p0 = s + q * qs + i * ms, *p1 = p0 + h * ms;
+        const float2 u = *p0, v = *p1;
+        if (dit) {
+            const float2 vw = cmul(v, w);
+            *p0 = cadd(u, vw);
+            *p1 = csub(u, vw);
+        } else {
+            *p0 = cadd(u, v);
+            *p1 = cmul(csub(u, v), w);
+        }
+    }
+    __syncthreads();
+}
+
+// The radix-2 stages of spans h and 2h (dit) or 2h and h (dif) in one pass.
+__device__ __forceinline__ void fft_radix4(float2 *s, int l, int ll, int qs, int ms, const float2 *tw, int tstep,
+                                           int h, bool dit, bool inv) {
+    const int quarter = 1 << (l - 2), total = quarter << ll, n = 1 << l;
+    const int w1step = (n / (2 * h)) * tstep, w2step = (n / (4 * h)) * tstep;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int q, j;
+        if (ms == 1) {
+            j = t & (quarter - 1);
+            q = t >> (l - 2);
+        } else {
+            q = t & ((1 << ll) - 1);
+            j = t >> ll;
+        }
+        const int k = j & (h - 1), i = ((j - k) << 2) + k;
+        float2 w1 = tw[k * w1step], w2 = tw[k * w2step];  // W_2h^k, W_4h^k
+        if (inv) {
+            w1.y = -w1.y;
+            w2.y = -w2.y;
+        }
+        float2 *p0 = s + q * qs + i * ms;
+        const int d = h * ms;
+        const float2 x0 = p0[0], x1 = p0[d], x2 = p0[2 * d], x3 = p0[3 * d];
+        if (dit) {
+            // span h: (x0, x1), (x2, x3) by W_2h^k; span 2h: (a0, a2) by
+            // W_4h^k, (a1, a3) by W_4h^(k + h) = W_4h^k W_4
+            const float2 t1 = cmul(x1, w1), t3 = cmul(x3, w1);
+            const float2 a0 = cadd(x0, t1), a1 = csub(x0, t1), a2 = cadd(x2, t3), a3 = csub(x2, t3);
+            const float2 b2 = cmul(a2, w2), b3 = cmul_w4(cmul(a3, w2), inv);
+            p0[0] = cadd(a0, b2);
+            p0[2 * d] = csub(a0, b2);
+            p0[d] = cadd(a1, b3);
+            p0[3 * d] = csub(a1, b3);
+        } else {
+            // span 2h: (x0, x2) by W_4h^k, (x1, x3) by W_4h^(k + h); span h:
+            // (a0, a1), (a2, a3) by W_2h^k
+            const float2 a0 = cadd(x0, x2), a2 = cmul(csub(x0, x2), w2);
+            const float2 a1 = cadd(x1, x3), a3 = cmul_w4(cmul(csub(x1, x3), w2), inv);
+            p0[0] = cadd(a0, a1);
+            p0[d] = cmul(csub(a0, a1), w1);
+            p0[2 * d] = cadd(a2, a3);
+            p0[3 * d] = cmul(csub(a2, a3), w1);
+        }
+    }
+    __syncthreads();
+}
+
+template <bool kDit>
+__device__ void fft_stages(float2 *s, int n, int l, int ll, int qs, int ms, const float2 *tw, bool inv) {
+    const int tstep = kFMaxN / n;
+    if (kDit) {
+        int st = 0;
+        if (l & 1) {
+            fft_radix2(s, l, ll, qs, ms, tw, tstep, 1, true, inv);
+            st = 1;
+        }
+        for (; st + 1 < l; st += 2) fft_radix4(s, l, ll, qs, ms, tw, tstep, 1 << st, true, inv);
+    } else {
+        int st = l - 1;  // the span 2^st comes first
+        for (; st >= 1; st -= 2) fft_radix4(s, l, ll, qs, ms, tw, tstep, 1 << (st - 1), false, inv);
+        if (st == 0) fft_radix2(s, l, ll, qs, ms, tw, tstep, 1, false, inv);
     }
 }
 
@@ -303,8 +374,8 @@ __global__ void __launch_bounds__(kFThreads) k_fft_plane_fwd(const __grid_consta
     }
     edge = __syncthreads_or(edge);
     if (tid == 0) a.edge[x] = edge;
-    fft_stages<true>(fs, a.nz, a.lz, a.ny, a.nz, 1, stw, false);
-    fft_stages<true>(fs, a.ny, a.ly, a.nz, 1, a.nz, stw, false);
+    fft_stages<true>(fs, a.nz, a.lz, a.ly, a.nz, 1, stw, false);
+    fft_stages<true>(fs, a.ny, a.ly, a.lz, 1, a.nz, stw, false);
     float2 *out = a.work + (long long)x * P;
     for (int e = tid; e < P; e += kFThreads) out[e] = fs[e];
 }
@@ -319,14 +390,14 @@ __global__ void __launch_bounds__(kFThreads) k_fft_columns(const __grid_constant
         fs[(bit_reverse(x, a.lx) << a.lz) + z] = a.work[(long long)x * P + y * a.nz + z];
     }
     __syncthreads();
-    fft_stages<true>(fs, a.nx, a.lx, a.nz, 1, a.nz, stw, false);
+    fft_stages<true>(fs, a.nx, a.lx, a.lz, 1, a.nz, stw, false);
     for (int e = tid; e < L; e += kFThreads) {
         const int x = e >> a.lz, z = e & (a.nz - 1);
         const float kh = __ldg(a.khat + (long long)x * P + y * a.nz + z);
         fs[e] = make_float2(fs[e].x * kh, fs[e].y * kh);
     }
     __syncthreads();
-    fft_stages<false>(fs, a.nx, a.lx, a.nz, 1, a.nz, stw, true);
+    fft_stages<false>(fs, a.nx, a.lx, a.lz, 1, a.nz, stw, true);
     for (int e = tid; e < L; e += kFThreads) {
         const int x = e >> a.lz, z = e & (a.nz - 1);
         a.work[(long long)x * P + y * a.nz + z] = fs[(bit_reverse(x, a.lx) << a.lz) + z];
@@ -341,8 +412,8 @@ __global__ void __launch_bounds__(kFThreads) k_fft_plane_inv(const __grid_consta
     const float2 *in = a.work + (long long)x * P;
     for (int e = tid; e < P; e += kFThreads) fs[e] = in[e];
     __syncthreads();
-    fft_stages<false>(fs, a.nz, a.lz, a.ny, a.nz, 1, stw, true);
-    fft_stages<false>(fs, a.ny, a.ly, a.nz, 1, a.nz, stw, true);
+    fft_stages<false>(fs, a.nz, a.lz, a.ly, a.nz, 1, stw, true);
+    fft_stages<false>(fs, a.ny, a.ly, a.lz, 1, a.nz, stw, true);
     float *dp = a.dst + (long long)x * P, *dn = dp + a.G;
     for (int e = tid; e < P; e += kFThreads) {
         const int y = e >> a.lz, z = e & (a.nz - 1);
