@@ -111,6 +111,11 @@ class ClockSampler:
                  "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts after nvidia-smi's own start-up (NVML
+            # initialisation), once its first sample has arrived
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self

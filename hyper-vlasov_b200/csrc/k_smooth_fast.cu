@@ -217,12 +217,19 @@ const void *march_kernel(int r) {
 // set.  Both species go through one complex transform, rho_p + i rho_n: the
 // stencil's spectrum is real (the stencil is even), so the product keeps them
 // apart.  Three passes over a complex work grid:
-//   1. per x plane: load both species, flag the edge slabs, 2D transform along
-//      z then y in shared memory (radix 2, decimation in time from a
-//      bit-reversed load);
-//   2. per y: transform along x, multiply by the spectrum, inverse along x
-//      (decimation in frequency, stored back from bit-reversed order);
-//   3. per x plane: inverse along z and y, both species stored, clamped at 0.
+//   1. per x plane: load both species (rows in bit-reversed y order), flag
+//      the edge slabs, transform along z (decimation in frequency: z leaves
+//      in bit-reversed order) and along y (decimation in time: y leaves in
+//      natural order);
+//   2. per y: transform along x (decimation in time from a bit-reversed
+//      load), multiply by the spectrum, inverse along x (decimation in
+//      frequency, stored back from bit-reversed order);
+//   3. per x plane: inverse along z (bit-reversed in, natural out) and along
+//      y (natural in, bit-reversed out), both species stored from the
+//      permuted rows, clamped at 0.
+// Only whole rows are permuted in shared memory, so no pass scatters single
+// elements across banks.  The spectrum keeps z in bit-reversed order between
+// the passes, and so does khat.
 constexpr int kFThreads = 1024;
 constexpr int kFMaxN = 128;        // longest axis of the FFT form
 constexpr int kFMaxPlane = 16384;  // complex elements of a plane or column slab (128 KB)
@@ -234,7 +241,7 @@ struct FftArgs {
     const float *src;            // 2G: protons, neutrons
     float *dst;                  // 2G
     float2 *work;                // G complex
-    const float *khat;           // G: spectrum x term / G
+    const float *khat;           // G: spectrum x term / G, z in bit-reversed order
     const float2 *tw;            // kFMaxN / 2 twiddles exp(-2 pi i m / kFMaxN)
     int *edge;                   // [nx]
     float post;                  // current term / the term folded into khat
@@ -370,11 +377,11 @@ __global__ void __launch_bounds__(kFThreads) k_fft_plane_fwd(const __grid_consta
         const float rp = __ldg(sp + e), rn = __ldg(sn + e);
         if ((rp != 0.0f || rn != 0.0f) && (xedge || y < a.B || y >= a.ny - a.B || z < a.W || z >= a.nz - a.W))
             edge = 1;
-        fs[(bit_reverse(y, a.ly) << a.lz) + bit_reverse(z, a.lz)] = make_float2(rp, rn);
+        fs[(bit_reverse(y, a.ly) << a.lz) + z] = make_float2(rp, rn);
     }
     edge = __syncthreads_or(edge);
     if (tid == 0) a.edge[x] = edge;
-    fft_stages<true>(fs, a.nz, a.lz, a.ly, a.nz, 1, stw, false);
+    fft_stages<false>(fs, a.nz, a.lz, a.ly, a.nz, 1, stw, false);
     fft_stages<true>(fs, a.ny, a.ly, a.lz, 1, a.nz, stw, false);
     float2 *out = a.work + (long long)x * P;
     for (int e = tid; e < P; e += kFThreads) out[e] = fs[e];
@@ -412,18 +419,30 @@ __global__ void __launch_bounds__(kFThreads) k_fft_plane_inv(const __grid_consta
     const float2 *in = a.work + (long long)x * P;
     for (int e = tid; e < P; e += kFThreads) fs[e] = in[e];
     __syncthreads();
-    fft_stages<false>(fs, a.nz, a.lz, a.ly, a.nz, 1, stw, true);
+    fft_stages<true>(fs, a.nz, a.lz, a.ly, a.nz, 1, stw, true);
     fft_stages<false>(fs, a.ny, a.ly, a.lz, 1, a.nz, stw, true);
     float *dp = a.dst + (long long)x * P, *dn = dp + a.G;
     for (int e = tid; e < P; e += kFThreads) {
         const int y = e >> a.lz, z = e & (a.nz - 1);
-        const float2 v = fs[(bit_reverse(y, a.ly) << a.lz) + bit_reverse(z, a.lz)];
+        const float2 v = fs[(bit_reverse(y, a.ly) << a.lz) + z];
         // the exact sum is non-negative; the transform's rounding (~1e-7 of
         // the maximum) must not leave negative densities, where the Skyrme
         // term rho^gamma has no value
         dp[e] = fmaxf(v.x * a.post, 0.0f);
         dn[e] = fmaxf(v.y * a.post, 0.0f);
     }
+}
+
+// khat(kx, ky, zrev(kz)) = sum_a cx[a][kx] Y_a(ky, kz): the last sum of the
+// stencil's spectrum, one node per thread, in double.
+__global__ void k_fft_khat(int nx, int P, int nz, int lz, int na, const double *cx, const double *ya, float *khat) {
+    const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (id >= (long long)nx * P) return;
+    const int kx = (int)(id / P), q = (int)(id - (long long)kx * P);
+    double acc = 0.0;
+    for (int a = 0; a < na; a++) acc += cx[a * nx + kx] * ya[(size_t)a * P + q];
+    const int ky = q >> lz, kz = q & (nz - 1);
+    khat[(long long)kx * P + ((long long)ky << lz) + bit_reverse(kz, lz)] = (float)acc;
 }
 
 int log2_exact(int n) {
@@ -575,20 +594,12 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     const hv_run_params &pr = c->params;
     f.fft_term = (1.0 / pr.part_per_nucleon) * (1.0 / std::pow(2.0 * kPi * sig * sig, 1.5));
     const double scale = f.fft_term / (double)gg.G;
-    std::vector<float> kh((size_t)gg.G);
-    std::vector<double> acc(P);
-    for (int kx = 0; kx <= nx / 2; kx++) {
-        std::fill(acc.begin(), acc.end(), 0.0);
-        for (int a = 0; a <= A; a++) {
-            if (f.bm[a] < 0) continue;
-            const double cx = (a ? 2.0 : 1.0) * gxd[a] * std::cos(twopi * a * kx / nx);
-            const double *yr = &ya[(size_t)a * P];
-            for (int q = 0; q < P; q++) acc[q] += cx * yr[q];
-        }
-        // K is even in kx: planes kx and nx - kx are equal
-        for (int q = 0; q < P; q++) kh[(size_t)kx * P + q] = (float)(acc[q] * scale);
-        if (kx > 0 && kx < nx - kx)
-            std::copy(kh.begin() + (size_t)kx * P, kh.begin() + (size_t)(kx + 1) * P, kh.begin() + (size_t)(nx - kx) * P);
+    // cx[a][kx] = m_a g(a) cos(2 pi a kx / nx) x term / G (zero for |a| without taps)
+    std::vector<double> cxv((size_t)(A + 1) * nx, 0.0);
+    for (int a = 0; a <= A; a++) {
+        if (f.bm[a] < 0) continue;
+        for (int kx = 0; kx < nx; kx++)
+            cxv[(size_t)a * nx + kx] = (a ? 2.0 : 1.0) * gxd[a] * std::cos(twopi * a * kx / nx) * scale;
     }
     std::vector<float2> tw(kFMaxN / 2);
     for (int m = 0; m < kFMaxN / 2; m++)
@@ -597,8 +608,31 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     HV_CUDA(cudaMalloc((void **)&f.khat, sizeof(float) * gg.G));
     HV_CUDA(cudaMalloc(&f.tw, sizeof(float2) * tw.size()));
     HV_CUDA(cudaMalloc((void **)&f.edge, sizeof(int) * nx));
-    HV_CUDA(cudaMemcpy(f.khat, kh.data(), sizeof(float) * gg.G, cudaMemcpyHostToDevice));
-    HV_CUDA(cudaMemcpy(f.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+    // copies ordered on the context stream before the kernels that read
+    // them (a cudaMemcpy from pageable memory may return before its DMA ends)
+    HV_CUDA(cudaMemcpyAsync(f.tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, c->stream));
+    {
+        double *dcx = nullptr, *dya = nullptr;
+        HV_CUDA(cudaMalloc((void **)&dcx, sizeof(double) * cxv.size()));
+        if (cudaMalloc((void **)&dya, sizeof(double) * ya.size()) != cudaSuccess) {
+            cudaFree(dcx);
+            set_last_error("smoothing plan: device allocation failed");
+            return HV_ERR_CUDA;
+        }
+        cudaError_t ce =
+            cudaMemcpyAsync(dcx, cxv.data(), sizeof(double) * cxv.size(), cudaMemcpyHostToDevice, c->stream);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(dya, ya.data(), sizeof(double) * ya.size(), cudaMemcpyHostToDevice, c->stream);
+        if (ce == cudaSuccess) {
+            k_fft_khat<<<(unsigned)((gg.G + 255) / 256), 256, 0, c->stream>>>(nx, P, nz, lz, A + 1, dcx, dya,
+                                                                             f.khat);
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(c->stream);
+        cudaFree(dcx);
+        cudaFree(dya);
+        HV_CUDA(ce);
+    }
     const size_t plane = sizeof(float2) * (size_t)std::max(P, nx * nz);
     for (const void *k : {(const void *)k_fft_plane_fwd, (const void *)k_fft_columns, (const void *)k_fft_plane_inv})
         HV_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));

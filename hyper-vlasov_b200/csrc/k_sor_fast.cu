@@ -1465,6 +1465,9 @@ hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std:
     HV_CUDA(cudaMemcpy(w.args, args.data(), sizeof(SorArgs<float, float>) * n, cudaMemcpyHostToDevice));
     HV_CUDA(cudaMemcpy(w.binst, binst.data(), sizeof(int) * binst.size(), cudaMemcpyHostToDevice));
     HV_CUDA(cudaMemcpy(w.bfirst, bfirst.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    // a cudaMemcpy from pageable memory may return before its DMA ends; the
+    // wave's kernels run later on other streams
+    HV_CUDA(cudaDeviceSynchronize());
     w.ctx = cs;
     w.nblocks = (int)binst.size();
     w.smem = smem;
