@@ -736,6 +736,7 @@ void hv_fast_options_default(hv_fast_options *o) {
     o->graph_steps = 8;
     o->sor_exchange = HV_SOR_EXCHANGE_AUTO;
     o->smooth_fft = 1;
+    o->sor_omega = 0.0;
 }
 
 hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
@@ -746,7 +747,8 @@ hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
     if (o->sor_inner_min < 1 || o->sor_inner_max < o->sor_inner_min || o->sor_inner_max > 4096) return HV_ERR_BAD_ARG;
     if (o->sort_every < 0 || o->graph_steps < 0 || o->graph_steps > 64) return HV_ERR_BAD_ARG;
     if (o->sor_exchange != HV_SOR_EXCHANGE_AUTO && o->sor_exchange != HV_SOR_EXCHANGE_FLAGS) return HV_ERR_BAD_ARG;
-    if (o->smooth_fft != 0 && o->smooth_fft != 1) return HV_ERR_BAD_ARG;
+    if (o->smooth_fft < 0 || o->smooth_fft > 2) return HV_ERR_BAD_ARG;
+    if (!(o->sor_omega == 0.0 || (o->sor_omega > 0.0 && o->sor_omega < 2.0))) return HV_ERR_BAD_ARG;
     HV_CUDA(cudaSetDevice(c->device));
     HV_CUDA(cudaStreamSynchronize(c->stream));
     if (c->fused.graph) {

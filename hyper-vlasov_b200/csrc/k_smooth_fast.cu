@@ -233,6 +233,7 @@ const void *march_kernel(int r) {
 constexpr int kFThreads = 1024;
 constexpr int kFMaxN = 128;        // longest axis of the FFT form
 constexpr int kFMaxPlane = 16384;  // complex elements of a plane or column slab (128 KB)
+constexpr int kFftAutoHalfWidth = 6;  // smooth_fft = 1: stencils at least this wide
 
 struct FftArgs {
     int nx, ny, nz, lx, ly, lz;  // axis lengths and their log2
@@ -674,7 +675,9 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
     a.src = rho_raw;
     a.dst = rho;
     a.edge = nullptr;
-    if (f.fft && c->fast.smooth_fft) {
+    // auto: the transform pays off against the direct sum for wide stencils
+    const bool wide = std::max(f.A, std::max(f.B, f.W)) >= kFftAutoHalfWidth;
+    if (f.fft && (c->fast.smooth_fft == 2 || (c->fast.smooth_fft == 1 && wide))) {
         FftArgs q;
         q.nx = g.nx;
         q.ny = g.ny;

@@ -1350,11 +1350,12 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.dhy2i = 1.0 / (dy * dy);
     a.dhz2i = 1.0 / (dz * dz);
     a.ddiag = 2.0 * (a.dhx2i + a.dhy2i + a.dhz2i);
-    a.cx = (S)(sp.omega * a.dhx2i / a.ddiag);
-    a.cy = (S)(sp.omega * a.dhy2i / a.ddiag);
-    a.cz = (S)(sp.omega * a.dhz2i / a.ddiag);
-    a.cself = (S)(1.0 - sp.omega);
-    a.src_scale = sp.omega / a.ddiag;
+    const double omega = c->fast.sor_omega > 0.0 ? c->fast.sor_omega : sp.omega;
+    a.cx = (S)(omega * a.dhx2i / a.ddiag);
+    a.cy = (S)(omega * a.dhy2i / a.ddiag);
+    a.cz = (S)(omega * a.dhz2i / a.ddiag);
+    a.cself = (S)(1.0 - omega);
+    a.src_scale = omega / a.ddiag;
     a.src_c = 4.0 * kPi * kE2;
     a.tol = sp.tol;
     a.max_iter = sp.max_iter;

@@ -66,7 +66,7 @@ class hv_run_params(C.Structure):
 class hv_fast_options(C.Structure):
     _fields_ = [("sor_warm_start", C.c_int), ("sor_inner_min", C.c_int), ("sor_inner_max", C.c_int),
                 ("sort_every", C.c_int), ("graph_steps", C.c_int), ("sor_exchange", C.c_int),
-                ("smooth_fft", C.c_int)]
+                ("smooth_fft", C.c_int), ("sor_omega", C.c_double)]
 
 
 HV_WARM_PREVIOUS = 0

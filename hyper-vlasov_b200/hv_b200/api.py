@@ -122,12 +122,12 @@ class Session:
 
     def set_fast_options(self, **kw):
         """Updates fields of hv_fast_options (sor_warm_start, sor_inner_min,
-        sor_inner_max, sort_every, graph_steps, sor_exchange, smooth_fft)."""
+        sor_inner_max, sort_every, graph_steps, sor_exchange, smooth_fft, sor_omega)."""
         o = self.fast_options()
         for k, v in kw.items():
             if not hasattr(o, k):
                 raise KeyError(k)
-            setattr(o, k, int(v))
+            setattr(o, k, float(v) if k == "sor_omega" else int(v))
         L.check(self.lib.hv_ctx_set_fast_options(self._ctx, C.byref(o)), "hv_ctx_set_fast_options")
 
     KERNELS = ("particle", "smooth", "skyrme", "sor", "forces")
