@@ -116,6 +116,18 @@ __device__ __forceinline__ void deposit_at(const Geom &g, T *rho, long long off,
             if (bx && by) atomicAdd(b2 + sx2 + sy2, make_float2(dx * dy * tz, dx * dy * dz));
             return;
         }
+        // nz a multiple of 4 and the base index 1 mod 4: the z-pair is the
+        // middle of a 16-byte-aligned float4 whose outer two elements (inside
+        // the row: z0 - 1 >= 0, z0 + 2 < nz) receive exact zeros
+        if (bz && (nz & 3) == 0 && ((off + x0 * sx + y0 * sy + z0) & 3) == 1) {
+            float4 *b4 = reinterpret_cast<float4 *>(b - 1);
+            const long long sx4 = sx / 4, sy4 = sy / 4;
+            atomicAdd(b4, make_float4(0.0f, tx * ty * tz, tx * ty * dz, 0.0f));
+            if (bx) atomicAdd(b4 + sx4, make_float4(0.0f, dx * ty * tz, dx * ty * dz, 0.0f));
+            if (by) atomicAdd(b4 + sy4, make_float4(0.0f, tx * dy * tz, tx * dy * dz, 0.0f));
+            if (bx && by) atomicAdd(b4 + sx4 + sy4, make_float4(0.0f, dx * dy * tz, dx * dy * dz, 0.0f));
+            return;
+        }
     }
     atomicAdd(b, tx * ty * tz);
     if (bx) atomicAdd(b + sx, dx * ty * tz);
