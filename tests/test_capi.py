@@ -148,3 +148,28 @@ def test_context_rejects_bad_arguments_before_touching_a_device(hv):
         _lib.HV_ERR_BAD_ARG
     assert lib.hv_ctx_destroy(None) == _lib.HV_OK
     assert lib.hv_run(None, 1, 0, None) == _lib.HV_ERR_BAD_ARG
+
+
+def test_ctypes_structs_match_the_c_layout(hv, tmp_path):
+    """Every struct that the Python mirror declares has the C header's size
+    and field offsets (gcc on a generated program that prints them)."""
+    from hv_b200 import _lib
+    structs = [(n, c) for n, c in vars(_lib).items()
+               if isinstance(c, type) and issubclass(c, C.Structure) and n.startswith("hv_")]
+    assert len(structs) >= 8
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "hv_b200.h"', 'int main(void) {']
+    for name, cls in structs:
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", HEADER_DIR, str(src), "-o", str(exe)], check=True)
+    out = dict(ln.rsplit(" ", 1) for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                          check=True).stdout.split("\n") if ln)
+    for name, cls in structs:
+        assert int(out[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(out[f"{name}.{fname}"]) == getattr(cls, fname).offset, f"{name}.{fname}"
