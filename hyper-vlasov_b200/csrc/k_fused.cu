@@ -10,6 +10,7 @@
 // so x and k are read and written once per step (48 B per particle in
 // float).  The closing half kick of the last step is applied by
 // k_close_kick when hv_run returns, leaving the state the plain path leaves.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -244,31 +245,43 @@ __global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__re
 template <typename T>
 __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U, const double *__restrict__ phi,
                             T *F4) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 2 * g.G) return;
-    const bool prot = i < g.G;
-    const long long id = prot ? i : i - g.G;
-    const T *Us = U + (prot ? 0 : g.G);
+    // block (j, i, species): one z row, so no division recovers the indices
+    const int j = blockIdx.x, ii = blockIdx.y;
+    const bool prot = blockIdx.z == 0;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long sx = (long long)ny * nz, sy = nz;
-    const int k = (int)(id % nz), j = (int)((id / nz) % ny), ii = (int)(id / sx);
+    const T *Us = U + (prot ? 0 : g.G);
+    const long long row = (long long)ii * sx + (long long)j * sy;
     auto u = [&](long long q) { return prot ? Us[q] + (T)phi[q] : Us[q]; };
-    T gx, gy, gz;
-    if (ii == 0) gx = (u(id + sx) - u(id)) * idx;
-    else if (ii == nx - 1) gx = (u(id) - u(id - sx)) * idx;
-    else gx = (u(id + sx) - u(id - sx)) * (T(0.5) * idx);
-    if (j == 0) gy = (u(id + sy) - u(id)) * idy;
-    else if (j == ny - 1) gy = (u(id) - u(id - sy)) * idy;
-    else gy = (u(id + sy) - u(id - sy)) * (T(0.5) * idy);
-    if (k == 0) gz = (u(id + 1) - u(id)) * idz;
-    else if (k == nz - 1) gz = (u(id) - u(id - 1)) * idz;
-    else gz = (u(id + 1) - u(id - 1)) * (T(0.5) * idz);
-    T *o = F4 + 4 * i;
-    o[0] = -gx;
-    o[1] = -gy;
-    o[2] = -gz;
-    o[3] = T(0);
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+        const long long id = row + k;
+        const T uc = u(id);
+        T gx, gy, gz;
+        if (ii == 0) gx = (u(id + sx) - uc) * idx;
+        else if (ii == nx - 1) gx = (uc - u(id - sx)) * idx;
+        else gx = (u(id + sx) - u(id - sx)) * (T(0.5) * idx);
+        if (j == 0) gy = (u(id + sy) - uc) * idy;
+        else if (j == ny - 1) gy = (uc - u(id - sy)) * idy;
+        else gy = (u(id + sy) - u(id - sy)) * (T(0.5) * idy);
+        if (k == 0) gz = (u(id + 1) - uc) * idz;
+        else if (k == nz - 1) gz = (uc - u(id - 1)) * idz;
+        else gz = (u(id + 1) - u(id - 1)) * (T(0.5) * idz);
+        const long long i = (prot ? 0 : g.G) + id;
+        if constexpr (sizeof(T) == 4) {
+            reinterpret_cast<float4 *>(F4)[i] = make_float4(-gx, -gy, -gz, 0.0f);
+        } else {
+            T *o = F4 + 4 * i;
+            o[0] = -gx;
+            o[1] = -gy;
+            o[2] = -gz;
+            o[3] = T(0);
+        }
+    }
 }
+
+// k_forces_f4's launch: one block per (y row, x plane, species), threads along z
+inline dim3 forces_grid(const Geom &g) { return dim3((unsigned)g.ny, (unsigned)g.nx, 2u); }
+inline dim3 forces_block(const Geom &g) { return dim3((unsigned)std::min(128, (g.nz + 31) / 32 * 32)); }
 
 template <typename T>
 __global__ void k_pack_f4(long long n, const T *__restrict__ Fx, const T *__restrict__ Fy, const T *__restrict__ Fz,
@@ -444,7 +457,7 @@ hv_status enqueue_phase_c(hv_ctx *c) {
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
     {
         ProfScope ps(c, HV_K_FORCES);
-        k_forces_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
+        k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
                                                                   reinterpret_cast<T *>(f.F4));
     }
     HV_CUDA(cudaGetLastError());
@@ -498,7 +511,8 @@ hv_status initial_typed(hv_ctx *c) {
     HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, nullptr, kRing, false));
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
-    k_forces_f4<T><<<nblk(2 * g.G, 256), 256, 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64, reinterpret_cast<T *>(f.F4));
+    k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
+                                                                       reinterpret_cast<T *>(f.F4));
     HV_CUDA(cudaGetLastError());
     int status[3] = {0, 0, 0};
     HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
