@@ -476,6 +476,24 @@ hv_status enqueue_step(hv_ctx *c) {
     return enqueue_phase_c<T>(c);
 }
 
+// Starting phi of the fused path's first solve inside the grid: the field of
+// a uniformly charged sphere of the protons (radius 1.2 A^(1/3) fm, centred
+// like the monopole boundary): 1.44 Z / r outside, 1.44 Z (3 R^2 - r^2) /
+// (2 R^3) inside.  The boundary nodes keep their values; the solve's stopping
+// rule is unchanged, so only its iteration count depends on this guess.
+__global__ void k_sphere_guess(Geom g, int Z, double R, double *phi) {
+    const int j = blockIdx.x, i = blockIdx.y;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    if (i == 0 || j == 0 || i == nx - 1 || j == ny - 1) return;
+    const double x = g.dmx * (2.0 * i / nx - 1.0), y = g.dmy * (2.0 * j / ny - 1.0);
+    for (int k = 1 + threadIdx.x; k < nz - 1; k += blockDim.x) {
+        const double z = g.dmz * (2.0 * k / nz - 1.0);
+        const double r = sqrt(x * x + y * y + z * z);
+        const double v = r >= R ? 1.44 * Z / r : 1.44 * Z * (3.0 * R * R - r * r) / (2.0 * R * R * R);
+        phi[((long long)i * ny + j) * nz + k] = v;
+    }
+}
+
 // The initial field solve of cpu_simulate (src/hyper_vlasov.cpp:53-62) on the
 // fused kernels: deposit, smoothing, Coulomb boundary (double monopole,
 // include/tools.hpp:283-300), Skyrme, SOR from phi = 0 inside, forces, and the
@@ -501,6 +519,9 @@ hv_status initial_typed(hv_ctx *c) {
     if (!c->boundary_set) {
         HV_CUDA(cudaMemsetAsync(f.phi64, 0, sizeof(double) * g.G, c->stream));
         HV_TRY(launch_boundary<double>(c, f.phi64));
+        const double R = 1.2 * std::cbrt((double)(c->params.z + c->params.n));
+        k_sphere_guess<<<dim3((unsigned)g.ny, (unsigned)g.nx), 128, 0, c->stream>>>(g, c->params.z, R, f.phi64);
+        HV_CUDA(cudaGetLastError());
         c->boundary_set = true;
     } else {
         k_widen<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, s.phi, f.phi64);
