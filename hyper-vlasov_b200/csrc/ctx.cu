@@ -6,6 +6,8 @@
 #include <new>
 #include <string>
 
+#include <cub/cub.cuh>
+
 #include "hv_internal.h"
 
 namespace hv {
@@ -172,6 +174,53 @@ __global__ void k_permute(int n, const int *__restrict__ perm, const T *__restri
     if (s < n) out[s] = in[perm[s]];
 }
 
+// Keys of the fused path's slot re-sort: species * (G + 1) + the particle's
+// CIC base cell, G for a particle outside the grid, so that the sort keeps the
+// protons' slots before the neutrons'.
+template <typename T>
+__global__ void k_slot_keys(Geom g, int protons, int total, const T *__restrict__ x, const T *__restrict__ y,
+                            const T *__restrict__ z, unsigned int *keys, int *vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const T cx = (g.nx / T(2.0)) * (x[i] / T(g.dmx) + T(1.0));
+    const T cy = (g.ny / T(2.0)) * (y[i] / T(g.dmy) + T(1.0));
+    const T cz = (g.nz / T(2.0)) * (z[i] / T(g.dmz) + T(1.0));
+    long long cell = g.G;
+    if (cx >= T(0) && cy >= T(0) && cz >= T(0) && cx < g.nx && cy < g.ny && cz < g.nz)
+        cell = ((long long)(int)cx * g.ny + (int)cy) * g.nz + (int)cz;
+    keys[i] = (unsigned int)(cell + (i < protons ? 0 : g.G + 1));
+    vals[i] = i;
+}
+
+template <typename T>
+hv_status sort_slots_typed(hv_ctx *c, State<T> &s) {
+    const int n = c->total;
+    if (n == 0) return HV_OK;
+    Scratch &sc = c->scratch;
+    if (!sc.sort_tmp) HV_CUDA(cudaMalloc(&sc.sort_tmp, sizeof(double) * (size_t)n));
+    k_slot_keys<T><<<div_up(n, 256), 256, 0, c->stream>>>(c->geom, c->protons, n, s.x, s.y, s.z, sc.keys, sc.vals);
+    HV_CUDA(cudaGetLastError());
+    const unsigned long long nkeys = 2ull * ((unsigned long long)c->geom.G + 1);
+    int end_bit = 1;
+    while ((1ull << end_bit) < nkeys) end_bit++;
+    size_t bytes = sc.cub_tmp_bytes;
+    HV_CUDA(cub::DeviceRadixSort::SortPairs(sc.cub_tmp, bytes, sc.keys, sc.keys_alt, sc.vals, sc.vals_alt, n, 0,
+                                            end_bit, c->stream));
+    // every per-particle array and the caller permutation follow the new order
+    T *tmp = reinterpret_cast<T *>(sc.sort_tmp);
+    T *arrs[] = {s.x, s.y, s.z, s.kx, s.ky, s.kz, s.fx, s.fy, s.fz};
+    for (T *a : arrs) {
+        k_permute<T><<<div_up(n, 256), 256, 0, c->stream>>>(n, sc.vals_alt, a, tmp);
+        HV_CUDA(cudaMemcpyAsync(a, tmp, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    int *ptmp = reinterpret_cast<int *>(sc.sort_tmp);
+    k_permute<int><<<div_up(n, 256), 256, 0, c->stream>>>(n, sc.vals_alt, c->perm, ptmp);
+    HV_CUDA(cudaMemcpyAsync(c->perm, ptmp, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, c->stream));
+    HV_CUDA(cudaGetLastError());
+    c->permuted = true;
+    return HV_OK;
+}
+
 template <typename T>
 T *part_ptr(State<T> &s, int which) {
     switch (which) {
@@ -299,6 +348,14 @@ hv_status plain_step(hv_ctx *c, hv_observables *row) {
 bool slots_permuted(hv_ctx *c) { return c->permuted; }
 
 }  // namespace
+
+// Re-sorts the particle slots by CIC cell within each species (a stable radix
+// sort), so that the particles of a warp gather and deposit in few cells; the
+// fused path calls it every hv_fast_options.sort_every steps, between graph
+// launches.  Downloads and uploads follow the slot permutation.
+hv_status fused_sort_slots(hv_ctx *c) {
+    return c->prec == HV_F64 ? sort_slots_typed<double>(c, c->d64) : sort_slots_typed<float>(c, c->d32);
+}
 
 hv_status plain_step_f64(hv_ctx *c, hv_observables *row) { return plain_step<double>(c, row); }
 
@@ -487,7 +544,7 @@ hv_status hv_ctx_destroy(hv_ctx *c) {
     free_state(c->d32);
     Scratch &s = c->scratch;
     void *ptrs[] = {c->perm, c->taps_dev, s.partials, s.maxbits, s.result, s.keys, s.keys_alt, s.vals, s.vals_alt,
-                    s.cell_start, s.cub_tmp};
+                    s.cell_start, s.cub_tmp, s.sort_tmp};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (s.h_result) cudaFreeHost(s.h_result);

@@ -78,6 +78,7 @@ struct Scratch {
     int *cell_start = nullptr;      // [2G + 1]
     void *cub_tmp = nullptr;
     size_t cub_tmp_bytes = 0;
+    void *sort_tmp = nullptr;       // total x 8 bytes: the slot re-sort's gather buffer
 };
 
 // Partition and device buffers of the persistent SOR solver (k_sor_fast.cu).
@@ -136,6 +137,7 @@ struct Fused {
     double *obs_rows_dev = nullptr;  // reduced rows (device)
     cudaGraphExec_t graph = nullptr;
     int graph_len = 0;
+    int last_sort = -(1 << 30);   // step of the last slot re-sort
     bool prev_valid = false;      // phi64_prev holds the previous step's phi
     bool f4_current = false;      // F4 holds the forces of the current positions
     int m_hint = 8;               // iterations of the previous SOR solve (seeds the first cycle)
@@ -194,6 +196,7 @@ template <typename T>
 hv_status launch_deposit_atomic(hv_ctx *c, const T *x, const T *y, const T *z, T *rho);
 template <typename T>
 hv_status launch_deposit_sorted(hv_ctx *c, const T *x, const T *y, const T *z, T *rho);
+hv_status fused_sort_slots(hv_ctx *c);
 template <typename T>
 hv_status launch_smooth(hv_ctx *c, const T *rho_raw, T *rho);
 template <typename T>

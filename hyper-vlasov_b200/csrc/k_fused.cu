@@ -649,6 +649,13 @@ hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
     std::vector<int> its(kRing);
     while (done < n_steps) {
         const int k = std::min(chunk, n_steps - done);
+        // slot re-sort by cell every sort_every steps (at most once per
+        // chunk), outside the graph: its kernels keep their pointers
+        const int step_now = c->step_index + done;
+        if (c->fast.sort_every > 0 && step_now - f.last_sort >= c->fast.sort_every) {
+            HV_TRY(fused_sort_slots(c));
+            f.last_sort = step_now;
+        }
         bool launched = false;
         if (c->fast.graph_steps > 0 && k == chunk && !c->prof.on) {
             if (!f.graph || f.graph_len != k) {

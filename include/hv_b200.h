@@ -313,7 +313,11 @@ typedef struct hv_fast_options {
                              previous solve's iterations (at most max), the
                              later ones follow the observed rate, clamped to
                              [min, max]                                        */
-    int sort_every;       /* re-sort particle slots by cell every n steps (0 = off) */
+    int sort_every;       /* hv_run on HV_PATH_FUSED re-sorts the particle slots
+                             by cell (protons before neutrons) every n steps, at
+                             most once per graph launch (0 = off); downloads
+                             stay in the caller's order.  Batched runs keep
+                             their slot order                                  */
     int graph_steps;      /* steps captured per CUDA graph launch (0 = no graph) */
     int sor_exchange;     /* hv_sor_exchange                                    */
     int smooth_fft;       /* Gaussian smoothing as an FFT convolution where it is
