@@ -572,7 +572,18 @@ def our_arm(args, world, rank, local):
     fft = pow2 and (opts.smooth_fft == 2 or (opts.smooth_fft == 1 and half_width >= 6))
     launches_per_step = 6 + (3 if fft else 0)
     chunk = opts.graph_steps or 8
-    gpu_launches = K * launches_per_step + math.ceil(K / chunk)
+    # slot re-sorts at chunk starts (as the fused run schedules them): each
+    # launches its key kernel and ten gathers of ours (the radix sort is CUB's)
+    resorts, last, step = 0, -(1 << 30), 0
+    for n_run in (W, K):
+        done = 0
+        while done < n_run:
+            if opts.sort_every > 0 and step + done - last >= opts.sort_every:
+                last = step + done
+                resorts += n_run == K
+            done += min(chunk, n_run - done)
+        step += n_run
+    gpu_launches = K * launches_per_step + math.ceil(K / chunk) + 11 * resorts
     sess.close()
 
     # the same K steps from the other initial guess of the solve (the
