@@ -197,7 +197,6 @@ hv_status sort_slots_typed(hv_ctx *c, State<T> &s) {
     const int n = c->total;
     if (n == 0) return HV_OK;
     Scratch &sc = c->scratch;
-    if (!sc.sort_tmp) HV_CUDA(cudaMalloc(&sc.sort_tmp, sizeof(double) * (size_t)n));
     k_slot_keys<T><<<div_up(n, 256), 256, 0, c->stream>>>(c->geom, c->protons, n, s.x, s.y, s.z, sc.keys, sc.vals);
     HV_CUDA(cudaGetLastError());
     const unsigned long long nkeys = 2ull * ((unsigned long long)c->geom.G + 1);
@@ -262,13 +261,12 @@ hv_status upload_part(hv_ctx *c, int which, const void *host) {
     if (!host) return HV_ERR_BAD_ARG;
     const size_t bytes = sizeof(T) * c->total;
     if (slots_permuted(c)) {
-        // stage in caller order, then gather into slot order
-        T *stage = nullptr;
-        HV_CUDA(cudaMallocAsync((void **)&stage, bytes, c->stream));
+        // stage in caller order (the re-sort's gather buffer), then gather
+        // into slot order
+        T *stage = reinterpret_cast<T *>(c->scratch.sort_tmp);
         HV_CUDA(cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, c->stream));
         k_permute<T><<<div_up(c->total, 256), 256, 0, c->stream>>>(c->total, c->perm, stage, d);
         HV_CUDA(cudaGetLastError());
-        HV_CUDA(cudaFreeAsync(stage, c->stream));
     } else {
         HV_CUDA(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, c->stream));
     }
@@ -283,12 +281,10 @@ hv_status download_part(hv_ctx *c, int which, void *host) {
     if (!host) return HV_ERR_BAD_ARG;
     const size_t bytes = sizeof(T) * c->total;
     if (slots_permuted(c)) {
-        T *stage = nullptr;
-        HV_CUDA(cudaMallocAsync((void **)&stage, bytes, c->stream));
+        T *stage = reinterpret_cast<T *>(c->scratch.sort_tmp);
         k_unpermute<T><<<div_up(c->total, 256), 256, 0, c->stream>>>(c->total, c->perm, d, stage);
         HV_CUDA(cudaGetLastError());
         HV_CUDA(cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, c->stream));
-        HV_CUDA(cudaFreeAsync(stage, c->stream));
     } else {
         HV_CUDA(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, c->stream));
     }
@@ -364,12 +360,10 @@ template <typename T>
 hv_status download_slots_t(hv_ctx *c, const T *d, T *host) {
     const size_t bytes = sizeof(T) * c->total;
     if (slots_permuted(c)) {
-        T *stage = nullptr;
-        HV_CUDA(cudaMallocAsync((void **)&stage, bytes, c->stream));
+        T *stage = reinterpret_cast<T *>(c->scratch.sort_tmp);
         k_unpermute<T><<<div_up(c->total, 256), 256, 0, c->stream>>>(c->total, c->perm, d, stage);
         HV_CUDA(cudaGetLastError());
         HV_CUDA(cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, c->stream));
-        HV_CUDA(cudaFreeAsync(stage, c->stream));
     } else {
         HV_CUDA(cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, c->stream));
     }
@@ -524,7 +518,8 @@ hv_status hv_ctx_create(const hv_world *world, int protons, int neutrons, hv_pre
         cudaMalloc((void **)&s.vals, sizeof(int) * n) != cudaSuccess ||
         cudaMalloc((void **)&s.vals_alt, sizeof(int) * n) != cudaSuccess ||
         cudaMalloc((void **)&s.cell_start, sizeof(int) * (2 * c->geom.G + 1)) != cudaSuccess ||
-        cudaMalloc(&s.cub_tmp, s.cub_tmp_bytes > 0 ? s.cub_tmp_bytes : 16) != cudaSuccess)
+        cudaMalloc(&s.cub_tmp, s.cub_tmp_bytes > 0 ? s.cub_tmp_bytes : 16) != cudaSuccess ||
+        cudaMalloc(&s.sort_tmp, sizeof(double) * (size_t)n) != cudaSuccess)
         return fail(cuda_status(cudaErrorMemoryAllocation, "scratch"));
     k_iota<<<div_up(n, 256), 256, 0, c->stream>>>(n, c->perm);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(cuda_status(cudaGetLastError(), "create"));

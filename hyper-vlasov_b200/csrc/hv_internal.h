@@ -78,7 +78,8 @@ struct Scratch {
     int *cell_start = nullptr;      // [2G + 1]
     void *cub_tmp = nullptr;
     size_t cub_tmp_bytes = 0;
-    void *sort_tmp = nullptr;       // total x 8 bytes: the slot re-sort's gather buffer
+    void *sort_tmp = nullptr;       // total x 8 bytes: the slot re-sort's gather buffer, and the stage of
+                                    // uploads and downloads in permuted slot order
 };
 
 // Partition and device buffers of the persistent SOR solver (k_sor_fast.cu).
