@@ -97,9 +97,10 @@ def build(force=False, jobs=None, verbose=False):
     return LIB
 
 
-def build_oracle(verbose=False):
-    """Builds the checker libraries under oracle/ (and oracle/_ref/ where the
-    reference tree is present)."""
+def build_oracle(verbose=False, reference_root=None):
+    """Builds the checker libraries under oracle/, and oracle/_ref/ from the
+    reference tree at reference_root (or $HV_REFERENCE_ROOT) when one is given
+    and present; without one, oracle/_ref/ is left as it is."""
     oracle = os.path.join(ROOT, "oracle")
     env = dict(os.environ)
     env.pop("CC", None)
@@ -107,8 +108,8 @@ def build_oracle(verbose=False):
     r = subprocess.run(["make", "-s", "-C", oracle, "all"], capture_output=True, text=True, env=env)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
-    ref_root = env.get("HV_REFERENCE_ROOT", "/root/reference")
-    if os.path.isdir(os.path.join(ref_root, "include")):
+    ref_root = reference_root or env.get("HV_REFERENCE_ROOT")
+    if ref_root and os.path.isdir(os.path.join(ref_root, "include")):
         r = subprocess.run(["make", "-s", "-C", oracle, "ref", f"REF_ROOT={ref_root}"], capture_output=True,
                            text=True, env=env)
         if r.returncode != 0:
@@ -120,11 +121,12 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--jobs", type=int, default=None)
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--reference-root", default=None, help="reference tree to build oracle/_ref/ from")
     a = ap.parse_args()
     try:
         build(a.force, a.jobs, verbose=True)
         if not a.no_oracle:
-            build_oracle(verbose=True)
+            build_oracle(verbose=True, reference_root=a.reference_root)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

@@ -237,6 +237,12 @@ struct Adjoint {
     double *mu = nullptr;    // G, zero on the boundary
     double *partials = nullptr;
     double *acc = nullptr;   // 4: dJ/d(A, B, gamma, C)
+    // the slot-to-caller permutation of the checkpointed particle state (the
+    // plain steps of a forward run keep the slot order, so one copy serves all
+    // checkpoints); restored with them, since a fused run between forward and
+    // backward may re-sort the slots
+    int *perm = nullptr;
+    bool permuted = false;
     int nb_sky = 0;
     int adj_sor_its = 0;     // iterations of the transposed solves of the last backward pass
     bool ready = false;      // a forward run's checkpoints are held
@@ -248,6 +254,7 @@ void adjoint_release(hv_ctx *c) {
     double *bufs[] = {a->ckpt, a->seg, a->lam, a->LF, a->LU, a->Lrho, a->Lraw, a->src, a->mu, a->partials, a->acc};
     for (double *p : bufs)
         if (p) cudaFree(p);
+    if (a->perm) cudaFree(a->perm);
     delete a;
     c->adjoint = nullptr;
 }
@@ -283,6 +290,10 @@ hv_status adjoint_alloc(hv_ctx *c, int steps, int every) {
     a->nb_sky = 2 * c->sm_count;
     HV_TRY(alloc(&a->partials, 4 * (size_t)a->nb_sky));
     HV_TRY(alloc(&a->acc, 4));
+    if (cudaMalloc((void **)&a->perm, sizeof(int) * (N > 0 ? N : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return HV_ERR_OOM;
+    }
     a->cap_steps = steps;
     a->cap_every = every;
     return HV_OK;
@@ -318,6 +329,8 @@ hv_status load_ckpt(hv_ctx *c, int s) {
     for (int k = 0; k < 9; k++)
         if (N) HV_CUDA(cudaMemcpyAsync(dst[k], src + k * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
     HV_CUDA(cudaMemcpyAsync(st.phi, src + 9 * N, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+    if (N) HV_CUDA(cudaMemcpyAsync(c->perm, a->perm, sizeof(int) * N, cudaMemcpyDeviceToDevice, c->stream));
+    c->permuted = a->permuted;
     c->step_index = a->ck_step[s];
     c->excited = a->ck_excited[s];
     c->boundary_set = a->ck_boundary[s];
@@ -404,6 +417,8 @@ hv_status hv_adjoint_forward(hv_ctx *c, int n_steps, int checkpoint_every, hv_ob
     a->steps = n_steps;
     a->every = every;
     a->nseg = (n_steps + every - 1) / every;
+    if (c->total) HV_CUDA(cudaMemcpyAsync(a->perm, c->perm, sizeof(int) * c->total, cudaMemcpyDeviceToDevice, c->stream));
+    a->permuted = c->permuted;
     for (int n = 0; n < n_steps; n++) {
         if (n % every == 0) HV_TRY(save_ckpt(c, n / every));
         hv_observables *row = obs ? &obs[n] : nullptr;

@@ -3,8 +3,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include <cub/cub.cuh>
 
@@ -789,6 +792,10 @@ void hv_fast_options_default(hv_fast_options *o) {
     o->sor_exchange = HV_SOR_EXCHANGE_AUTO;
     o->smooth_fft = 1;
     o->sor_omega = 0.0;
+    o->sor_wait_limit = 0;
+    o->sor_coarse = 1;
+    o->sor_coarse_sweeps = 16;
+    o->deposit_aggregate = 1;
 }
 
 hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
@@ -801,6 +808,10 @@ hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
     if (o->sor_exchange != HV_SOR_EXCHANGE_AUTO && o->sor_exchange != HV_SOR_EXCHANGE_FLAGS) return HV_ERR_BAD_ARG;
     if (o->smooth_fft < 0 || o->smooth_fft > 2) return HV_ERR_BAD_ARG;
     if (!(o->sor_omega == 0.0 || (o->sor_omega > 0.0 && o->sor_omega < 2.0))) return HV_ERR_BAD_ARG;
+    if (o->sor_wait_limit < 0) return HV_ERR_BAD_ARG;
+    if (o->sor_coarse < 0 || o->sor_coarse > 1 || o->sor_coarse_sweeps < 1 || o->sor_coarse_sweeps > 4096)
+        return HV_ERR_BAD_ARG;
+    if (o->deposit_aggregate < 0 || o->deposit_aggregate > 1) return HV_ERR_BAD_ARG;
     HV_CUDA(cudaSetDevice(c->device));
     HV_CUDA(cudaStreamSynchronize(c->stream));
     if (c->fused.graph) {
@@ -829,6 +840,13 @@ hv_status hv_ctx_set_profiling(hv_ctx *c, int enable) {
         c->prof.launches[k] = 0;
     }
     return HV_OK;
+}
+
+hv_status hv_ctx_autotune(hv_ctx *c, int trial_steps, hv_autotune_report *report) {
+    if (!c || trial_steps < 1 || trial_steps > 1024) return HV_ERR_BAD_ARG;
+    HV_CUDA(cudaSetDevice(c->device));
+    if (report) std::memset(report, 0, sizeof(*report));
+    return fused_autotune(c, trial_steps, report);
 }
 
 hv_status hv_ctx_kernel_times(hv_ctx *c, double *total_ms, int *launches, int n) {
@@ -870,19 +888,139 @@ hv_status hv_run(hv_ctx *c, int n_steps, int path, hv_observables *obs) {
     return HV_OK;
 }
 
+}  // extern "C"
+
+namespace hv {
+namespace {
+
+// Contexts kept between hv_simulate calls, keyed by what fixes their device
+// buffers: device, world, particle counts and precision.  A context is taken
+// out of the cache for the length of a call, so concurrent calls never share
+// one; at most kSimCacheMax idle contexts are kept (the oldest is destroyed
+// first).  The cache is never destroyed at exit: freeing device memory after
+// the CUDA runtime has shut down is not safe, and the process's memory goes
+// with it anyway.
+struct SimKey {
+    int device;
+    hv_world world;
+    int protons, neutrons;
+    hv_precision prec;
+};
+
+bool same_key(const SimKey &a, const SimKey &b) {
+    if (a.device != b.device || a.protons != b.protons || a.neutrons != b.neutrons || a.prec != b.prec) return false;
+    for (int i = 0; i < 3; i++)
+        if (a.world.n[i] != b.world.n[i] || a.world.d_max[i] != b.world.d_max[i]) return false;
+    return true;
+}
+
+bool same_params(const hv_run_params &a, const hv_run_params &b) {
+    return a.z == b.z && a.n == b.n && a.part_per_nucleon == b.part_per_nucleon && a.sigma_r == b.sigma_r &&
+           a.dt == b.dt && a.t_exc == b.t_exc && a.eta_exc == b.eta_exc && a.skyrme.A == b.skyrme.A &&
+           a.skyrme.B == b.skyrme.B && a.skyrme.C == b.skyrme.C && a.skyrme.gamma == b.skyrme.gamma &&
+           a.sor.omega == b.sor.omega && a.sor.tol == b.sor.tol && a.sor.criterion == b.sor.criterion &&
+           a.sor.max_iter == b.sor.max_iter && a.deposit_mode == b.deposit_mode;
+}
+
+constexpr size_t kSimCacheMax = 4;
+std::mutex g_sim_mutex;
+std::vector<std::pair<SimKey, hv_ctx *>> &sim_cache() {
+    static auto *cache = new std::vector<std::pair<SimKey, hv_ctx *>>();
+    return *cache;
+}
+
+hv_ctx *sim_take(const SimKey &k) {
+    std::lock_guard<std::mutex> lock(g_sim_mutex);
+    auto &cache = sim_cache();
+    for (size_t i = 0; i < cache.size(); i++)
+        if (same_key(cache[i].first, k)) {
+            hv_ctx *c = cache[i].second;
+            cache.erase(cache.begin() + (long)i);
+            return c;
+        }
+    return nullptr;
+}
+
+void sim_put(const SimKey &k, hv_ctx *c) {
+    hv_ctx *evict = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_sim_mutex);
+        auto &cache = sim_cache();
+        cache.emplace_back(k, c);
+        if (cache.size() > kSimCacheMax) {
+            evict = cache.front().second;
+            cache.erase(cache.begin());
+        }
+    }
+    if (evict) hv_ctx_destroy(evict);
+}
+
+// A cached context brought back to the state hv_ctx_create leaves: step 0,
+// not excited, Coulomb boundary and fields unset, phi zero, identity slot
+// order and the fused solver's first-cycle seed at its initial value, so that
+// the call computes what it would on a new context.  Plans, graphs and
+// buffers are kept (new parameters re-plan the fused path).
+hv_status sim_reset(hv_ctx *c, const hv_run_params *params) {
+    HV_CUDA(cudaSetDevice(c->device));
+    if (!same_params(c->params, *params)) HV_TRY(hv_ctx_set_params(c, params));
+    c->step_index = 0;
+    c->excited = false;
+    c->boundary_set = false;
+    c->fields_valid = false;
+    const size_t es = c->prec == HV_F64 ? 8 : 4;
+    void *phi = c->prec == HV_F64 ? (void *)c->d64.phi : (void *)c->d32.phi;
+    HV_CUDA(cudaMemsetAsync(phi, 0, es * (size_t)c->geom.G, c->stream));
+    if (c->permuted && c->total > 0) {
+        k_iota<<<div_up(c->total, 256), 256, 0, c->stream>>>(c->total, c->perm);
+        HV_CUDA(cudaGetLastError());
+    }
+    c->permuted = false;
+    fused_invalidate(c);
+    c->fused.m_hint = Fused().m_hint;
+    return HV_OK;
+}
+
+}  // namespace
+}  // namespace hv
+
+extern "C" {
+
 hv_status hv_simulate(const hv_world *world, int protons, int neutrons, hv_precision prec,
                       const hv_run_params *params, int path, int n_steps, void *x, void *y, void *z, void *kx,
                       void *ky, void *kz, hv_observables *obs) {
-    if (n_steps < 0) return HV_ERR_BAD_ARG;
+    if (n_steps < 0 || !world || !params) return HV_ERR_BAD_ARG;
     if (protons + neutrons > 0 && (!x || !y || !z || !kx || !ky || !kz)) return HV_ERR_BAD_ARG;
-    hv_ctx *c = nullptr;
-    HV_TRY(hv_ctx_create(world, protons, neutrons, prec, params, -1, &c));
-    hv_status st = hv_upload_particles(c, x, y, z, kx, ky, kz);
+    HV_TRY(check_world(world));
+    HV_TRY(check_params(params));
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error("no CUDA device");
+        return HV_ERR_NO_DEVICE;
+    }
+    const SimKey key{device, *world, protons, neutrons, prec};
+    hv_ctx *c = sim_take(key);
+    hv_status st = HV_OK;
+    if (c) st = sim_reset(c, params);
+    else st = hv_ctx_create(world, protons, neutrons, prec, params, device, &c);
+    if (st == HV_OK) st = hv_upload_particles(c, x, y, z, kx, ky, kz);
     // hv_run performs the initial field solve on the chosen path
     if (st == HV_OK) st = hv_run(c, n_steps, path, obs);
     if (st == HV_OK) st = hv_download_particles(c, x, y, z, kx, ky, kz);
-    hv_ctx_destroy(c);
+    if (!c) return st;
+    if (st == HV_OK) sim_put(key, c);  // kept for the next call of the same shape
+    else hv_ctx_destroy(c);
     return st;
+}
+
+hv_status hv_simulate_release(void) {
+    std::vector<std::pair<SimKey, hv_ctx *>> held;
+    {
+        std::lock_guard<std::mutex> lock(g_sim_mutex);
+        held.swap(sim_cache());
+    }
+    for (auto &e : held) hv_ctx_destroy(e.second);
+    return HV_OK;
 }
 
 }  // extern "C"

@@ -101,6 +101,12 @@ struct SorFast {
     unsigned *bar = nullptr;   // [0] arrivals, [1] generation
     int *status = nullptr;     // [0] error, [1] iterations, [2] converged, [3] m hint
     double *metric = nullptr;  // final stopping quantity
+    // coarse-grid correction: factor F (0: none for this grid), interior
+    // extents of the coarse grid, restriction stage buffers
+    int cf = 0, cmx = 0, cmy = 0, cmz = 0;
+    float *t1 = nullptr, *t2 = nullptr;
+    int tile_candidates = 0;   // ranked P x R candidates of a float solve
+    int tile_rank = 0;         // the one planned
 };
 
 // Decomposed smoothing plan (k_smooth_fast.cu).
@@ -132,7 +138,8 @@ struct Fused {
     double *phi64_prev2 = nullptr; // the step before's (quadratic extrapolation)
     void *F4 = nullptr;           // interleaved forces, 4 x T per node
     double *obs_partials = nullptr;  // per-step observable partials
-    int obs_blocks = 0;
+    int obs_blocks = 0;           // blocks of the particle step (one partial row each)
+    int pblock = 256;             // threads per block of the particle step
     int obs_rows = 0;             // capacity in steps
     int *sor_its = nullptr;       // per-step SOR iterations (device)
     double *obs_rows_dev = nullptr;  // reduced rows (device)
@@ -228,6 +235,7 @@ hv_status launch_observe(hv_ctx *c, const T *x, const T *y, const T *z, hv_obser
 hv_status fused_prepare(hv_ctx *c);
 hv_status fused_release(hv_ctx *c);
 hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs);
+hv_status fused_autotune(hv_ctx *c, int trial, hv_autotune_report *rep);
 void fused_invalidate(hv_ctx *c);
 
 // Several float SOR solves run by one cooperative launch (k_sor_fast.cu).
@@ -259,6 +267,8 @@ State<float> &state<float>(hv_ctx *c);
 hv_status download_slots(hv_ctx *c, const void *dev, void *host);
 // re-plans a context's fused SOR with at most max_blocks blocks (0: all SMs)
 hv_status sor_fast_replan(hv_ctx *c, int max_blocks);
+// re-plans it with the tile of the given rank (float solves; see plan_for)
+hv_status sor_fast_replan_rank(hv_ctx *c, int rank, int *count);
 
 // parts of fused float steps for the batched driver (k_fused.cu)
 hv_status fused_batch_ready(hv_ctx *c);

@@ -22,13 +22,16 @@ hv_status sor_fast_plan(hv_ctx *c);
 void sor_fast_release(hv_ctx *c);
 template <typename T>
 hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, bool step_solve);
+hv_status sor_fast_clear_error(hv_ctx *c);
 hv_status smooth_fast_plan(hv_ctx *c);
 void smooth_fast_release(hv_ctx *c);
 hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho);
 
 namespace {
 
-constexpr int kPBlock = 256;
+constexpr int kPBlock = 256;      // default threads per block of the particle step
+constexpr int kPBlockMax = 512;   // largest of the autotuner's candidates
+constexpr int kPGridMax = 8;      // most blocks per SM of the particle step
 constexpr int kRing = 64;  // observable rows kept on the device
 
 // control words (Fused::ctl)
@@ -140,6 +143,98 @@ __device__ __forceinline__ void deposit_at(const Geom &g, T *rho, long long off,
     if (bx && by && bz) atomicAdd(b + sx + sy + 1, dx * dy * dz);
 }
 
+// The z-pair-wise vector atomics of deposit_at for one base node n0 (index in
+// the stacked grid) and eight corner weights w[c], c = dx + 2 dy + 4 dz
+// (corners with an index equal to n already zeroed or skipped by bx/by/bz).
+__device__ __forceinline__ void add_corners(const Geom &g, float *rho, long long n0, bool bx, bool by, bool bz,
+                                            const float (&w)[8]) {
+    const int nz = g.nz;
+    const long long sx = (long long)g.ny * nz, sy = nz;
+    float *b = rho + n0;
+    if (bz && (nz & 1) == 0 && (n0 & 1) == 0) {
+        float2 *b2 = reinterpret_cast<float2 *>(b);
+        const long long sx2 = sx / 2, sy2 = sy / 2;
+        atomicAdd(b2, make_float2(w[0], w[4]));
+        if (bx) atomicAdd(b2 + sx2, make_float2(w[1], w[5]));
+        if (by) atomicAdd(b2 + sy2, make_float2(w[2], w[6]));
+        if (bx && by) atomicAdd(b2 + sx2 + sy2, make_float2(w[3], w[7]));
+        return;
+    }
+    if (bz && (nz & 3) == 0 && (n0 & 3) == 1) {
+        float4 *b4 = reinterpret_cast<float4 *>(b - 1);
+        const long long sx4 = sx / 4, sy4 = sy / 4;
+        atomicAdd(b4, make_float4(0.0f, w[0], w[4], 0.0f));
+        if (bx) atomicAdd(b4 + sx4, make_float4(0.0f, w[1], w[5], 0.0f));
+        if (by) atomicAdd(b4 + sy4, make_float4(0.0f, w[2], w[6], 0.0f));
+        if (bx && by) atomicAdd(b4 + sx4 + sy4, make_float4(0.0f, w[3], w[7], 0.0f));
+        return;
+    }
+    atomicAdd(b, w[0]);
+    if (bx) atomicAdd(b + sx, w[1]);
+    if (by) atomicAdd(b + sy, w[2]);
+    if (bx && by) atomicAdd(b + sx + sy, w[3]);
+    if (bz) atomicAdd(b + 1, w[4]);
+    if (bx && bz) atomicAdd(b + sx + 1, w[5]);
+    if (by && bz) atomicAdd(b + sy + 1, w[6]);
+    if (bx && by && bz) atomicAdd(b + sx + sy + 1, w[7]);
+}
+
+// CIC deposit of one particle per lane of a warp (all 32 lanes call it;
+// valid false for a lane past the last particle), aggregated over runs of
+// consecutive lanes with the same base node: the slots are re-sorted by cell
+// every few steps, so neighbouring lanes mostly share one.  A ballot marks
+// each run's last lane, a segmented suffix sum over shuffles gives the run's
+// first lane the sums of its lanes' eight corner weights, and that lane alone
+// issues the atomics (distribute_volumetric_particles_cic,
+// include/tools.hpp:35-96: the same cells, weights and corner drops; only the
+// order of the float additions differs).
+__device__ __forceinline__ void deposit_warp(const Geom &g, float *rho, long long off, float px, float py, float pz,
+                                             bool valid) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int lane = threadIdx.x & 31;
+    const float cx = (nx / 2.0f) * (px / (float)g.dmx + 1.0f);
+    const float cy = (ny / 2.0f) * (py / (float)g.dmy + 1.0f);
+    const float cz = (nz / 2.0f) * (pz / (float)g.dmz + 1.0f);
+    const bool in = valid && !(cx < 0.0f || cy < 0.0f || cz < 0.0f || cx >= nx || cy >= ny || cz >= nz);
+    int x0 = 0, y0 = 0, z0 = 0;
+    float w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long key = -1;
+    if (in) {
+        x0 = (int)cx;
+        y0 = (int)cy;
+        z0 = (int)cz;
+        const float dx = cx - x0, dy = cy - y0, dz = cz - z0;
+        const float tx = 1.0f - dx, ty = 1.0f - dy, tz = 1.0f - dz;
+        w[0] = tx * ty * tz;
+        w[1] = dx * ty * tz;
+        w[2] = tx * dy * tz;
+        w[3] = dx * dy * tz;
+        w[4] = tx * ty * dz;
+        w[5] = dx * ty * dz;
+        w[6] = tx * dy * dz;
+        w[7] = dx * dy * dz;
+        key = off + ((long long)x0 * ny + y0) * nz + z0;
+    }
+    const long long knext = __shfl_down_sync(0xffffffffu, key, 1);
+    const long long kprev = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool last = lane == 31 || knext != key;
+    const bool first = lane == 0 || kprev != key;
+    const unsigned ends = __ballot_sync(0xffffffffu, last);
+    if (ends != 0xffffffffu) {  // some run is longer than one lane
+        const int run_end = lane + __ffs(ends >> lane) - 1;
+        const unsigned longest = __reduce_max_sync(0xffffffffu, (unsigned)(run_end - lane + 1));
+        for (int d = 1; d < (int)longest; d <<= 1) {
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const float o = __shfl_down_sync(0xffffffffu, w[c], d);
+                if (lane + d <= run_end) w[c] += o;
+            }
+        }
+    }
+    if (!first || key < 0) return;
+    add_corners(g, rho, key, x0 + 1 < nx, y0 + 1 < ny, z0 + 1 < nz, w);
+}
+
 template <typename T>
 struct PArgs {
     Geom g;
@@ -149,53 +244,78 @@ struct PArgs {
     T *rho_raw;
     T h, fd, dp, dn;
     int deposit;  // 1: atomic CIC deposit of x_{n+1} here; 0: the sorted deposit follows
+    int aggregate;  // float atomic deposit aggregated over warp runs of equal base nodes
     const int *ctl;
     double *obs;  // [kRing][blocks][6]
 };
 
-// One step of every particle; observables of x_n into the ring row of step n.
+// One particle of one step: gather f_n, the closing kick/2 of the previous
+// step, observables of x_n, the excitation, the opening kick/2 and the drift;
+// returns x_{n+1} and the particle's species offset in the stacked grids.
 template <typename T>
-__global__ void __launch_bounds__(kPBlock) k_particle_step(PArgs<T> a) {
+__device__ __forceinline__ void particle_update(const PArgs<T> &a, int i, bool close, bool excite, T dmx, T dmy,
+                                                T dmz, double (&v)[6], T &px, T &py, T &pz, long long &off) {
+    const int s = i < a.protons ? 0 : 1;
+    off = s ? a.g.G : 0;
+    px = a.x[i];
+    py = a.y[i];
+    pz = a.z[i];
+    T qx = a.kx[i], qy = a.ky[i], qz = a.kz[i];
+    T fx, fy, fz;
+    gather_at<T>(a.g, a.F4, off, px, py, pz, fx, fy, fz);
+    if (close) {  // closing kick/2 of the previous step (physics.hpp:248-258)
+        qx += a.h * fx;
+        qy += a.h * fy;
+        qz += a.h * fz;
+    }
+    // observables of x_n (tools.hpp:302-338)
+    v[s] += (double)pz;
+    if (!(px < -dmx || px > dmx || py < -dmy || py > dmy || pz < -dmz || pz > dmz)) {
+        v[2 + s] += (double)(px * px + py * py + pz * pz);
+        v[4 + s] += 1.0;
+    }
+    if (excite) qz += s ? -a.dn : a.dp;  // physics.hpp:236-246
+    qx += a.h * fx;                      // opening kick/2
+    qy += a.h * fy;
+    qz += a.h * fz;
+    px += a.fd * qx;  // drift (physics.hpp:260-270)
+    py += a.fd * qy;
+    pz += a.fd * qz;
+    a.x[i] = px;
+    a.y[i] = py;
+    a.z[i] = pz;
+    a.kx[i] = qx;
+    a.ky[i] = qy;
+    a.kz[i] = qz;
+}
+
+// One step of every particle; observables of x_n into the ring row of step n.
+template <typename T, int kB>
+__global__ void __launch_bounds__(kB) k_particle_step(PArgs<T> a) {
     const int step = a.ctl[CTL_STEP];
     const bool close = a.ctl[CTL_CLOSE] != 0;
     const bool excite = a.ctl[CTL_EXCITE] == step;
     const T dmx = T(a.g.dmx), dmy = T(a.g.dmy), dmz = T(a.g.dmz);
     double v[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.total; i += gridDim.x * blockDim.x) {
-        const int s = i < a.protons ? 0 : 1;
-        const long long off = s ? a.g.G : 0;
-        T px = a.x[i], py = a.y[i], pz = a.z[i];
-        T qx = a.kx[i], qy = a.ky[i], qz = a.kz[i];
-        T fx, fy, fz;
-        gather_at<T>(a.g, a.F4, off, px, py, pz, fx, fy, fz);
-        if (close) {  // closing kick/2 of the previous step (physics.hpp:248-258)
-            qx += a.h * fx;
-            qy += a.h * fy;
-            qz += a.h * fz;
+    // warp-uniform trip count (the aggregated deposit needs every lane)
+    const int stride = gridDim.x * blockDim.x;
+    for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < a.total; i0 += stride) {
+        const int i = i0 + (threadIdx.x & 31);
+        const bool valid = i < a.total;
+        T px = T(0), py = T(0), pz = T(0);
+        long long off = 0;
+        if (valid) particle_update<T>(a, i, close, excite, dmx, dmy, dmz, v, px, py, pz, off);
+        if (!a.deposit) continue;
+        if constexpr (sizeof(T) == 4) {
+            if (a.aggregate) {
+                deposit_warp(a.g, reinterpret_cast<float *>(a.rho_raw), off, px, py, pz, valid);
+                continue;
+            }
         }
-        // observables of x_n (tools.hpp:302-338)
-        v[s] += (double)pz;
-        if (!(px < -dmx || px > dmx || py < -dmy || py > dmy || pz < -dmz || pz > dmz)) {
-            v[2 + s] += (double)(px * px + py * py + pz * pz);
-            v[4 + s] += 1.0;
-        }
-        if (excite) qz += s ? -a.dn : a.dp;  // physics.hpp:236-246
-        qx += a.h * fx;                      // opening kick/2
-        qy += a.h * fy;
-        qz += a.h * fz;
-        px += a.fd * qx;  // drift (physics.hpp:260-270)
-        py += a.fd * qy;
-        pz += a.fd * qz;
-        a.x[i] = px;
-        a.y[i] = py;
-        a.z[i] = pz;
-        a.kx[i] = qx;
-        a.ky[i] = qy;
-        a.kz[i] = qz;
-        if (a.deposit) deposit_at<T>(a.g, a.rho_raw, off, px, py, pz);
+        if (valid) deposit_at<T>(a.g, a.rho_raw, off, px, py, pz);
     }
     // deterministic block reduction of the six sums
-    __shared__ double sh[6][kPBlock / 32];
+    __shared__ double sh[6][kB / 32];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     for (int c = 0; c < 6; c++) {
         double u = v[c];
@@ -205,7 +325,7 @@ __global__ void __launch_bounds__(kPBlock) k_particle_step(PArgs<T> a) {
     __syncthreads();
     if (threadIdx.x < 6) {
         double u = 0.0;
-        for (int q = 0; q < kPBlock / 32; q++) u += sh[threadIdx.x][q];
+        for (int q = 0; q < kB / 32; q++) u += sh[threadIdx.x][q];
         a.obs[((long long)(step % kRing) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = u;
     }
 }
@@ -414,11 +534,16 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     a.dp = e * nn / (zz + nn);
     a.dn = e * zz / (zz + nn);
     a.deposit = sorted ? 0 : 1;
+    a.aggregate = c->fast.deposit_aggregate;
     a.ctl = ctl;
     a.obs = f.obs_partials;
     if (c->total > 0) {
         ProfScope ps(c, HV_K_PARTICLE);
-        k_particle_step<T><<<f.obs_blocks, kPBlock, 0, c->stream>>>(a);
+        switch (f.pblock) {
+            case 128: k_particle_step<T, 128><<<f.obs_blocks, 128, 0, c->stream>>>(a); break;
+            case 512: k_particle_step<T, 512><<<f.obs_blocks, 512, 0, c->stream>>>(a); break;
+            default: k_particle_step<T, kPBlock><<<f.obs_blocks, kPBlock, 0, c->stream>>>(a); break;
+        }
     } else {
         HV_CUDA(cudaMemsetAsync(f.obs_partials, 0, sizeof(double) * kRing * f.obs_blocks * 6, c->stream));
     }
@@ -529,6 +654,7 @@ hv_status initial_typed(hv_ctx *c) {
     int h_ctl[3] = {c->step_index, f.m_hint, 0};
     HV_CUDA(cudaMemcpyAsync(ctl, h_ctl, sizeof(int) * 3, cudaMemcpyHostToDevice, c->stream));
     // from phi = 0: neither extrapolated nor recorded as an earlier solution
+    HV_TRY(sor_fast_clear_error(c));
     HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, nullptr, kRing, false));
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
@@ -589,6 +715,7 @@ hv_status run_begin(hv_ctx *c, int n_steps, int *exc_out) {
             }
     }
     int h_ctl[5] = {c->step_index, f.m_hint, 0, exc, 0};
+    HV_TRY(sor_fast_clear_error(c));
     HV_CUDA(cudaMemcpyAsync(ctl + CTL_STEP, &h_ctl[0], sizeof(int), cudaMemcpyHostToDevice, c->stream));
     HV_CUDA(cudaMemcpyAsync(ctl + CTL_EXCITE, &h_ctl[3], sizeof(int) * 2, cudaMemcpyHostToDevice, c->stream));
     HV_CUDA(cudaStreamSynchronize(c->stream));
@@ -730,7 +857,9 @@ hv_status fused_prepare(hv_ctx *c) {
     HV_CUDA(cudaMemsetAsync(f.phi64_prev2, 0, sizeof(double) * g.G, c->stream));
     HV_CUDA(cudaMalloc(&f.F4, es * 4 * 2 * g.G));
     f.obs_blocks = 4 * c->sm_count;
-    HV_CUDA(cudaMalloc((void **)&f.obs_partials, sizeof(double) * kRing * f.obs_blocks * 6));
+    f.pblock = kPBlock;
+    // partial rows for the largest grid the autotuner may choose
+    HV_CUDA(cudaMalloc((void **)&f.obs_partials, sizeof(double) * kRing * kPGridMax * c->sm_count * 6));
     HV_CUDA(cudaMalloc((void **)&f.obs_rows_dev, sizeof(double) * kRing * 8));
     HV_CUDA(cudaMalloc((void **)&f.sor_its, sizeof(int) * (kRing + CTL_N)));
     HV_CUDA(cudaMemsetAsync(f.sor_its, 0, sizeof(int) * (kRing + CTL_N), c->stream));
@@ -778,6 +907,95 @@ hv_status fused_run(hv_ctx *c, int n_steps, hv_observables *obs) {
     return c->prec == HV_F64 ? run_typed<double>(c, n_steps, obs) : run_typed<float>(c, n_steps, obs);
 }
 
+// ---- autotuner of a single run ---------------------------------------------
+namespace {
+
+// Device milliseconds per launch of kernel `kid` over `trial` fused steps
+// (direct launches with CUDA events, after one untimed step that loads the
+// configuration's kernels).
+hv_status time_kernel(hv_ctx *c, int kid, int trial, double *ms) {
+    HV_TRY(fused_run(c, 1, nullptr));
+    HV_TRY(hv_ctx_set_profiling(c, 1));
+    const hv_status st = fused_run(c, trial, nullptr);
+    const double total = c->prof.ms[kid];
+    const int n = c->prof.launches[kid];
+    HV_TRY(hv_ctx_set_profiling(c, 0));
+    HV_TRY(st);
+    *ms = n > 0 ? total / n : 0.0;
+    return HV_OK;
+}
+
+void drop_graph(hv_ctx *c) {
+    if (c->fused.graph) cudaGraphExecDestroy(c->fused.graph);
+    c->fused.graph = nullptr;
+    c->fused.graph_len = 0;
+}
+
+}  // namespace
+
+// Chooses the particle step's block size and grid, then the SOR tile, by
+// timing each candidate's kernel over trial steps (coordinate descent: the
+// particle candidates with the planned tile, then the tiles with the chosen
+// particle configuration).  The trial steps advance the run.
+hv_status fused_autotune(hv_ctx *c, int trial, hv_autotune_report *rep) {
+    HV_TRY(fused_run(c, 0, nullptr));  // initial solve and plans, if not done
+    HV_TRY(fused_prepare(c));
+    Fused &f = c->fused;
+    int count = 0;
+    double best_ms = 0.0, ms = 0.0;
+    const int blocks[3] = {128, 256, 512}, grids[3] = {2, 4, 8};
+    int best_b = f.pblock, best_g = f.obs_blocks;
+    for (int pb : blocks)
+        for (int pg : grids) {
+            f.pblock = pb;
+            f.obs_blocks = pg * c->sm_count;
+            drop_graph(c);
+            HV_TRY(time_kernel(c, HV_K_PARTICLE, trial, &ms));
+            count++;
+            if (count == 1 || ms < best_ms) {
+                best_ms = ms;
+                best_b = pb;
+                best_g = f.obs_blocks;
+            }
+        }
+    f.pblock = best_b;
+    f.obs_blocks = best_g;
+    const double particle_ms = best_ms;
+    // SOR tiles: the plan's first few candidates
+    int ntile = 0, best_rank = 0;
+    double sor_best = 0.0;
+    for (int rank = 0; rank < 4; rank++) {
+        if (rank > 0 && rank >= ntile) break;
+        HV_TRY(sor_fast_replan_rank(c, rank, &ntile));
+        drop_graph(c);
+        if (!f.sor.ok) continue;
+        HV_TRY(time_kernel(c, HV_K_SOR, trial, &ms));
+        count++;
+        if (rank == 0 || ms < sor_best) {
+            sor_best = ms;
+            best_rank = rank;
+        }
+    }
+    HV_TRY(sor_fast_replan_rank(c, best_rank, &ntile));
+    drop_graph(c);
+    if (!f.sor.ok) {
+        set_last_error("autotune: the chosen SOR tile does not fit on chip");
+        return HV_ERR_UNSUPPORTED;
+    }
+    if (rep) {
+        rep->particle_block = f.pblock;
+        rep->particle_grid = f.obs_blocks;
+        rep->sor_planes = f.sor.P;
+        rep->sor_rows = f.sor.R;
+        rep->sor_blocks = f.sor.nblocks;
+        rep->sor_tile_rank = best_rank;
+        rep->candidates = count;
+        rep->particle_ms = particle_ms;
+        rep->sor_ms = sor_best;
+    }
+    return HV_OK;
+}
+
 // ---- batched driver support (batch.cu): float contexts, parts of a step on a
 // caller's stream
 namespace {
@@ -821,6 +1039,9 @@ void fused_batch_sor_inputs(hv_ctx *c, const float **rho, int **ctl, int **its_r
 void fused_invalidate(hv_ctx *c) {
     c->fused.f4_current = false;
     c->fused.prev_valid = false;
+    // the step counter may have been rewound (an adjoint pass restores
+    // checkpoints): the next fused run re-sorts at its first chunk
+    c->fused.last_sort = Fused().last_sort;
 }
 
 }  // namespace hv

@@ -49,8 +49,11 @@ namespace hv {
 namespace {
 
 constexpr int kSorThreads = 1024;
-constexpr long long kMaxSpin = 1ll << 24;  // polls before a wait gives up (~1 s)
-constexpr long long kMaxPoll = 1ll << 22;  // polls of one tagged mirror entry
+// default bounds of the device-side waits (hv_fast_options.sor_wait_limit
+// replaces both): polls of a grid barrier or a neighbour's phase counter before
+// the wait gives up (~1 s), and polls of one tagged mirror entry
+constexpr long long kDefaultSpin = 1ll << 24;
+constexpr long long kDefaultPoll = 1ll << 22;
 #ifndef HV_SOR_POLL_NS
 #define HV_SOR_POLL_NS 64
 #endif
@@ -68,6 +71,7 @@ struct SorArgs {
     double src_scale;       // omega / diag: the residual is stored pre-scaled
     double tol;
     int max_iter, criterion, inner_min, inner_max;
+    long long max_spin, max_poll;  // bounds of the waits (kDefaultSpin, kDefaultPoll)
     int extrapolate;        // initial guess: 0 previous phi, else extrapolation of this order (1, 2)
     const T *rho;
     double *phi64, *phi64_prev, *phi64_prev2;
@@ -81,6 +85,13 @@ struct SorArgs {
     int *ctl;               // [0] step counter, [1] iterations of the previous solve, [2] phi history held
     int *its_ring;          // per-step iterations, indexed by step % ring
     int ring;
+    // coarse-grid correction (staged float form): coarsening factor F, interior
+    // extents of the coarse grid (its nodes sit at every F-th fine node, with
+    // zero corrections at 0 and n / F), red+black iterations per cycle, and
+    // the two restriction stages' buffers t1 [nx][ny][cmz], t2 [nx][cmy][cmz]
+    int coarse, cf, cmx, cmy, cmz, csweeps;
+    float *t1, *t2;
+    double hx, hy, hz;      // fine grid spacings
     // several solves in one launch: block -> instance, first block of an
     // instance, and the instances' arguments (null for a single solve)
     const SorArgs *batch;
@@ -100,7 +111,7 @@ __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volati
 
 // Grid barrier for co-resident blocks; false when a wait timed out or another
 // block reported an error.
-__device__ bool grid_barrier(unsigned *bar, int nblocks, int *err) {
+__device__ bool grid_barrier(unsigned *bar, int nblocks, int *err, long long max_spin) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -114,7 +125,7 @@ __device__ bool grid_barrier(unsigned *bar, int nblocks, int *err) {
         } else {
             long long spin = 0;
             while (ld_relaxed(bar + 1) == gen) {
-                if (++spin > kMaxSpin || ld_volatile(err)) {
+                if (++spin > max_spin || ld_volatile(err)) {
                     atomicExch(err, 1);
                     ok = 0;
                     break;
@@ -144,7 +155,7 @@ __device__ bool wait_neighbours(const SorArgs<T, S> &a, int bx, int by, unsigned
         if (nb >= 0) {
             long long spin = 0;
             while (ld_relaxed(a.phase + nb) < target) {
-                if (++spin > kMaxSpin || ld_volatile(a.status)) {
+                if (++spin > a.max_spin || ld_volatile(a.status)) {
                     atomicExch(a.status, 1);
                     good = 0;
                     break;
@@ -330,11 +341,11 @@ __device__ __forceinline__ void st_tagged4(u64 *p, float4 v, unsigned tag) {
 // polled together: both sources are loaded, then all tags are checked, and
 // only a miss repeats the loads, so a row whose ghosts are already written
 // costs one L2 round trip.  A null source is not read (its value is zero).
-// Bounded: after kMaxPoll polls, or when another block has reported an error,
+// Bounded: after max_poll polls, or when another block has reported an error,
 // it records the error, sets `failed` and returns what it read; a thread that
 // has failed once reads each further source once without waiting.
-__device__ __forceinline__ void poll_pair(const u64 *g0, const u64 *g1, unsigned tag, int *status, bool &failed,
-                                          float4 &v0, float4 &v1) {
+__device__ __forceinline__ void poll_pair(const u64 *g0, const u64 *g1, unsigned tag, int *status,
+                                          long long max_poll, bool &failed, float4 &v0, float4 &v1) {
     u64 w[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
     const u64 *g[2] = {g0, g1};
     long long n = 0;
@@ -358,7 +369,7 @@ __device__ __forceinline__ void poll_pair(const u64 *g0, const u64 *g1, unsigned
                 ok = ok && (unsigned)(w[i][0] >> 32) == tag && (unsigned)(w[i][1] >> 32) == tag &&
                      (unsigned)(w[i][2] >> 32) == tag && (unsigned)(w[i][3] >> 32) == tag;
         if (ok || failed) break;
-        if ((++n & 63) == 0 && (n > kMaxPoll || ld_volatile(status))) {
+        if ((++n & 63) == 0 && (n > max_poll || ld_volatile(status))) {
             failed = true;
             atomicExch(status, 1);
             break;
@@ -409,14 +420,15 @@ __device__ __forceinline__ void sweep_quads_tagged(const SorArgs<T, float> &a, c
         const u64 *gq = a.tmirror + ((2ll * x + cp) * cstride + (long long)y * nz2 + 4 * q);
         float4 m4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), p4 = m4;
         if (tag_in && (gx0 || gx1))
-            poll_pair(gx0 ? gq - 2 * cstride : nullptr, gx1 ? gq + 2 * cstride : nullptr, tag_in, a.status, failed,
-                      m4, p4);
+            poll_pair(gx0 ? gq - 2 * cstride : nullptr, gx1 ? gq + 2 * cstride : nullptr, tag_in, a.status,
+                      a.max_poll, failed, m4, p4);
         if (p > 0) m4 = reinterpret_cast<const float4 *>(orow - 2 * B.hp)[q];
         if (p + 1 < B.np) p4 = reinterpret_cast<const float4 *>(orow + 2 * B.hp)[q];
         const float4 xs = add4(m4, p4);
         m4 = p4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (tag_in && (gy0 || gy1))
-            poll_pair(gy0 ? gq - nz2 : nullptr, gy1 ? gq + nz2 : nullptr, tag_in, a.status, failed, m4, p4);
+            poll_pair(gy0 ? gq - nz2 : nullptr, gy1 ? gq + nz2 : nullptr, tag_in, a.status, a.max_poll, failed, m4,
+                      p4);
         if (j > 0) m4 = reinterpret_cast<const float4 *>(orow - nz2)[q];
         if (j + 1 < B.nr) p4 = reinterpret_cast<const float4 *>(orow + nz2)[q];
         const float4 ys = add4(m4, p4);
@@ -612,7 +624,7 @@ __device__ __forceinline__ void sweep_face(const SorArgs<T, float> &a, const Fac
 // a miss repeats them.  Bounded like poll_pair.
 template <int kG>
 __device__ __forceinline__ void fetch_ghosts(const u64 *tm, const GhostQuad (&g)[kG], long long coff, unsigned tag,
-                                             float *gbuf, int *status, bool &failed) {
+                                             float *gbuf, int *status, long long max_poll, bool &failed) {
     u64 w[kG][4];
 #pragma unroll
     for (int i = 0; i < kG; i++) w[i][0] = w[i][1] = w[i][2] = w[i][3] = 0;
@@ -639,7 +651,7 @@ __device__ __forceinline__ void fetch_ghosts(const u64 *tm, const GhostQuad (&g)
                     ok = ok && (unsigned)(w[i][0] >> 32) == tag && (unsigned)(w[i][1] >> 32) == tag &&
                          (unsigned)(w[i][2] >> 32) == tag && (unsigned)(w[i][3] >> 32) == tag;
             if (ok || failed) break;
-            if ((++n & 63) == 0 && (n > kMaxPoll || ld_volatile(status))) {
+            if ((++n & 63) == 0 && (n > max_poll || ld_volatile(status))) {
                 failed = true;
                 atomicExch(status, 1);
                 break;
@@ -701,6 +713,242 @@ __device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block
     }
 }
 
+// ---- coarse-grid correction --------------------------------------------
+// Each cycle of the staged float solve starts its correction from the
+// solution of the correction equation on a coarse grid, instead of from zero.
+// The red-black sweeps damp the rough part of the error within a few
+// iterations, but its smooth part decays by less than 1 % per iteration on a
+// 128^3 grid; the coarse grid removes that part in one step.  The coarse grid
+// has every F-th fine node per axis (F a power of two, chosen so that its
+// interior has at most 15 nodes per axis); the fine grid's n nodes per axis
+// are treated as n intervals whose last node (n) carries a zero correction
+// like the Dirichlet node n - 1, so every level spans the same box.  Transfers
+// are the standard pair: restriction by full weighting composed over the log2
+// F levels -- per axis the triangle (F - |d|) / F^2, |d| < F -- and trilinear
+// prolongation.  The coarse equation lap_H e = -R r (7-point, spacing F h per
+// axis, zero boundary) is solved exactly by a discrete sine transform per axis
+// (S_jk = sin(pi (j+1)(k+1) / (m+1)), S S = (m+1)/2 I), redundantly in every
+// block's shared memory, so that no block waits for another to solve it.
+// Restriction is separable: stage 1 filters each block's own z rows (its
+// residual source is in shared memory), stage 2 the y direction (all blocks,
+// after a grid barrier), stage 3 the x direction (every block, after another).
+constexpr int kCoarseMax = 15;
+
+struct Coarse {
+    float *ec, *tmp;       // [mx][my][mz]: the coarse field and a transform buffer
+    float *sx, *sy, *sz;   // sine matrices [m][m]
+    float *lam;            // [mx + my + mz] eigenvalues of the 1-D coarse operators
+    float *prof;           // [rows][mz + 2] z-profiles of own and ghost rows
+    __host__ __device__ static size_t bytes(int mx, int my, int mz, int rows) {
+        const size_t M = (size_t)mx * my * mz;
+        return 4 * (2 * M + (size_t)mx * mx + (size_t)my * my + (size_t)mz * mz + mx + my + mz +
+                    (size_t)rows * (mz + 2)) + 64;
+    }
+    __device__ Coarse(void *base, int mx, int my, int mz) {
+        const size_t M = (size_t)mx * my * mz;
+        float *p = reinterpret_cast<float *>(base);
+        ec = p;
+        tmp = ec + M;
+        sx = tmp + M;
+        sy = sx + mx * mx;
+        sz = sy + my * my;
+        lam = sz + mz * mz;
+        prof = lam + mx + my + mz;
+    }
+};
+
+// Sine matrices and the eigenvalues (2 cos(pi (j+1) / (m+1)) - 2) / H^2 of
+// the 1-D coarse operators, H = F h per axis.
+template <typename T, typename S>
+__device__ void coarse_tables(const SorArgs<T, S> &a, const Coarse &cs) {
+    const int ms[3] = {a.cmx, a.cmy, a.cmz};
+    float *mats[3] = {cs.sx, cs.sy, cs.sz};
+    const double hs[3] = {a.hx, a.hy, a.hz};
+    int loff = 0;
+    for (int ax = 0; ax < 3; ax++) {
+        const int m = ms[ax];
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+            const int j = e / m, k = e - j * m;
+            mats[ax][e] = (float)sinpi((double)((j + 1) * (k + 1)) / (double)(m + 1));
+        }
+        const double H = a.cf * hs[ax];
+        for (int j = threadIdx.x; j < m; j += blockDim.x)
+            cs.lam[loff + j] = (float)((2.0 * cospi((double)(j + 1) / (double)(m + 1)) - 2.0) / (H * H));
+        loff += m;
+    }
+}
+
+// Stage 1: the triangle filter along z of the block's own rows of the
+// pre-scaled residual (shared memory), at the coarse z nodes, into t1.
+template <typename T, typename S>
+__device__ void coarse_stage1(const SorArgs<T, S> &a, const Block &B, const S *ss) {
+    const int F = a.cf, mz = a.cmz, nz2 = a.nz2, nz = a.nz, ny = a.ny;
+    const float w0 = 1.0f / (float)(F * F);
+    for (int o = threadIdx.x; o < B.np * B.nr * mz; o += blockDim.x) {
+        const int K = o % mz, l = o / mz, p = l / B.nr, j = l - p * B.nr;
+        const int x = B.x0 + p, y = B.y0 + j;
+        float acc = 0.0f;
+        if (y >= 1 && y <= ny - 2) {
+            const int kc = F * (K + 1);
+            for (int d = 1 - F; d < F; d++) {
+                const int k = kc + d;
+                if (k < 1 || k > nz - 2) continue;
+                const int c0 = (x + y + k) & 1;
+                acc = fmaf((float)(F - abs(d)), (float)ss[((p * 2 + c0) * B.nr + j) * nz2 + (k >> 1)], acc);
+            }
+        }
+        __stcg(a.t1 + ((long long)x * ny + y) * mz + K, acc * w0);
+    }
+}
+
+// Stage 2 (every block's share of the outputs): the filter along y, into t2.
+template <typename T, typename S>
+__device__ void coarse_stage2(const SorArgs<T, S> &a, int b) {
+    const int F = a.cf, my = a.cmy, mz = a.cmz, ny = a.ny;
+    const float w0 = 1.0f / (float)(F * F);
+    const long long total = (long long)(a.nx - 2) * my * mz;
+    const long long stride = (long long)a.nblocks * blockDim.x;
+    for (long long o = (long long)b * blockDim.x + threadIdx.x; o < total; o += stride) {
+        const int K = (int)(o % mz), J = (int)((o / mz) % my), x = 1 + (int)(o / ((long long)my * mz));
+        const int yc = F * (J + 1);
+        float acc = 0.0f;
+        for (int d = 1 - F; d < F; d++) {
+            const int y = yc + d;
+            if (y < 1 || y > ny - 2) continue;
+            acc = fmaf((float)(F - abs(d)), __ldcg(a.t1 + ((long long)x * ny + y) * mz + K), acc);
+        }
+        __stcg(a.t2 + ((long long)x * my + J) * mz + K, acc * w0);
+    }
+}
+
+// out = S applied along one axis of in ([mx][my][mz], z fastest): thread
+// (k, g) keeps row k of S in registers and produces element k of lines g,
+// g + G, ...
+__device__ __forceinline__ void dst_pass(const float *in, float *out, const float *Sm, int m, int axis, int mx, int my,
+                                         int mz) {
+    const int G = blockDim.x / m, t = threadIdx.x;
+    if (t >= G * m) return;
+    const int k = t % m, g = t / m;
+    float srow[kCoarseMax];
+#pragma unroll
+    for (int j = 0; j < kCoarseMax; j++) srow[j] = j < m ? Sm[k * m + j] : 0.0f;
+    const int L = mx * my * mz / m;
+    const int stride = axis == 2 ? 1 : axis == 1 ? mz : my * mz;
+    for (int line = g; line < L; line += G) {
+        int base;
+        if (axis == 2) base = line * mz;
+        else if (axis == 1) base = (line / mz) * my * mz + line % mz;
+        else base = line;
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < kCoarseMax; j++)
+            if (j < m) acc = fmaf(srow[j], in[base + j * stride], acc);
+        out[base + k * stride] = acc;
+    }
+}
+
+// Stage 3 and the coarse solve: the filter along x of t2 (every block reads
+// all of it), scaled back from the pre-scaled residual to r, then
+// e = S_x S_y S_z (-(S_x S_y S_z R r) / (lam_x + lam_y + lam_z)) 8 / ((mx+1)(my+1)(mz+1)).
+template <typename T, typename S>
+__device__ void coarse_solve(const SorArgs<T, S> &a, const Coarse &cs) {
+    const int F = a.cf, mx = a.cmx, my = a.cmy, mz = a.cmz, M = mx * my * mz;
+    const float w0 = (float)(1.0 / ((double)F * F * a.src_scale));
+    for (int o = threadIdx.x; o < M; o += blockDim.x) {
+        const int K = o % mz, J = (o / mz) % my, I = o / (my * mz);
+        const int xc = F * (I + 1);
+        float acc = 0.0f;
+        for (int d = 1 - F; d < F; d++) {
+            const int x = xc + d;
+            if (x < 1 || x > a.nx - 2) continue;
+            acc = fmaf((float)(F - abs(d)), __ldcg(a.t2 + ((long long)x * my + J) * mz + K), acc);
+        }
+        cs.ec[o] = acc * w0;
+    }
+    __syncthreads();
+    dst_pass(cs.ec, cs.tmp, cs.sz, mz, 2, mx, my, mz);
+    __syncthreads();
+    dst_pass(cs.tmp, cs.ec, cs.sy, my, 1, mx, my, mz);
+    __syncthreads();
+    dst_pass(cs.ec, cs.tmp, cs.sx, mx, 0, mx, my, mz);
+    __syncthreads();
+    const float norm = 8.0f / (float)((mx + 1) * (my + 1) * (mz + 1));
+    for (int o = threadIdx.x; o < M; o += blockDim.x) {
+        const int K = o % mz, J = (o / mz) % my, I = o / (my * mz);
+        cs.tmp[o] *= -norm / (cs.lam[I] + cs.lam[mx + J] + cs.lam[mx + my + K]);
+    }
+    __syncthreads();
+    dst_pass(cs.tmp, cs.ec, cs.sz, mz, 2, mx, my, mz);
+    __syncthreads();
+    dst_pass(cs.ec, cs.tmp, cs.sy, my, 1, mx, my, mz);
+    __syncthreads();
+    dst_pass(cs.tmp, cs.ec, cs.sx, mx, 0, mx, my, mz);
+    __syncthreads();
+}
+
+// The coarse field at coarse node (I, J, K) of the full grid, zero on its faces.
+__device__ __forceinline__ float coarse_at(const Coarse &cs, int mx, int my, int mz, int I, int J, int K) {
+    if (I < 1 || J < 1 || K < 1 || I > mx || J > my || K > mz) return 0.0f;
+    return cs.ec[((I - 1) * my + (J - 1)) * mz + (K - 1)];
+}
+
+// Trilinear prolongation of the coarse field into the block's own
+// correction (both colours, every node; zero on the Dirichlet rows and
+// z ends) and into the ghost buffer (the other blocks' black values across
+// the block's faces, read by the cycle's first red sweep).  Separable: the
+// (x, y) interpolation of each row's coarse z profile first, then z.
+template <typename T>
+__device__ void coarse_prolong(const SorArgs<T, float> &a, const Block &B, const Coarse &cs, float *sd, float *gbuf,
+                               const unsigned *gsrc, int ng) {
+    const int F = a.cf, mx = a.cmx, my = a.cmy, mz = a.cmz, ny = a.ny, nz = a.nz, nz2 = a.nz2;
+    const int own_rows = B.np * B.nr, rows = own_rows + ng, pw = mz + 2;
+    const float inv = 1.0f / (float)F;
+    for (int o = threadIdx.x; o < rows * pw; o += blockDim.x) {
+        const int r = o / pw, Kp = o - r * pw;
+        int x, y;
+        if (r < own_rows) {
+            x = B.x0 + r / B.nr;
+            y = B.y0 + r % B.nr;
+        } else {
+            const unsigned g = gsrc[r - own_rows];
+            y = (int)((g / (unsigned)nz2) % (unsigned)ny);
+            x = (int)(g / (unsigned)(2 * ny * nz2));
+        }
+        float v = 0.0f;
+        if (y >= 1 && y <= ny - 2) {
+            const int I = x / F, J = y / F;
+            const float tx = (float)(x - I * F) * inv, ty = (float)(y - J * F) * inv;
+            v = (1.0f - tx) * ((1.0f - ty) * coarse_at(cs, mx, my, mz, I, J, Kp) +
+                               ty * coarse_at(cs, mx, my, mz, I, J + 1, Kp)) +
+                tx * ((1.0f - ty) * coarse_at(cs, mx, my, mz, I + 1, J, Kp) +
+                      ty * coarse_at(cs, mx, my, mz, I + 1, J + 1, Kp));
+        }
+        cs.prof[o] = v;
+    }
+    __syncthreads();
+    auto zval = [&](int r, int k) -> float {
+        if (k < 1 || k > nz - 2) return 0.0f;
+        const int K = k / F;
+        const float t = (float)(k - K * F) * inv;
+        const float *pr = cs.prof + r * pw;
+        return (1.0f - t) * pr[K] + t * pr[K + 1];
+    };
+    for (int o = threadIdx.x; o < own_rows * 2 * nz2; o += blockDim.x) {
+        const int kh = o % nz2, rc = o / nz2, c = rc & 1, r = rc >> 1;
+        const int p = r / B.nr, j = r - p * B.nr, x = B.x0 + p, y = B.y0 + j;
+        const int k = ((c - x - y) & 1) + 2 * kh;
+        sd[((p * 2 + c) * B.nr + j) * nz2 + kh] = zval(r, k);
+    }
+    for (int o = threadIdx.x; o < ng * nz2; o += blockDim.x) {
+        const int kh = o % nz2, g = o / nz2;
+        const unsigned gs = gsrc[g];
+        const int y = (int)((gs / (unsigned)nz2) % (unsigned)ny), x = (int)(gs / (unsigned)(2 * ny * nz2));
+        const int k = ((1 - x - y) & 1) + 2 * kh;
+        gbuf[g * nz2 + kh] = zval(own_rows + g, k);
+    }
+    __syncthreads();
+}
+
 // kTag: tagged exchange (float corrections in quads).  kInner, kFace,
 // kGhost > 0: staged sweep with at most that many inner quads per compute
 // thread, perimeter quads per thread and ghost quads per fetch thread, decoded
@@ -729,6 +977,9 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     // tagged sweeps: row tables and the ghost buffer
     const Staged st(sd + (size_t)a.P * 2 * a.R * nz2 * (a.src_smem ? 2 : 1), a.P, a.R);
     unsigned *order = st.order;
+    // coarse-grid correction: its arrays follow the ghost buffer
+    const Coarse cs(st.gbuf + (size_t)2 * (a.P + a.R) * nz2, a.cmx, a.cmy, a.cmz);
+    int ng_rows = 0;  // ghost rows listed in st.gsrc (staged sweeps)
     auto SD = [&](int p, int c, int j, int t) -> S & { return sd[((p * 2 + c) * nr + j) * nz2 + t]; };
     unsigned my_phase = 0;
     // colour sweeps: thread -> half-line position t_own, rows r_start, +rows_step
@@ -825,6 +1076,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
             }
         }
         __syncthreads();
+        ng_rows = s_ng;
         const int nq = nz2 / 4, nfq = s_nf * nq, ngq = s_ng * nq;
         const int ip = max(np - 2, 0), ir = max(nr - 2, 0), niq = ip * ir * nq;
         const int nct = nth - kGhostThreads;
@@ -874,6 +1126,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         }
         // the first sweep reads zero ghosts
         for (int e = tid; e < 2 * (a.P + a.R) * nz2; e += nth) st.gbuf[e] = 0.0f;
+        if (a.coarse) coarse_tables(a, cs);
     }
 
     // ---- entry: zero delta (shared and own global mirror) -----------------
@@ -937,7 +1190,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
             if (tid == 0) a.partials[4 * b + 2] = (double)bm;
         }
         // delta of every block is final in global memory after this barrier
-        if (!grid_barrier(a.bar, a.nblocks, err)) return;
+        if (!grid_barrier(a.bar, a.nblocks, err, a.max_spin)) return;
 
         // ---- FP64 residual of phi + delta on own interior nodes ----------
         // The first check of a solve evaluates b + L phi from phi's stencil
@@ -1054,7 +1307,13 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
             block_sum2(rr, none);
             if (tid == 0) a.partials[4 * b + 0] = rr;
         }
-        if (!grid_barrier(a.bar, a.nblocks, err)) return;
+        if constexpr (kStaged) {
+            if (a.coarse) {
+                __syncthreads();  // every own row's residual source is in shared memory
+                coarse_stage1(a, B, ss);
+            }
+        }
+        if (!grid_barrier(a.bar, a.nblocks, err, a.max_spin)) return;
 
         // ---- every block sums the partials in the same fixed order ------
         if (tid < 32) {
@@ -1080,8 +1339,10 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         maxd = s_tot[2];
         cycles++;
 
-        // ---- the next cycle starts from delta = 0 -------------------------
-        for (int e = tid; e < own; e += nth) sd[e] = S(0);
+        // ---- the next cycle starts from delta = 0 (or the coarse grid's
+        // correction, which overwrites every own node) -----------------------
+        if (!a.coarse)
+            for (int e = tid; e < own; e += nth) sd[e] = S(0);
         if constexpr (!kTag)
             for (int p = 0; p < np; p++)
                 for (int c = 0; c < 2; c++)
@@ -1094,7 +1355,10 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         // ---- next inner cycle length: predicted from the observed rate ---
         if (tid == 0) {
             int mm = m;
-            if (a.criterion == HV_SOR_REL_RESIDUAL && rel_prev > 0.0 && rel < rel_prev && m_prev > 0) {
+            if (a.coarse) {
+                // a fixed number of iterations after each coarse correction
+                mm = a.csweeps;
+            } else if (a.criterion == HV_SOR_REL_RESIDUAL && rel_prev > 0.0 && rel < rel_prev && m_prev > 0) {
                 double q = pow(rel / rel_prev, 1.0 / m_prev);
                 double pred = log(a.tol / rel) / log(q);
                 mm = pred < 1e6 ? (int)ceil(pred) : a.inner_max;
@@ -1109,6 +1373,16 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
         last_max = S(0);
 
         // ---- m red+black iterations on delta, tagged exchange -------------
+        if constexpr (kStaged) {
+            if (a.coarse) {
+                // restriction stages 2 and 3, the coarse solve and its
+                // prolongation, which the sweeps below start from
+                coarse_stage2(a, b);
+                if (!grid_barrier(a.bar, a.nblocks, err, a.max_spin)) return;
+                coarse_solve(a, cs);
+                coarse_prolong<T>(a, B, cs, sd, st.gbuf, st.gsrc, ng_rows);
+            }
+        }
         if constexpr (kTag) {
             bool failed = false;
             for (int it = 0; it < m; it++) {
@@ -1131,7 +1405,8 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
                         __syncthreads();
                         if (tid < kGhostThreads) {
                             const unsigned tag_next = (c == 1 && it == m - 1) ? 0u : tag_out;
-                            fetch_ghosts<kGhost>(a.tmirror, ghost, c * cstride, tag_next, st.gbuf, a.status, failed);
+                            fetch_ghosts<kGhost>(a.tmirror, ghost, c * cstride, tag_next, st.gbuf, a.status, a.max_poll,
+                                                failed);
                         } else {
 #pragma unroll
                             for (int k = 0; k < kInner; k++) sweep_inner<T>(a, inner[k], c, hp, sd, ss, track, last_max);
@@ -1197,7 +1472,7 @@ __global__ void __launch_bounds__(kSorThreads, 1) k_sor_fast(SorArgs<T, S> p) {
 }  // namespace
 
 template <typename S>
-static hv_status plan_for(hv_ctx *c, int max_blocks) {
+static hv_status plan_for(hv_ctx *c, int max_blocks, int rank = 0) {
     SorFast &f = c->fused.sor;
     const Geom &g = c->geom;
     cudaDeviceProp prop;
@@ -1209,38 +1484,64 @@ static hv_status plan_for(hv_ctx *c, int max_blocks) {
     const int nz2 = (g.nz + 1) / 2;
     const int interior = g.nx - 2;
     f.ok = false;
+    // coarse-grid correction of the float solve: the smallest power-of-two
+    // factor F that divides every axis and leaves at most kCoarseMax interior
+    // coarse nodes per axis (at least one)
+    int cf = 0, cm[3] = {0, 0, 0};
+    if (sizeof(S) == 4) {
+        const int n3[3] = {g.nx, g.ny, g.nz};
+        for (int F = 2; F <= 256 && !cf; F *= 2) {
+            bool ok = true;
+            for (int ax = 0; ax < 3; ax++) {
+                const int m = n3[ax] / F - 1;
+                ok = ok && n3[ax] % F == 0 && m >= 1 && m <= kCoarseMax;
+                cm[ax] = m;
+            }
+            if (ok) cf = F;
+            else if (n3[0] / F - 1 < 1 || n3[1] / F - 1 < 1 || n3[2] / F - 1 < 1) break;
+        }
+    }
     if (sizeof(S) == 4 && nz2 % 4 == 0) {
         // float corrections in quads: blocks of P planes x R rows with the
-        // source in shared memory, chosen for the fewest quads per thread, then
+        // source in shared memory, ranked by the fewest quads per thread, then
         // the smallest total face (blocks x (P + R): the rows exchanged per
-        // sweep), then the fewest blocks
+        // sweep), then the fewest blocks; the plan takes candidate `rank` of
+        // that order (0, the first, unless the autotuner chose another)
         const long long nq = nz2 / 4;
-        long long best[3] = {0, 0, 0};
+        struct Cand {
+            long long key[3];
+            int P, R, bxn, byn;
+            size_t smem;
+        };
+        std::vector<Cand> cands;
         for (int P = 1; P <= interior; P++)
             for (int R = 1; R <= g.ny; R++) {
                 const size_t own = (size_t)P * 2 * R * nz2;
-                const size_t smem = sizeof(S) * own * 2 + Staged::bytes(P, R, nz2);
+                const size_t smem = sizeof(S) * own * 2 + Staged::bytes(P, R, nz2) +
+                                    (cf ? Coarse::bytes(cm[0], cm[1], cm[2], P * R + 2 * (P + R)) : 0);
                 if (smem > limit) break;
                 const long long bxn = (interior + P - 1) / P, byn = (g.ny + R - 1) / R;
                 if (bxn * byn > cap) continue;
-                const long long key[3] = {((long long)P * R * nq + kSorThreads - 1) / kSorThreads,
-                                          bxn * byn * (P + R), bxn * byn};
-                if (f.ok && !(key[0] < best[0] || (key[0] == best[0] && (key[1] < best[1] ||
-                                                   (key[1] == best[1] && key[2] < best[2])))))
-                    continue;
-                best[0] = key[0];
-                best[1] = key[1];
-                best[2] = key[2];
-                f.P = P;
-                f.R = R;
-                f.bx = (int)bxn;
-                f.by = (int)byn;
-                f.nblocks = (int)(bxn * byn);
-                f.smem = smem;
-                f.src_smem = true;
-                f.tables = true;
-                f.ok = true;
+                cands.push_back(Cand{{((long long)P * R * nq + kSorThreads - 1) / kSorThreads, bxn * byn * (P + R),
+                                      bxn * byn},
+                                     P, R, (int)bxn, (int)byn, smem});
             }
+        std::stable_sort(cands.begin(), cands.end(), [](const Cand &u, const Cand &v) {
+            return std::lexicographical_compare(u.key, u.key + 3, v.key, v.key + 3);
+        });
+        f.tile_candidates = (int)cands.size();
+        if (!cands.empty()) {
+            const Cand &b = cands[rank < (int)cands.size() ? rank : 0];
+            f.P = b.P;
+            f.R = b.R;
+            f.bx = b.bxn;
+            f.by = b.byn;
+            f.nblocks = b.bxn * b.byn;
+            f.smem = b.smem;
+            f.src_smem = true;
+            f.tables = true;
+            f.ok = true;
+        }
     }
     // otherwise smallest blocks first (most parallel), the source in shared
     // memory when it fits, a y split only when a plane does not fit
@@ -1300,6 +1601,23 @@ static hv_status plan_for(hv_ctx *c, int max_blocks) {
     HV_CUDA(cudaMalloc((void **)&f.status, sizeof(int) * 8));
     HV_CUDA(cudaMalloc((void **)&f.metric, sizeof(double) * 2));
     HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 8, c->stream));
+    if (cf && f.tables) {
+        f.cf = cf;
+        f.cmx = cm[0];
+        f.cmy = cm[1];
+        f.cmz = cm[2];
+        const size_t n1 = (size_t)g.nx * g.ny * cm[2], n2 = (size_t)g.nx * cm[1] * cm[2];
+        HV_CUDA(cudaMalloc((void **)&f.t1, sizeof(float) * n1));
+        HV_CUDA(cudaMalloc((void **)&f.t2, sizeof(float) * n2));
+        HV_CUDA(cudaMemsetAsync(f.t1, 0, sizeof(float) * n1, c->stream));
+        HV_CUDA(cudaMemsetAsync(f.t2, 0, sizeof(float) * n2, c->stream));
+    }
+    return HV_OK;
+}
+
+// Clears the error word of the fused solver before a run's solves.
+hv_status sor_fast_clear_error(hv_ctx *c) {
+    HV_CUDA(cudaMemsetAsync(c->fused.sor.status, 0, sizeof(int), c->stream));
     return HV_OK;
 }
 
@@ -1310,7 +1628,7 @@ hv_status sor_fast_plan(hv_ctx *c) {
 
 void sor_fast_release(hv_ctx *c) {
     SorFast &f = c->fused.sor;
-    void *ptrs[] = {f.delta, f.src, f.resid, f.partials, f.phase, f.status, f.metric};
+    void *ptrs[] = {f.delta, f.src, f.resid, f.partials, f.phase, f.status, f.metric, f.t1, f.t2};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     f = SorFast();
@@ -1319,6 +1637,16 @@ void sor_fast_release(hv_ctx *c) {
 hv_status sor_fast_replan(hv_ctx *c, int max_blocks) {
     sor_fast_release(c);
     return c->prec == HV_F64 ? plan_for<double>(c, max_blocks) : plan_for<float>(c, max_blocks);
+}
+
+// Re-plans with the tile of the given rank among the ranked candidates of a
+// float solve (see plan_for); *count receives the number of candidates.
+hv_status sor_fast_replan_rank(hv_ctx *c, int rank, int *count) {
+    sor_fast_release(c);
+    const hv_status st = c->prec == HV_F64 ? plan_for<double>(c, 0, rank) : plan_for<float>(c, 0, rank);
+    if (count) *count = c->fused.sor.tile_candidates;
+    c->fused.sor.tile_rank = rank < c->fused.sor.tile_candidates ? rank : 0;
+    return st;
 }
 
 // The arguments of one solve and its kernel form: 0 phase counters, 1 the
@@ -1362,6 +1690,8 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.criterion = sp.criterion;
     a.inner_min = c->fast.sor_inner_min;
     a.inner_max = c->fast.sor_inner_max;
+    a.max_spin = c->fast.sor_wait_limit > 0 ? c->fast.sor_wait_limit : kDefaultSpin;
+    a.max_poll = c->fast.sor_wait_limit > 0 ? c->fast.sor_wait_limit : kDefaultPoll;
     a.extrapolate = c->fast.sor_warm_start == HV_WARM_EXTRAPOLATE ? 1
                     : c->fast.sor_warm_start == HV_WARM_QUADRATIC ? 2 : 0;
     a.rho = rho;
@@ -1393,6 +1723,18 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
         if (ni <= 1 && nf <= 1 && ng <= 2) form = 2;
         else if (ni <= 2 && nf <= 1 && ng <= 3) form = 3;
     }
+    // the coarse-grid correction: staged float sweeps, relative-residual rule
+    a.coarse = (f.cf > 0 && form >= 2 && c->fast.sor_coarse && sp.criterion == HV_SOR_REL_RESIDUAL) ? 1 : 0;
+    a.cf = f.cf;
+    a.cmx = f.cmx;
+    a.cmy = f.cmy;
+    a.cmz = f.cmz;
+    a.csweeps = c->fast.sor_coarse_sweeps;
+    a.t1 = f.t1;
+    a.t2 = f.t2;
+    a.hx = dx;
+    a.hy = dy;
+    a.hz = dz;
     return form;
 }
 
@@ -1417,7 +1759,10 @@ template <typename T>
 hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, bool step_solve) {
     SorFast &f = c->fused.sor;
     HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
-    HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, c->stream));
+    // words 1..3 describe this solve; the error word (0) stays set from an
+    // earlier solve of the run, so that a later solve cannot hide it (and
+    // gives up at its first wait)
+    HV_CUDA(cudaMemsetAsync(f.status + 1, 0, sizeof(int) * 3, c->stream));
     SorArgs<T, T> a;
     const int form = sor_fast_args<T>(c, rho, ctl, its_ring, ring, a);
     if (!step_solve) a.extrapolate = 0;
@@ -1444,6 +1789,7 @@ hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std:
         if (c->prec != HV_F32 || !c->fused.sor.ok) return HV_ERR_UNSUPPORTED;
         const int fi = sor_fast_args<float>(c, rho[i], ctl[i], its_ring[i], ring, args[i]);
         if (fi == 0) return HV_ERR_UNSUPPORTED;  // the batched form needs the tagged exchange
+        args[i].coarse = 0;  // the waves run the plain sweeps
         any1 = any1 || fi == 1;
         all2 = all2 && fi == 2;
         bfirst[i] = (int)binst.size();
@@ -1479,7 +1825,7 @@ hv_status sor_wave_launch(const SorWave &w, cudaStream_t st) {
     for (hv_ctx *c : w.ctx) {
         const SorFast &f = c->fused.sor;
         HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), st));
-        HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, st));
+        HV_CUDA(cudaMemsetAsync(f.status + 1, 0, sizeof(int) * 3, st));
     }
     SorArgs<float, float> p;
     std::memset(&p, 0, sizeof(p));

@@ -15,7 +15,6 @@
 // nothing has to be cleared.  Calls whose work overlaps on the GPU (on
 // different streams, or from different host threads) race on the array.
 #include <cmath>
-#include <mutex>
 
 #include "hv_internal.h"
 
@@ -26,7 +25,6 @@ constexpr int kThreads = 256;
 constexpr int kPerBlock = 1024;    // particles per block
 constexpr int kMaxBlocks = 4096;   // rows of partial sums
 constexpr int kWidth = 8;          // doubles per row (6 used)
-constexpr int kMaxDevices = 64;
 
 // Scratch of hv_observe_noalloc: rows 0..kMaxBlocks-1 hold per-block partial
 // sums, row kMaxBlocks the final sums.
@@ -82,22 +80,16 @@ __global__ void k_observe_final(int nblocks, double *scratch) {
     scratch[kMaxBlocks * kWidth + c] = u;
 }
 
-std::mutex g_mutex;
-double *g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on `device` (which must be current).
-// The name g_noalloc_scratch in host code is only a host-side stand-in, so
-// the address is looked up once per device and cached.
-hv_status scratch_for(int device, double **out) {
-    if (device < 0 || device >= kMaxDevices) return HV_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return cuda_status(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
-        g_scratch_ptr[device] = static_cast<double *>(p);
-    }
-    *out = g_scratch_ptr[device];
+// Device address of the scratch array on the current device.  The name
+// g_noalloc_scratch in host code is only a host-side stand-in, so every call
+// asks the runtime for the address on the device that is current (the lookup
+// allocates nothing).  Not caching it keeps the address right after the
+// device's context has been reset and created again.
+hv_status scratch_address(double **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_status(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress");
+    *out = static_cast<double *>(p);
     return HV_OK;
 }
 
@@ -134,10 +126,8 @@ extern "C" hv_status hv_observe_noalloc(const hv_world *world, int protons, int 
         return HV_ERR_BAD_ARG;
     }
     if (total > 0 && (!x || !y || !z)) return HV_ERR_BAD_ARG;
-    int device = 0;
-    HV_CUDA(cudaGetDevice(&device));
     double *scratch = nullptr;
-    HV_TRY(scratch_for(device, &scratch));
+    HV_TRY(scratch_address(&scratch));
     const int nblocks = total > 0 ? (int)((total + kPerBlock - 1) / kPerBlock) : 0;
     double v[6] = {0, 0, 0, 0, 0, 0};
     const Geom g = make_geom(*world);

@@ -9,7 +9,7 @@ from ._lib import (HV_DEPOSIT_ATOMIC, HV_DEPOSIT_SORTED, HV_F32, HV_F64, HV_FIEL
                    HV_FIELD_POTENTIAL, HV_PATH_FUSED, HV_PATH_PLAIN, HV_RNG_LIBC, HV_RNG_PHILOX, HV_SOR_EXCHANGE_AUTO, HV_SOR_EXCHANGE_FLAGS,
                    HV_SOR_MAX_UPDATE, HV_SOR_REL_RESIDUAL, HV_WARM_EXTRAPOLATE, HV_WARM_PREVIOUS, HV_WARM_QUADRATIC, OBS_DTYPE,
                    HVError, load)
-from .api import Session, generate_nucleus, simulate, workload_particles
+from .api import Session, generate_nucleus, simulate, simulate_release, workload_particles
 from .workloads import CA40_SMALL, PB208_2M, PB208_20K_128, PB208_104K, WORKLOADS, Workload
 
 __all__ = [
@@ -17,6 +17,6 @@ __all__ = [
     "HV_FIELD_DENSITY_RAW",
     "HV_FIELD_POTENTIAL", "HV_PATH_FUSED", "HV_PATH_PLAIN", "HV_RNG_LIBC", "HV_RNG_PHILOX", "HV_SOR_EXCHANGE_AUTO", "HV_SOR_EXCHANGE_FLAGS",
     "HV_SOR_MAX_UPDATE", "HV_SOR_REL_RESIDUAL", "HV_WARM_EXTRAPOLATE", "HV_WARM_PREVIOUS", "HV_WARM_QUADRATIC", "OBS_DTYPE", "HVError", "load", "Session",
-    "generate_nucleus", "simulate", "workload_particles", "CA40_SMALL", "PB208_2M", "PB208_20K_128", "PB208_104K",
+    "generate_nucleus", "simulate", "simulate_release", "workload_particles", "CA40_SMALL", "PB208_2M", "PB208_20K_128", "PB208_104K",
     "WORKLOADS", "Workload", "_lib",
 ]

@@ -66,7 +66,8 @@ class hv_run_params(C.Structure):
 class hv_fast_options(C.Structure):
     _fields_ = [("sor_warm_start", C.c_int), ("sor_inner_min", C.c_int), ("sor_inner_max", C.c_int),
                 ("sort_every", C.c_int), ("graph_steps", C.c_int), ("sor_exchange", C.c_int),
-                ("smooth_fft", C.c_int), ("sor_omega", C.c_double)]
+                ("smooth_fft", C.c_int), ("sor_omega", C.c_double), ("sor_wait_limit", C.c_int),
+                ("sor_coarse", C.c_int), ("sor_coarse_sweeps", C.c_int), ("deposit_aggregate", C.c_int)]
 
 
 HV_WARM_PREVIOUS = 0
@@ -82,6 +83,12 @@ class hv_observables(C.Structure):
         ("zcm_p", C.c_double), ("zcm_n", C.c_double), ("dipole", C.c_double),
         ("sor_iterations", C.c_int), ("flags", C.c_int),
     ]
+
+
+class hv_autotune_report(C.Structure):
+    _fields_ = [("particle_block", C.c_int), ("particle_grid", C.c_int), ("sor_planes", C.c_int),
+                ("sor_rows", C.c_int), ("sor_blocks", C.c_int), ("sor_tile_rank", C.c_int),
+                ("candidates", C.c_int), ("particle_ms", C.c_double), ("sor_ms", C.c_double)]
 
 
 class hv_woods_saxon(C.Structure):
@@ -164,11 +171,13 @@ SIGNATURES = {
     "hv_ctx_set_fast_options": (_S, [_P, _P]),
     "hv_ctx_get_fast_options": (_S, [_P, _P]),
     "hv_ctx_set_profiling": (_S, [_P, _I]),
+    "hv_ctx_autotune": (_S, [_P, _I, _P]),
     "hv_ctx_kernel_times": (_S, [_P, _P, _P, _I]),
     "hv_write_vtk": (_S, [_P, C.c_char_p]),
     "hv_initial_solve": (_S, [_P, _P]),
     "hv_run": (_S, [_P, _I, _I, _P]),
     "hv_simulate": (_S, [_P, _I, _I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    "hv_simulate_release": (_S, []),
     "hv_adjoint_forward": (_S, [_P, _I, _I, _P]),
     "hv_adjoint_backward": (_S, [_P, _P, _P, _P, _P]),
     "hv_particle_densities": (_S, [_P, _P, _P]),

@@ -122,13 +122,22 @@ class Session:
 
     def set_fast_options(self, **kw):
         """Updates fields of hv_fast_options (sor_warm_start, sor_inner_min,
-        sor_inner_max, sort_every, graph_steps, sor_exchange, smooth_fft, sor_omega)."""
+        sor_inner_max, sort_every, graph_steps, sor_exchange, smooth_fft, sor_omega,
+        sor_wait_limit, sor_coarse, sor_coarse_sweeps, deposit_aggregate)."""
         o = self.fast_options()
         for k, v in kw.items():
             if not hasattr(o, k):
                 raise KeyError(k)
             setattr(o, k, float(v) if k == "sor_omega" else int(v))
         L.check(self.lib.hv_ctx_set_fast_options(self._ctx, C.byref(o)), "hv_ctx_set_fast_options")
+
+    def autotune(self, trial_steps=4):
+        """hv_ctx_autotune: times the particle step's launch configurations and
+        the SOR tiles over trial_steps fused steps each (the steps advance the
+        run) and keeps the fastest; returns what it chose as a dict."""
+        r = L.hv_autotune_report()
+        L.check(self.lib.hv_ctx_autotune(self._ctx, int(trial_steps), C.byref(r)), "hv_ctx_autotune")
+        return {k: getattr(r, k) for k, _ in r._fields_}
 
     KERNELS = ("particle", "smooth", "skyrme", "sor", "forces")
 
@@ -336,3 +345,9 @@ def simulate(w: Workload, x, y, z, kx, ky, kz, steps, precision=L.HV_F64, path=L
     L.check(lib.hv_simulate(C.byref(world), w.protons, w.neutrons, precision, C.byref(params), path, steps,
                             *[_p(a) for a in arrs], C.c_void_p(obs.ctypes.data)), "hv_simulate")
     return obs
+
+
+def simulate_release():
+    """hv_simulate_release: frees the device contexts hv_simulate keeps
+    between calls."""
+    L.check(L.load().hv_simulate_release(), "hv_simulate_release")

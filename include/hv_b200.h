@@ -274,9 +274,9 @@ HV_API hv_status hv_observe(hv_ctx *ctx, hv_observables *out);
  * Scratch is a fixed 256 KiB array inside the library, held by every GPU that
  * loads it until the process exits; one call handles at most
  * HV_NOALLOC_MAX_PARTICLES particles and rejects more with HV_ERR_BAD_ARG.
- * The first call on a device looks up the array's device address (do that
- * call before any stream capture).  All calls share the array: calls whose
- * work overlaps on the GPU race.  Work is queued on `stream` (a cudaStream_t,
+ * Each call looks up the array's address on the current device (a lookup
+ * that allocates nothing).  All calls share the array: calls whose work
+ * overlaps on the GPU race.  Work is queued on `stream` (a cudaStream_t,
  * NULL for the default stream) and the call returns after it completes. */
 #define HV_NOALLOC_MAX_PARTICLES (4096 * 1024)
 HV_API hv_status hv_observe_noalloc(const hv_world *world, int protons, int neutrons, int nucleus_z,
@@ -332,13 +332,63 @@ typedef struct hv_fast_options {
                              FP64 residual test; on 208Pb 128^3 (rule 1e-6)
                              1.8 / 1.85 / 1.9 / 1.93 took 169 / 144 / 120 / 105
                              iterations per step with D(t) equal to 1e-8      */
+    int sor_wait_limit;   /* polls a device-side wait of the fused solver (grid
+                             barrier, neighbour row) makes before it gives up
+                             and the run returns HV_ERR_TIMEOUT; 0 (the
+                             default): 2^24 for barriers, 2^22 per row entry
+                             (about a second).  The context stays usable after
+                             a timeout                                         */
+    int sor_coarse;       /* 1 (the default): each cycle of the fused float
+                             solve starts its correction from the correction
+                             equation solved exactly on a coarse grid (every
+                             F-th node, F the smallest power of two leaving at
+                             most 15 interior coarse nodes per axis; grids
+                             whose axes F does not divide, double solves, the
+                             max-update rule and batched runs go without), and
+                             runs sor_coarse_sweeps red+black iterations after
+                             it; 0: plain SOR cycles.  The stopping rule is
+                             unchanged; on 208Pb 128^3 ...                     */
+    int sor_coarse_sweeps;/* red+black iterations after each coarse correction
+                             (default 16)                                      */
+    int deposit_aggregate;/* 1 (the default): the float atomic deposit of the
+                             fused particle step sums the CIC weights of
+                             neighbouring lanes with the same base node (the
+                             slots are re-sorted by cell) and adds each run
+                             once; 0: one set of atomics per particle          */
 } hv_fast_options;
 
 /* Defaults: HV_WARM_QUADRATIC, inner 8..256, sort every 16 steps, 8-step graphs,
- * HV_SOR_EXCHANGE_AUTO, smooth_fft 1, sor_omega 0 (the run's omega). */
+ * HV_SOR_EXCHANGE_AUTO, smooth_fft 1, sor_omega 0 (the run's omega),
+ * sor_wait_limit 0, sor_coarse 1 with 16 sweeps per cycle, deposit_aggregate 1. */
 HV_API void hv_fast_options_default(hv_fast_options *o);
 HV_API hv_status hv_ctx_set_fast_options(hv_ctx *ctx, const hv_fast_options *o);
 HV_API hv_status hv_ctx_get_fast_options(const hv_ctx *ctx, hv_fast_options *o);
+
+/* What hv_ctx_autotune chose. */
+typedef struct hv_autotune_report {
+    int particle_block;    /* threads per block of the particle step          */
+    int particle_grid;     /* its blocks (a multiple of the SM count)         */
+    int sor_planes;        /* the SOR tile: planes x rows owned by one block  */
+    int sor_rows;
+    int sor_blocks;        /* blocks of the solve                             */
+    int sor_tile_rank;     /* rank of the tile in the plan's own order (0: the
+                              plan's heuristic choice)                        */
+    int candidates;        /* configurations timed                            */
+    double particle_ms;    /* device ms per launch of the chosen particle step */
+    double sor_ms;         /* device ms per launch of the solve with the chosen
+                              tile                                             */
+} hv_autotune_report;
+
+/* Chooses the fused path's launch configuration for this context by timing
+ * candidates over trial_steps steps each (CUDA events around each launch):
+ * first the particle step's block size (128, 256, 512 threads) and grid (2, 4,
+ * 8 blocks per SM) with the planned SOR tile, then the SOR tile among the
+ * plan's four best-ranked P x R partitions (the ranking hv_run's plan uses:
+ * fewest quads per thread, then least exchanged face, then fewest blocks).
+ * The trial steps advance the run like hv_run (solving the initial fields
+ * first if needed); the choice holds for later hv_run calls on the context.
+ * No counterpart in the reference. */
+HV_API hv_status hv_ctx_autotune(hv_ctx *ctx, int trial_steps, hv_autotune_report *report);
 
 /* Kernels of one fused step, for hv_ctx_kernel_times. */
 typedef enum hv_kernel_id {
@@ -382,11 +432,20 @@ HV_API hv_status hv_run(hv_ctx *ctx, int n_steps, int path, hv_observables *obs)
 /* The whole gpu_simulate slot (src/hyper_vlasov.cpp:120-123) with host
  * buffers: uploads the particles, runs the initial solve and n_steps steps,
  * downloads the final particles (in place) and n_steps observable rows.
- * Element type of the particle pointers follows prec. */
+ * Element type of the particle pointers follows prec.  Runs on the current
+ * device.  The device context of a call is kept afterwards and reused by the
+ * next call with the same device, world, particle counts and precision (any
+ * run parameters), reset to the state a new context starts from, so that a
+ * caller stepping many nuclei of one shape pays for allocation and planning
+ * once; at most four idle contexts are kept, and a call that fails destroys
+ * its context.  Concurrent calls never share a context. */
 HV_API hv_status hv_simulate(const hv_world *world, int protons, int neutrons,
                       hv_precision prec, const hv_run_params *params, int path,
                       int n_steps, void *x, void *y, void *z,
                       void *kx, void *ky, void *kz, hv_observables *obs);
+/* Destroys the contexts hv_simulate keeps between calls (device memory is
+ * returned); the next call creates a new one. */
+HV_API hv_status hv_simulate_release(void);
 
 /* compute_particle_densities (include/tools.hpp:170-203), part of the
  * reference's initialisation (initialize_particles, include/physics.hpp:34-97):

@@ -97,6 +97,16 @@ ORC_DECLARE(float, f)
 /* OpenMP thread count of the restatement. */
 void orc_set_threads(int n);
 
+/* Seeded synthetic nucleus (MT19937-64), the inputs of every workload: see
+ * hv_oracle.c.  Returns 0, or 1 for a bad argument. */
+#include <stdint.h>
+int orc_generate_nucleus_d(uint64_t seed, int protons, int neutrons, double radius, double k_fermi, double *x,
+                           double *y, double *z, double *kx, double *ky, double *kz);
+int orc_generate_nucleus_f(uint64_t seed, int protons, int neutrons, double radius, double k_fermi, float *x,
+                           float *y, float *z, float *kx, float *ky, float *kz);
+/* the n-th output (n >= 1) of MT19937-64 seeded with `seed` */
+uint64_t orc_mt64_nth(uint64_t seed, long long n);
+
 #ifdef __cplusplus
 }
 #endif

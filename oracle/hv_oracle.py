@@ -267,6 +267,26 @@ def reference_available(variant=""):
     return os.path.exists(os.path.join(REF_DIR, f"libhvref{variant}.so"))
 
 
+def _generate(lib, seed, protons, neutrons, radius, k_fermi, dtype):
+    """Six arrays x..kz of the seeded synthetic nucleus from the checker
+    library `lib` (orc_generate_nucleus_*, hv_oracle.c)."""
+    dt = np.dtype(dtype)
+    total = int(protons) + int(neutrons)
+    arrs = [np.zeros(total, dt) for _ in range(6)]
+    f = lib.orc_generate_nucleus_d if dt == np.float64 else lib.orc_generate_nucleus_f
+    f.restype = C.c_int
+    f.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_double, C.c_double] + [_P] * 6
+    if f(int(seed), int(protons), int(neutrons), float(radius), float(k_fermi), *[_ptr(a) for a in arrs]) != 0:
+        raise ValueError("orc_generate_nucleus: bad argument")
+    return arrs
+
+
+def workload_inputs(lib, w, dtype):
+    """The inputs of workload w (any object with seed, protons, neutrons,
+    radius and k_fermi) from the checker library `lib`."""
+    return _generate(lib, w.seed, w.protons, w.neutrons, w.radius, w.k_fermi, dtype)
+
+
 class Reference:
     """The reference's own routines.  variant: "" (-ffp-contract=off),
     "_native" (the reference Makefile's -O3 -march=native), "_portable"

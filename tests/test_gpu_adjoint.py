@@ -165,3 +165,23 @@ def test_adjoint_matches_fp64_tangent_linear_cpu_run(hv):
         g_tl[i] = wts @ dD
     assert np.max(np.abs(d_cpu - d_gpu)) <= 1e-9 * np.abs(d_cpu).max()
     assert np.all(np.abs(g_adj - g_tl) <= 1e-6 * np.abs(g_tl).max()), (g_adj, g_tl)
+
+
+def test_adjoint_backward_after_a_resorting_fused_run_keeps_the_caller_order(hv):
+    """A fused run between the forward and the backward pass re-sorts the
+    particle slots; the backward pass restores the forward's checkpoints with
+    their slot permutation, so the state it leaves downloads in the caller's
+    order, equal to the forward's final state."""
+    steps = 8
+    w, parts, theta = _setup(hv, steps)
+    with hv.Session.from_workload(w, hv.HV_F64) as s:
+        s.upload_particles(*parts)
+        s.initial_solve()
+        s.adjoint_forward(steps, 4)
+        after_forward = s.download_particles()
+        s.set_fast_options(sort_every=1)
+        s.run(3, hv.HV_PATH_FUSED)
+        s.adjoint_backward(np.ones(steps), theta)
+        after_backward = s.download_particles()
+    for a, b in zip(after_backward, after_forward):
+        assert a.tobytes() == b.tobytes()

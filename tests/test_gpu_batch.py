@@ -84,3 +84,45 @@ def test_batch_rejects_double_contexts(hv):
     with hv.Session.from_workload(w, hv.HV_F64) as s:
         with pytest.raises(hv.HVError):
             Batch([s])
+
+
+def test_batch_instances_of_every_nucleus_match_the_double_oracle(hv):
+    """The 64-run batched workload (full test-particle counts) advanced
+    together for 40 steps; for one instance of each nucleus (16O, 40Ca, 90Zr,
+    208Pb: the smallest of each), D(t) within 1e-3 of the double oracle's
+    largest |D| from the same float particles -- the FP32 form's accuracy
+    bound, checked on the batched form."""
+    import os
+
+    from hv_b200.batch import Batch
+    from hv_b200.workloads import batch_workloads
+    from hv_oracle import Oracle, RunSpec
+    from conftest import max_rel
+    ws = batch_workloads(64, seed=0)
+    steps = 40
+    pick = {}
+    for i, w in enumerate(ws):
+        key = w.name.split("-")[0]
+        if key not in pick or w.particles + w.G < ws[pick[key]].particles + ws[pick[key]].G:
+            pick[key] = i
+    assert sorted(pick) == ["16O", "208Pb", "40Ca", "90Zr"]
+    sess = _sessions(hv, ws)
+    try:
+        with Batch(sess) as b:
+            obs = b.run(steps)
+    finally:
+        for s in sess:
+            s.close()
+    o = Oracle(np.float64)
+    o.set_threads(os.cpu_count() or 4)
+    for key, i in sorted(pick.items()):
+        w = ws[i]
+        A, B, C, gm = w.skyrme()
+        run = RunSpec(z=w.Z, n=w.N, part_per_nucleon=w.ppn, sigma_r=w.sigma_r, dt=w.dt, t_exc=w.t_exc,
+                      eta_exc=w.eta, A=A, B=B, C=C, gamma=gm, sor_omega=w.sor_omega, sor_tol=w.sor_tol,
+                      sor_criterion=w.sor_criterion, sor_max_iter=w.sor_max_iter)
+        p = [a.astype(np.float64) for a in hv.workload_particles(w, np.float32)]
+        obs_o, _ = o.simulate(w.world_tuple(), run, w.protons, w.neutrons, *p, steps)
+        assert not np.any(obs[i]["flags"] & 1), w.name
+        err = max_rel(obs[i]["dipole"], obs_o["dipole"])
+        assert err <= 1e-3, (w.name, err)

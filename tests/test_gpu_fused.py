@@ -5,8 +5,10 @@ Tolerances
     double oracle (the accuracy target of the float form), <= 1e-6 for the
     double fused path against the double plain path;
   * SOR: every step converges to the same stopping rule (relative residual
-    1e-6); the fused solver checks it every few iterations, so it may run up
-    to sor_inner_max iterations more than the plain solver, never fewer;
+    1e-6); with plain SOR cycles (sor_coarse = 0) the fused solver checks it
+    every few iterations, so it may run up to sor_inner_max iterations more
+    than the plain solver, never fewer; with the coarse-grid correction (the
+    default) far fewer, and D(t) within 1e-6 of the plain cycles' run;
   * fields after a fused run: smoothed density and potential of the final
     positions within 1e-5 (float) of the oracle's, forces within 1e-4.
 """
@@ -57,7 +59,7 @@ def test_fused_f32_dipole_within_1e_3_of_double_oracle(hv):
     steps = 200
     p32 = hv.workload_particles(w, np.float32)
     obs_o, _ = _oracle(w, steps, [p.astype(np.float64) for p in p32])
-    obs, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_PREVIOUS)
+    obs, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_PREVIOUS, sor_coarse=0)
     assert np.array_equal(obs["t"], obs_o["t"].astype(np.float32).astype(np.float64)) or \
         np.max(np.abs(obs["t"] - obs_o["t"])) < 1e-4
     err = max_rel(obs["dipole"], obs_o["dipole"])
@@ -101,14 +103,14 @@ def test_extrapolated_warm_start_saves_iterations(hv):
     steps = 60
     p32 = hv.workload_particles(w, np.float32)
     obs_a, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_PREVIOUS, sor_inner_min=1,
-                      sor_inner_max=8)
+                      sor_inner_max=8, sor_coarse=0)
     obs_b, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_EXTRAPOLATE, sor_inner_min=1,
-                      sor_inner_max=8)
+                      sor_inner_max=8, sor_coarse=0)
     assert obs_b["sor_iterations"][10:].sum() < obs_a["sor_iterations"][10:].sum()
     assert max_rel(obs_b["dipole"], obs_a["dipole"]) < 1e-3
     # the quadratic guess 3 phi_n - 3 phi_(n-1) + phi_(n-2) (the default)
     obs_c, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_warm_start=hv.HV_WARM_QUADRATIC, sor_inner_min=1,
-                      sor_inner_max=8)
+                      sor_inner_max=8, sor_coarse=0)
     assert obs_c["sor_iterations"][10:].sum() < obs_b["sor_iterations"][10:].sum()
     assert max_rel(obs_c["dipole"], obs_a["dipole"]) < 1e-3
     assert not np.any(obs_c["flags"] & 1)
@@ -125,7 +127,7 @@ def test_first_steps_after_the_fused_initial_solve_start_from_solutions(hv):
     its = {}
     for ws in (hv.HV_WARM_PREVIOUS, hv.HV_WARM_QUADRATIC):
         with hv.Session.from_workload(w, hv.HV_F32) as s:
-            s.set_fast_options(sor_warm_start=ws, sor_inner_min=1, sor_inner_max=8)
+            s.set_fast_options(sor_warm_start=ws, sor_inner_min=1, sor_inner_max=8, sor_coarse=0)
             s.upload_particles(*p32)
             its[ws] = s.run(6, hv.HV_PATH_FUSED)["sor_iterations"].astype(np.int64)
     prev, quad = its[hv.HV_WARM_PREVIOUS], its[hv.HV_WARM_QUADRATIC]
@@ -143,8 +145,8 @@ def test_sor_omega_override_keeps_the_stopping_rule(hv):
     w = hv.CA40_SMALL
     steps = 30
     p32 = hv.workload_particles(w, np.float32)
-    obs_a, _ = _fused(hv, w, steps, hv.HV_F32, p32)
-    obs_b, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_omega=1.9)
+    obs_a, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_coarse=0)
+    obs_b, _ = _fused(hv, w, steps, hv.HV_F32, p32, sor_omega=1.9, sor_coarse=0)
     assert not np.any(obs_b["flags"] & 1)
     assert obs_b["sor_iterations"][5:].sum() != obs_a["sor_iterations"][5:].sum()
     assert max_rel(obs_b["dipole"], obs_a["dipole"]) < 1e-4
@@ -334,7 +336,7 @@ def test_tagged_exchange_matches_flag_exchange(hv, n):
     res = []
     for exchange in (hv.HV_SOR_EXCHANGE_FLAGS, hv.HV_SOR_EXCHANGE_AUTO):
         with hv.Session(world, w.protons, w.neutrons, w.run_params(), hv.HV_F32) as s:
-            s.set_fast_options(sor_exchange=exchange)
+            s.set_fast_options(sor_exchange=exchange, sor_coarse=0)
             s.upload_particles(*p)
             s.initial_solve()
             obs = s.run(4, hv.HV_PATH_FUSED)
@@ -415,3 +417,135 @@ def test_fused_sorted_deposit_is_deterministic(hv, prec):
     assert all(np.array_equal(a, b) for a, b in zip(runs[0][1], runs[1][1]))
     obs_a, _ = _fused(hv, replace(w, deposit_mode=hv.HV_DEPOSIT_ATOMIC), 30, P, p)
     assert max_rel(runs[0][0]["dipole"], obs_a["dipole"]) < (1e-5 if prec == "f32" else 1e-10)
+
+
+def test_bounded_waits_time_out_and_the_context_recovers(hv):
+    """hv_fast_options.sor_wait_limit bounds every device-side wait of the
+    fused solver.  With a limit of one poll the blocks' grid barriers and
+    neighbour rows give up, the kernel returns and the run reports
+    HV_ERR_TIMEOUT (the reference's solver would instead warn and carry on,
+    include/physics.hpp:155-156); with the default limit restored, the same
+    context solves normally again and matches a new context's run."""
+    from hv_b200 import _lib as L
+    w = hv.PB208_104K
+    p32 = hv.workload_particles(w, np.float32)
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        # 64^3 takes several blocks of the solver, so some of them must wait
+        s.set_fast_options(sor_wait_limit=1)
+        s.upload_particles(*p32)
+        with pytest.raises(hv.HVError) as e:
+            s.run(2, hv.HV_PATH_FUSED)
+        assert e.value.status == L.HV_ERR_TIMEOUT
+        s.set_fast_options(sor_wait_limit=0)
+        s.upload_particles(*p32)
+        obs = s.run(6, hv.HV_PATH_FUSED)
+    assert not np.any(obs["flags"] & 1)
+    obs_new, _ = _fused(hv, w, 6, hv.HV_F32, p32)
+    assert max_rel(obs["dipole"], obs_new["dipole"]) < 1e-6, max_rel(obs["dipole"], obs_new["dipole"])
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_uploads_and_downloads_follow_the_slot_permutation(hv, prec):
+    """After fused runs have re-sorted the slots, particles uploaded (all
+    arrays, or one at a time) come back in the caller's order, bit for bit, in
+    both precisions; and D(t) after the re-sort matches an unsorted run."""
+    w = hv.CA40_SMALL
+    dt = np.float32 if prec == "f32" else np.float64
+    P = hv.HV_F32 if prec == "f32" else hv.HV_F64
+    parts = hv.workload_particles(w, dt)
+    rng = np.random.default_rng(5)
+    with hv.Session.from_workload(w, P) as s:
+        s.set_fast_options(sort_every=4)
+        s.upload_particles(*parts)
+        s.run(12, hv.HV_PATH_FUSED)
+        new = [(p + dt(0.1) * rng.standard_normal(p.size).astype(dt)).astype(dt) for p in parts]
+        s.upload_particles(*new)
+        got = s.download_particles()
+        for a, b in zip(got, new):
+            assert a.tobytes() == b.tobytes()
+        one = (new[2] * dt(0.5)).astype(dt)
+        s.upload_array("z", one)
+        assert s.download_array("z").tobytes() == one.tobytes()
+
+
+@pytest.mark.parametrize("wname,n", [("208Pb-20.8k-128^3", (128, 128, 128)), ("208Pb-104k-64^3", (64, 64, 64)),
+                                     ("40Ca-4k-32^3", (32, 32, 32)), ("40Ca-4k-32^3", (64, 32, 128))])
+def test_coarse_grid_correction_keeps_the_stopping_rule(hv, wname, n):
+    """The coarse-grid correction of the fused float solve (the default) ends
+    every solve at the same FP64 stopping rule as plain SOR cycles: D(t) and
+    the Coulomb potential agree within 1e-6 relative (the tolerance of each
+    solve), the particles to float rounding, and the iterations per step fall
+    well below the plain cycles' (coarse factors 8, 4, 2 and a non-cubic grid,
+    8 on each axis)."""
+    w = hv.WORKLOADS[wname]
+    world = _world(n, w.h)
+    p = hv.workload_particles(w, np.float32)
+    res = []
+    for coarse in (0, 1):
+        with hv.Session(world, w.protons, w.neutrons, w.run_params(), hv.HV_F32) as s:
+            s.set_fast_options(sor_coarse=coarse)
+            s.upload_particles(*p)
+            s.initial_solve()
+            obs = s.run(12, hv.HV_PATH_FUSED)
+            res.append((obs, s.download_particles(), s.download_field(hv.HV_FIELD_COULOMB)))
+    (o0, p0, c0), (o1, p1, c1) = res
+    assert not np.any(o0["flags"] & 1) and not np.any(o1["flags"] & 1)
+    assert max_rel(o1["dipole"], o0["dipole"]) < 1e-6, max_rel(o1["dipole"], o0["dipole"])
+    assert max_rel(c1, c0) < 1e-6, max_rel(c1, c0)
+    assert all(np.max(np.abs(a - b)) < 1e-4 for a, b in zip(p0, p1))
+    its0, its1 = o0["sor_iterations"][2:].mean(), o1["sor_iterations"][2:].mean()
+    if n[0] >= 64:
+        assert its1 < 0.6 * its0, (its1, its0)
+
+
+
+@pytest.mark.parametrize("wname", ["40Ca-4k-32^3", "208Pb-104k-64^3"])
+def test_warp_aggregated_deposit_matches_the_oracle(hv, wname):
+    """The fused float deposit summed over warp runs of equal base nodes
+    (hv_fast_options.deposit_aggregate, the default) against one set of
+    atomics per particle and against the oracle's deposit of the same final
+    positions: the raw density within float rounding (1e-5 of its maximum),
+    after re-sorted slots (sort_every = 1) and from unsorted ones."""
+    from hv_oracle import Oracle
+    w = hv.WORKLOADS[wname]
+    p32 = hv.workload_particles(w, np.float32)
+    o = Oracle(np.float32)
+    for every in (0, 1):
+        raws = []
+        for agg in (0, 1):
+            with hv.Session.from_workload(w, hv.HV_F32) as s:
+                s.set_fast_options(deposit_aggregate=agg, sort_every=every)
+                s.upload_particles(*p32)
+                s.run(3, hv.HV_PATH_FUSED)
+                raws.append(s.download_field(hv.HV_FIELD_DENSITY_RAW))
+                x, y, z, *_ = s.download_particles()
+        ref = o.deposit(w.world_tuple(), w.protons, w.neutrons, x, y, z)
+        assert max_rel(raws[1], ref) < 1e-5, (every, max_rel(raws[1], ref))
+        assert max_rel(raws[0], raws[1]) < 1e-3  # the two runs' particles differ by rounding
+
+
+def test_autotune_chooses_a_configuration_and_keeps_results(hv):
+    """hv_ctx_autotune times the particle step's block sizes and grids and the
+    SOR's best-ranked tiles, keeps the fastest, and the run continues with the
+    same physics: D(t) of the steps after it matches a run that advanced the
+    same number of steps without it (float rounding of the atomic deposit
+    aside: 1e-4)."""
+    w = hv.PB208_20K_128
+    p32 = hv.workload_particles(w, np.float32)
+    trial = 2
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        s.upload_particles(*p32)
+        rep = s.autotune(trial)
+        obs_a = s.run(8, hv.HV_PATH_FUSED)
+    assert rep["particle_block"] in (128, 256, 512)
+    assert rep["particle_grid"] > 0
+    assert rep["sor_planes"] >= 1 and rep["sor_rows"] >= 1 and rep["sor_blocks"] >= 1
+    assert 0 <= rep["sor_tile_rank"] < 4 and rep["candidates"] >= 10
+    assert rep["particle_ms"] > 0 and rep["sor_ms"] > 0
+    steps_taken = int(round(obs_a["t"][0] / w.dt))
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        s.upload_particles(*p32)
+        s.run(steps_taken, hv.HV_PATH_FUSED)
+        obs_b = s.run(8, hv.HV_PATH_FUSED)
+    assert np.allclose(obs_a["t"], obs_b["t"])
+    assert max_rel(obs_a["dipole"], obs_b["dipole"]) < 1e-4, max_rel(obs_a["dipole"], obs_b["dipole"])

@@ -97,3 +97,33 @@ def test_plain_f32_tracks_f64(hv):
         s.initial_solve()
         o64 = s.run(steps, hv.HV_PATH_PLAIN)
     assert max_rel(o32["dipole"], o64["dipole"]) < 1e-3
+
+
+def test_simulate_reuses_its_context_as_new(hv):
+    """hv_simulate keeps its device context between calls of one shape: a
+    second call (after a call of another nucleus shape and one with other
+    parameters, on the fused path that re-sorts the slots) computes what the
+    first did -- bit for bit on the deterministic plain FP64 path -- and
+    hv_simulate_release frees the kept contexts."""
+    from dataclasses import replace
+    w = hv.CA40_SMALL
+    steps = 4
+    parts = hv.workload_particles(w, np.float64)
+    a = [v.copy() for v in parts]
+    obs1 = hv.simulate(w, *a, steps, hv.HV_F64, hv.HV_PATH_PLAIN)
+    # the same shape on the fused path (slots re-sorted), other parameters
+    b = [v.copy() for v in parts]
+    hv.simulate(replace(w, t0=-2600.0), *b, 20, hv.HV_F64, hv.HV_PATH_FUSED)
+    # another shape in between
+    w2 = replace(w, ppn=50)
+    hv.simulate(w2, *hv.workload_particles(w2, np.float64), 2, hv.HV_F64, hv.HV_PATH_PLAIN)
+    c = [v.copy() for v in parts]
+    obs2 = hv.simulate(w, *c, steps, hv.HV_F64, hv.HV_PATH_PLAIN)
+    assert obs1.tobytes() == obs2.tobytes()
+    for u, v in zip(a, c):
+        assert u.tobytes() == v.tobytes()
+    hv.simulate_release()
+    d = [v.copy() for v in parts]
+    obs3 = hv.simulate(w, *d, steps, hv.HV_F64, hv.HV_PATH_PLAIN)
+    assert obs3.tobytes() == obs1.tobytes()
+    hv.simulate_release()

@@ -75,3 +75,71 @@ def test_assignment_covers_every_run_once(world):
     assert sorted(sum(parts, [])) == list(range(20))
     loads = [sum(costs[i] for i in p) for p in parts]
     assert max(loads) - min(loads) <= max(costs)
+
+
+def _batch_runs():
+    """Small instances of the batched workload (grids up to 48^3, 20 test
+    particles per nucleon) for CPU ranks."""
+    from dataclasses import replace
+
+    from hv_b200.workloads import batch_workloads
+    return [replace(w, ppn=20) for w in batch_workloads(64, seed=0) if w.n <= 48][:6]
+
+
+def _oracle_dipole(w, steps):
+    """D(t) of one run from the C oracle (the CPU stand-in for a rank's device
+    compute), from the seeded inputs the library's generator gives."""
+    import numpy as np
+
+    from hv_oracle import Oracle, RunSpec, workload_inputs
+    o = Oracle(np.float64)
+    o.set_threads(1)
+    A, B, C, gm = w.skyrme()
+    run = RunSpec(z=w.Z, n=w.N, part_per_nucleon=w.ppn, sigma_r=w.sigma_r, dt=w.dt, t_exc=w.t_exc, eta_exc=w.eta,
+                  A=A, B=B, C=C, gamma=gm, sor_omega=w.sor_omega, sor_tol=w.sor_tol,
+                  sor_criterion=w.sor_criterion, sor_max_iter=w.sor_max_iter)
+    parts = workload_inputs(o.lib, w, np.float64)
+    obs, _ = o.simulate(w.world_tuple(), run, w.protons, w.neutrons, *parts, steps)
+    return [float(v) for v in obs["dipole"]]
+
+
+def _batch_worker(rank, world, port, steps, q):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        runs = _batch_runs()
+        mine = replicas.assign_runs([replicas.run_cost(w.particles, w.G) for w in runs], world)[rank]
+        series = {i: _oracle_dipole(runs[i], steps) for i in mine}
+        merged = replicas.gather_series(series, world)
+        q.put((rank, mine, merged))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_share_a_batch_and_gather_its_dipole_series():
+    """Two gloo ranks take their LPT shares of six instances of the batched
+    workload, compute each run's D(t) (the C oracle standing in for the
+    device), and gather the series: every rank ends with all six, equal bit
+    for bit to one process computing them all."""
+    steps = 3
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_worker, args=(r, world, port, steps, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=300) for _ in range(world)], key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    runs = _batch_runs()
+    assert sorted(res[0][1] + res[1][1]) == list(range(len(runs)))
+    single = {i: _oracle_dipole(w, steps) for i, w in enumerate(runs)}
+    for _, _, merged in res:
+        assert sorted(merged) == list(range(len(runs)))
+        assert all(merged[i] == single[i] for i in single)

@@ -6,8 +6,10 @@ It is called through the C ABI on particle arrays that live in device memory
 the test owns, and its result is compared with the context-based hv_observe on
 the same particles, within the tolerance of the other observable tests
 (1e-12 on centres of mass, 1e-11 on mean squared radii), on two calls in a row
-with different particles.  This file is collected last so that a run that
-stops at the first failure has run every other test first.
+with different particles.  The device's free memory (cudaMemGetInfo) is the
+same before and after each of those calls: the entry point allocates nothing.
+This file is collected last so that a run that stops at the first failure has
+run every other test first.
 """
 from __future__ import annotations
 
@@ -37,6 +39,11 @@ def test_noalloc_observe_matches_context_observe_twice(hv, dtype):
     prec = hv.HV_F64 if dtype == "f64" else hv.HV_F32
     parts = hv.workload_particles(w, npdt)
     stream = torch.cuda.current_stream().cuda_stream
+    # one call before the measured ones: the first launch of a kernel may load
+    # the library's device code, which the driver places in device memory
+    warm = [torch.from_numpy(p.copy()).cuda() for p in parts[:3]]
+    torch.cuda.synchronize()
+    assert _noalloc(lib, L, w, prec, warm, stream)[0] == L.HV_OK, lib.hv_last_error()
     with hv.Session.from_workload(w, prec, device=0) as s:
         for call in range(2):
             if call == 1:  # different particles on the second call, same sizes
@@ -46,8 +53,11 @@ def test_noalloc_observe_matches_context_observe_twice(hv, dtype):
             ref = s.observe()
             xs = [torch.from_numpy(p.copy()).cuda() for p in parts[:3]]
             torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             st, got = _noalloc(lib, L, w, prec, xs, stream)
+            free_after = torch.cuda.mem_get_info()[0]
             assert st == L.HV_OK, lib.hv_last_error()
+            assert free_after == free_before, (free_before, free_after)
             assert abs(got.zcm_p - ref.zcm_p) < 1e-12 and abs(got.zcm_n - ref.zcm_n) < 1e-12
             assert abs(got.rms_p ** 2 - ref.rms_p ** 2) < 1e-11 and abs(got.rms_n ** 2 - ref.rms_n ** 2) < 1e-11
             assert abs(got.dipole - ref.dipole) < 1e-11
