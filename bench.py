@@ -187,18 +187,28 @@ def max_over_ranks(world, v):
     return replicas.max_over_ranks(v, world)
 
 
-def step_bytes(w, n_sor, wordsize=4):
+def sor_checks(n_sor, sweeps_per_cycle):
+    """FP64 residual checks of a solve of n_sor red+black iterations whose
+    cycles run sweeps_per_cycle iterations each (the coarse-corrected solve):
+    one before each cycle and one after the last."""
+    return math.ceil(n_sor / sweeps_per_cycle) + 1 if sweeps_per_cycle > 0 else 2
+
+
+def step_bytes(w, n_sor, wordsize=4, checks=2):
     """Algorithmic bytes of one step, per kernel: 48 B per particle (x, k read
     and written) and 4 G (24 + 3 n_sor) B of grid traffic (deposit 2 words per
     node, smoothing 4, Skyrme 4, merge 2, FDM 8, gather 6 minus overlap, SOR 3
-    per iteration)."""
+    per iteration).  The solve also streams its FP64 state: the extrapolated
+    start (read phi and its two predecessors, write all three: 48 B per node)
+    and each residual check (read phi and the carried residual, write both:
+    32 B per node)."""
     G, N = w.G, w.particles
     s = wordsize / 4.0
     return {
         "particle": s * (48 * N + 4 * G * (2 + 6)),
         "smooth": s * 4 * G * 4,
         "skyrme": s * 4 * G * 4,
-        "sor": s * 4 * G * 3 * n_sor,
+        "sor": s * 4 * G * 3 * n_sor + G * (48 + 32 * checks),
         "forces": s * 4 * G * 10,
     }
 
@@ -705,7 +715,10 @@ def our_arm(args, world, rank, local):
     kt = sess.kernel_times()
     sess.set_profiling(False)
     its_p = obs_p["sor_iterations"].astype(np.int64)
-    nbytes = step_bytes(w, its_p.mean(), 4 if prec == hv.HV_F32 else 8)
+    fo = sess.fast_options()
+    per_cycle = fo.sor_coarse_sweeps if (fo.sor_coarse and prec == hv.HV_F32) else 0
+    ws_ = 4 if prec == hv.HV_F32 else 8
+    nbytes = step_bytes(w, its_p.mean(), ws_, float(np.mean([sor_checks(n, per_cycle) for n in its_p])))
     tot_ms = sum(v[0] for v in kt.values())
     kernels = {}
     for k, (kms, n) in kt.items():
@@ -716,7 +729,7 @@ def our_arm(args, world, rank, local):
         kernels[k] = {"launches": n, "avg_ms": per, "share": kms / tot_ms if tot_ms else None,
                       "algorithmic_bytes": b, "gbs": b / (per / 1e3) / 1e9}
     peak, peak_kind = peaks()
-    sor_b = sum(step_bytes(w, n, 4 if prec == hv.HV_F32 else 8)["sor"] for n in its_p)
+    sor_b = sum(step_bytes(w, n, ws_, sor_checks(n, per_cycle))["sor"] for n in its_p)
     sor_ms = kt["sor"][0]
     achieved = sor_b / (sor_ms / 1e3) / 1e9 if sor_ms > 0 else None
     traffic = None
@@ -728,9 +741,11 @@ def our_arm(args, world, rank, local):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "traffic": traffic,
-                "kernel": "k_sor_fast (persistent red-black SOR)", "peak_source": peak_kind,
-                "bytes": "12 B per node per red+black iteration (read phi, rho_p; write phi)",
-                "mean_sor_iterations": float(its_p.mean())}
+                "kernel": "k_sor_fast (persistent red-black SOR, coarse-grid corrected)", "peak_source": peak_kind,
+                "bytes": "per solve: 12 B per node per red+black iteration (read phi, rho_p; write phi), 48 B per "
+                         "node for the extrapolated start, 32 B per node per FP64 residual check",
+                "mean_sor_iterations": float(its_p.mean()),
+                "sor_checks_per_solve": float(np.mean([sor_checks(n, per_cycle) for n in its_p]))}
 
     # per step: particle step, smoothing, Skyrme, SOR, forces, step counter;
     # the FFT smoothing (power-of-two axes up to 128; by default for stencil

@@ -1789,7 +1789,6 @@ hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std:
         if (c->prec != HV_F32 || !c->fused.sor.ok) return HV_ERR_UNSUPPORTED;
         const int fi = sor_fast_args<float>(c, rho[i], ctl[i], its_ring[i], ring, args[i]);
         if (fi == 0) return HV_ERR_UNSUPPORTED;  // the batched form needs the tagged exchange
-        args[i].coarse = 0;  // the waves run the plain sweeps
         any1 = any1 || fi == 1;
         all2 = all2 && fi == 2;
         bfirst[i] = (int)binst.size();
@@ -1797,6 +1796,10 @@ hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std:
         smem = std::max(smem, c->fused.sor.smem);
     }
     const int form = any1 ? 1 : all2 ? 2 : 3;
+    // the coarse-grid correction needs the staged sweep (its ghost buffer and
+    // row tables); a wave of generic tagged sweeps runs plain cycles
+    if (form == 1)
+        for (auto &a : args) a.coarse = 0;
     int dev = 0;
     HV_CUDA(cudaGetDevice(&dev));
     cudaDeviceProp prop;

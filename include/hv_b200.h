@@ -347,7 +347,8 @@ typedef struct hv_fast_options {
                              max-update rule and batched runs go without), and
                              runs sor_coarse_sweeps red+black iterations after
                              it; 0: plain SOR cycles.  The stopping rule is
-                             unchanged; on 208Pb 128^3 ...                     */
+                             unchanged, so only the iterations per solve
+                             change                                            */
     int sor_coarse_sweeps;/* red+black iterations after each coarse correction
                              (default 16)                                      */
     int deposit_aggregate;/* 1 (the default): the float atomic deposit of the
