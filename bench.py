@@ -571,6 +571,7 @@ def batched(args, local, world=1, rank=0):
         with Batch(sess) as b:
             setup = time.perf_counter() - t0
             cap = b.autotune(2)
+            tiles = b.tiles()
             b.run(3)
             barrier(world)
             t0 = time.perf_counter()
@@ -597,6 +598,8 @@ def batched(args, local, world=1, rank=0):
     out = {"value": value, "unit": UNIT, "instances": len(all_ws), "particles": N, "n_gpus": world,
            "grid_nodes": sum(w.G for w in all_ws), "steps": K, "ms_per_step": 1e3 * el / K,
            "sor_waves_rank0": waves, "autotuned_sor_block_cap_rank0": cap, "setup_s": setup,
+           "autotuned_particle_block_rank0": tiles[0][3] if tiles else None,
+           "sor_tiles_rank0": {f"{P}x{R}": sum(1 for t in tiles if t[:2] == (P, R)) for P, R, *_ in tiles},
            "sor_iterations_per_step_mean_rank0": float(obs["sor_iterations"].mean()),
            "dipole_series_gathered": len(series)}
     if seq is not None:
@@ -747,7 +750,8 @@ def our_arm(args, world, rank, local):
                 "mean_sor_iterations": float(its_p.mean()),
                 "sor_checks_per_solve": float(np.mean([sor_checks(n, per_cycle) for n in its_p]))}
 
-    # per step: particle step, smoothing, Skyrme, SOR, forces, step counter;
+    # per step: particle step, smoothing, Skyrme, SOR, forces (which also
+    # advances the step counter);
     # the FFT smoothing (power-of-two axes up to 128; by default for stencil
     # half-widths >= 6 nodes, 4 sigma / h) adds its three passes before the
     # march kernel, which then only checks the edge flags
@@ -755,7 +759,7 @@ def our_arm(args, world, rank, local):
     pow2 = all(n & (n - 1) == 0 and 2 <= n <= 128 for n in (w.n, w.n, w.n))
     half_width = int(4.0 * w.sigma_r / w.h)
     fft = pow2 and (opts.smooth_fft == 2 or (opts.smooth_fft == 1 and half_width >= 6))
-    launches_per_step = 6 + (3 if fft else 0)
+    launches_per_step = 5 + (3 if fft else 0)
     chunk = opts.graph_steps or 8
     # slot re-sorts: one every sort_every steps, at the start of a graph
     # chunk; each launches its key kernel and ten gathers of ours (the radix

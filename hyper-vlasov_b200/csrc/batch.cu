@@ -15,7 +15,7 @@
 // How many blocks each instance's solve uses is a plan choice: fewer blocks
 // pack more instances into a wave, more blocks make each solve faster.
 // hv_batch_plan takes a cap; hv_batch_autotune times candidate caps on trial
-// steps and keeps the fastest.
+// steps and keeps the fastest, then the particle step's block size.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -284,11 +284,48 @@ hv_status hv_batch_autotune(hv_batch *b, int trial_steps, int *chosen_cap) {
             best_ms = ms;
         }
     }
+    if (best < 0) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return HV_ERR_UNSUPPORTED;
+    }
+    HV_TRY(hv_batch_plan(b, best));
+    // then the particle step's block size, the same for every instance
+    int best_pb = 0;
+    best_ms = 0.0f;
+    for (int pb : {128, 256, 512}) {
+        for (hv_ctx *c : b->ctx) c->fused.pblock = pb;
+        drop_graph(b);
+        HV_TRY(hv_batch_run(b, 1, nullptr));
+        HV_CUDA(cudaEventRecord(e0, b->stream));
+        HV_TRY(hv_batch_run(b, trial_steps, nullptr));
+        HV_CUDA(cudaEventRecord(e1, b->stream));
+        HV_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        HV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (best_pb == 0 || ms < best_ms) {
+            best_pb = pb;
+            best_ms = ms;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (best < 0) return HV_ERR_UNSUPPORTED;
-    HV_TRY(hv_batch_plan(b, best));
+    for (hv_ctx *c : b->ctx) c->fused.pblock = best_pb;
+    drop_graph(b);
     if (chosen_cap) *chosen_cap = best;
+    return HV_OK;
+}
+
+hv_status hv_batch_tiles(const hv_batch *b, int *sor_planes, int *sor_rows, int *sor_blocks, int *particle_block,
+                         int n) {
+    if (!b || n < 0 || n > (int)b->ctx.size()) return HV_ERR_BAD_ARG;
+    for (int i = 0; i < n; i++) {
+        const hv_ctx *c = b->ctx[i];
+        if (sor_planes) sor_planes[i] = c->fused.sor.P;
+        if (sor_rows) sor_rows[i] = c->fused.sor.R;
+        if (sor_blocks) sor_blocks[i] = c->fused.sor.nblocks;
+        if (particle_block) particle_block[i] = c->fused.pblock;
+    }
     return HV_OK;
 }
 

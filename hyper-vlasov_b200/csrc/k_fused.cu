@@ -364,7 +364,13 @@ __global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__re
 // merge (include/tools.hpp:377-384) folded in, written as (Fx,Fy,Fz,0).
 template <typename T>
 __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U, const double *__restrict__ phi,
-                            T *F4) {
+                            T *F4, int *advance) {
+    // the step's last kernel also advances the step counter (advance: the
+    // control words; null for the initial solve)
+    if (advance && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) {
+        advance[CTL_STEP] += 1;
+        advance[CTL_CLOSE] = 1;
+    }
     // block (j, i, species): one z row, so no division recovers the indices
     const int j = blockIdx.x, ii = blockIdx.y;
     const bool prot = blockIdx.z == 0;
@@ -437,11 +443,6 @@ template <typename T>
 __global__ void k_widen(long long n, const T *__restrict__ in, double *out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (double)in[i];
-}
-
-__global__ void k_advance(int *ctl) {
-    ctl[CTL_STEP] += 1;
-    ctl[CTL_CLOSE] = 1;
 }
 
 // rows[r] = sums over blocks (fixed order) of the ring row of step s0 + r
@@ -583,10 +584,8 @@ hv_status enqueue_phase_c(hv_ctx *c) {
     {
         ProfScope ps(c, HV_K_FORCES);
         k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
-                                                                  reinterpret_cast<T *>(f.F4));
+                                                                  reinterpret_cast<T *>(f.F4), ctl);
     }
-    HV_CUDA(cudaGetLastError());
-    k_advance<<<1, 1, 0, c->stream>>>(ctl);
     HV_CUDA(cudaGetLastError());
     return HV_OK;
 }
@@ -659,7 +658,7 @@ hv_status initial_typed(hv_ctx *c) {
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
     k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
-                                                                       reinterpret_cast<T *>(f.F4));
+                                                                       reinterpret_cast<T *>(f.F4), nullptr);
     HV_CUDA(cudaGetLastError());
     int status[3] = {0, 0, 0};
     HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));

@@ -1597,6 +1597,7 @@ static hv_status plan_for(hv_ctx *c, int max_blocks, int rank = 0) {
     HV_CUDA(cudaMalloc((void **)&f.partials, sizeof(double) * 4 * f.nblocks));
     HV_CUDA(cudaMemsetAsync(f.partials, 0, sizeof(double) * 4 * f.nblocks, c->stream));
     HV_CUDA(cudaMalloc((void **)&f.phase, sizeof(unsigned) * (f.nblocks + 2)));
+    HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
     f.bar = f.phase + f.nblocks;
     HV_CUDA(cudaMalloc((void **)&f.status, sizeof(int) * 8));
     HV_CUDA(cudaMalloc((void **)&f.metric, sizeof(double) * 2));
@@ -1616,8 +1617,13 @@ static hv_status plan_for(hv_ctx *c, int max_blocks, int rank = 0) {
 }
 
 // Clears the error word of the fused solver before a run's solves.
+// Also zeroes the barrier and phase counters: a solve that ended normally
+// leaves the tagged forms' arrival counter at zero, so their steps need no
+// reset of their own, but one that gave up may not.
 hv_status sor_fast_clear_error(hv_ctx *c) {
-    HV_CUDA(cudaMemsetAsync(c->fused.sor.status, 0, sizeof(int), c->stream));
+    const SorFast &f = c->fused.sor;
+    HV_CUDA(cudaMemsetAsync(f.status, 0, sizeof(int) * 4, c->stream));
+    HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
     return HV_OK;
 }
 
@@ -1758,13 +1764,13 @@ static const void *sor_kernel(int form) {
 template <typename T>
 hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, bool step_solve) {
     SorFast &f = c->fused.sor;
-    HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
-    // words 1..3 describe this solve; the error word (0) stays set from an
-    // earlier solve of the run, so that a later solve cannot hide it (and
-    // gives up at its first wait)
-    HV_CUDA(cudaMemsetAsync(f.status + 1, 0, sizeof(int) * 3, c->stream));
     SorArgs<T, T> a;
     const int form = sor_fast_args<T>(c, rho, ctl, its_ring, ring, a);
+    // the phase-counter form counts from zero in every solve; the tagged
+    // forms' barrier counter is back at zero after each completed solve (the
+    // run's start resets it, sor_fast_clear_error).  The error word stays set
+    // from an earlier solve of the run, so that a later one cannot hide it
+    if (form == 0) HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
     if (!step_solve) a.extrapolate = 0;
     void *args[] = {&a};
     HV_CUDA(cudaLaunchCooperativeKernel(sor_kernel<T, false>(form), dim3(f.nblocks), dim3(f.threads), args, f.smem,
@@ -1824,12 +1830,9 @@ hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std:
     return HV_OK;
 }
 
+// The waves run tagged forms only: each instance's barrier counter is back at
+// zero after its solve, and the batch's start resets it (run_begin).
 hv_status sor_wave_launch(const SorWave &w, cudaStream_t st) {
-    for (hv_ctx *c : w.ctx) {
-        const SorFast &f = c->fused.sor;
-        HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), st));
-        HV_CUDA(cudaMemsetAsync(f.status + 1, 0, sizeof(int) * 3, st));
-    }
     SorArgs<float, float> p;
     std::memset(&p, 0, sizeof(p));
     p.batch = reinterpret_cast<const SorArgs<float, float> *>(w.args);

@@ -191,6 +191,7 @@ SIGNATURES = {
     "hv_batch_autotune": (_S, [_P, _I, _P]),
     "hv_batch_run": (_S, [_P, _I, _P]),
     "hv_batch_waves": (_I, [_P]),
+    "hv_batch_tiles": (_S, [_P, _P, _P, _P, _P, _I]),
 }
 
 _lib = None

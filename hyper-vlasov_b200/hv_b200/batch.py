@@ -4,7 +4,8 @@
     sessions = [Session.from_workload(w, HV_F32) for w in batch_workloads(64)]
     for s, w in zip(sessions, ws): s.upload_particles(*workload_particles(w, np.float32))
     with Batch(sessions) as b:
-        b.autotune(2)               # SOR block cap chosen by timing (advances every run)
+        b.autotune(2)               # SOR block cap and particle block size chosen by timing
+                                    # (advances every run)
         obs = b.run(500)            # obs[i] = rows of instance i
 
 Each instance's rows are those of its own Session.run(steps, HV_PATH_FUSED),
@@ -37,6 +38,13 @@ class Batch:
 
     def waves(self):
         return self.lib.hv_batch_waves(self._b)
+
+    def tiles(self):
+        """Per instance: (SOR planes, rows, blocks, particle-step block size)."""
+        n = len(self.sessions)
+        arrs = [np.zeros(n, np.int32) for _ in range(4)]
+        L.check(self.lib.hv_batch_tiles(self._b, *[C.c_void_p(a.ctypes.data) for a in arrs], n), "hv_batch_tiles")
+        return list(zip(*[a.tolist() for a in arrs]))
 
     def run(self, steps):
         obs = np.zeros((len(self.sessions), steps), L.OBS_DTYPE)

@@ -592,7 +592,11 @@ HV_API hv_status hv_adjoint_backward(hv_ctx *ctx, const double *dJ_dD, const dou
  * instance whose grid needs more blocks' shared memory gets twice the cap, and
  * so on) and packs the solves into waves of at most one block per SM.  hv_batch_autotune
  * times trial_steps batched steps (plus one) for each candidate cap and keeps
- * the fastest; the trial steps advance every run.  hv_batch_run advances all
+ * the fastest, then does the same for the particle step's block size (128,
+ * 256 or 512 threads, the same for every instance); the trial steps advance
+ * every run.  hv_batch_tiles reports, for the first n instances, the SOR tile
+ * (planes x rows per block), the blocks of the solve and the particle step's
+ * block size (any pointer may be NULL).  hv_batch_run advances all
  * instances n_steps and writes n_steps observable rows per instance,
  * instance-major (obs[i * n_steps + s]; may be NULL). */
 typedef struct hv_batch hv_batch;
@@ -602,6 +606,8 @@ HV_API hv_status hv_batch_plan(hv_batch *batch, int sor_max_blocks);
 HV_API hv_status hv_batch_autotune(hv_batch *batch, int trial_steps, int *chosen_cap);
 HV_API hv_status hv_batch_run(hv_batch *batch, int n_steps, hv_observables *obs);
 HV_API int hv_batch_waves(const hv_batch *batch);
+HV_API hv_status hv_batch_tiles(const hv_batch *batch, int *sor_planes, int *sor_rows, int *sor_blocks,
+                                int *particle_block, int n);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,10 @@ def test_batch_autotune_and_continued_runs(hv):
         with Batch(sess) as b:
             cap = b.autotune(2)
             assert cap in (0, 64, 32, 16, 8, 4)
+            tiles = b.tiles()
+            assert len(tiles) == len(ws)
+            assert all(P >= 1 and R >= 1 and nb >= 1 and pb in (128, 256, 512) for P, R, nb, pb in tiles)
+            assert len({pb for *_, pb in tiles}) == 1  # one particle block size for all
             o1 = b.run(8)
             o2 = b.run(9)
     finally:
