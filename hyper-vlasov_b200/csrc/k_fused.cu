@@ -32,6 +32,7 @@ namespace {
 constexpr int kPBlock = 256;      // default threads per block of the particle step
 constexpr int kPBlockMax = 512;   // largest of the autotuner's candidates
 constexpr int kPGridMax = 8;      // most blocks per SM of the particle step
+constexpr int kForceRows = 8;     // y rows per thread of the forces kernel
 constexpr int kRing = 64;  // observable rows kept on the device
 
 // control words (Fused::ctl)
@@ -348,15 +349,42 @@ __global__ void k_close_kick(Geom g, int protons, int total, const T *__restrict
 
 // Skyrme potential (include/physics.hpp:272-281, physics_formulas.hpp:70-77).
 template <typename T>
-__global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__restrict__ rho, T *U) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= G) return;
-    const T rp = rho[i], rn = rho[i + G];
+__device__ __forceinline__ void skyrme_node(T A, T B, T C, T gamma, T rp, T rn, T &up, T &un) {
     const T t = (rp + rn) / T(0.16);
     const T base = A * t + B * pow(t, gamma);
     const T iso = T(2.0) * C * ((rn - rp) / T(0.16));
-    U[i] = base - iso;
-    U[i + G] = base + iso;
+    up = base - iso;
+    un = base + iso;
+}
+
+template <typename T>
+__global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__restrict__ rho, T *U) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if constexpr (sizeof(T) == 4) {
+        // four nodes per thread with 16-byte loads and stores (G a multiple
+        // of 4): enough bytes in flight per thread for the memory system
+        if ((G & 3) == 0) {
+            if (4 * i >= G) return;
+            const float4 p = __ldg(reinterpret_cast<const float4 *>(rho) + i);
+            const float4 n = __ldg(reinterpret_cast<const float4 *>(rho + G) + i);
+            float4 up, un;
+            skyrme_node<T>(A, B, C, gamma, p.x, n.x, up.x, un.x);
+            skyrme_node<T>(A, B, C, gamma, p.y, n.y, up.y, un.y);
+            skyrme_node<T>(A, B, C, gamma, p.z, n.z, up.z, un.z);
+            skyrme_node<T>(A, B, C, gamma, p.w, n.w, up.w, un.w);
+            reinterpret_cast<float4 *>(U)[i] = up;
+            reinterpret_cast<float4 *>(U + G)[i] = un;
+            return;
+        }
+    }
+    if (i >= G) return;
+    skyrme_node<T>(A, B, C, gamma, rho[i], rho[i + G], U[i], U[i + G]);
+}
+
+// threads of k_skyrme_fast: one per node, or one per four in float
+template <typename T>
+inline long long skyrme_threads(long long G) {
+    return (sizeof(T) == 4 && (G & 3) == 0) ? G / 4 : G;
 }
 
 // -grad(U + phi_p) with the reference's one-sided faces
@@ -371,42 +399,53 @@ __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U
         advance[CTL_STEP] += 1;
         advance[CTL_CLOSE] = 1;
     }
-    // block (j, i, species): one z row, so no division recovers the indices
-    const int j = blockIdx.x, ii = blockIdx.y;
+    // block (row group, x plane, species), threads along z: each thread walks
+    // kForceRows consecutive y rows at its z, keeping the y-1, y and y+1
+    // values of U + phi in registers, so a node loads five values, not seven
+    const int ii = blockIdx.y;
     const bool prot = blockIdx.z == 0;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long sx = (long long)ny * nz, sy = nz;
     const T *Us = U + (prot ? 0 : g.G);
-    const long long row = (long long)ii * sx + (long long)j * sy;
     auto u = [&](long long q) { return prot ? Us[q] + (T)phi[q] : Us[q]; };
+    const int j0 = blockIdx.x * kForceRows, j1 = min(j0 + kForceRows, ny);
     for (int k = threadIdx.x; k < nz; k += blockDim.x) {
-        const long long id = row + k;
-        const T uc = u(id);
-        T gx, gy, gz;
-        if (ii == 0) gx = (u(id + sx) - uc) * idx;
-        else if (ii == nx - 1) gx = (uc - u(id - sx)) * idx;
-        else gx = (u(id + sx) - u(id - sx)) * (T(0.5) * idx);
-        if (j == 0) gy = (u(id + sy) - uc) * idy;
-        else if (j == ny - 1) gy = (uc - u(id - sy)) * idy;
-        else gy = (u(id + sy) - u(id - sy)) * (T(0.5) * idy);
-        if (k == 0) gz = (u(id + 1) - uc) * idz;
-        else if (k == nz - 1) gz = (uc - u(id - 1)) * idz;
-        else gz = (u(id + 1) - u(id - 1)) * (T(0.5) * idz);
-        const long long i = (prot ? 0 : g.G) + id;
-        if constexpr (sizeof(T) == 4) {
-            reinterpret_cast<float4 *>(F4)[i] = make_float4(-gx, -gy, -gz, 0.0f);
-        } else {
-            T *o = F4 + 4 * i;
-            o[0] = -gx;
-            o[1] = -gy;
-            o[2] = -gz;
-            o[3] = T(0);
+        long long id = (long long)ii * sx + (long long)j0 * sy + k;
+        T um = j0 > 0 ? u(id - sy) : T(0);
+        T uc = u(id);
+        for (int j = j0; j < j1; j++, id += sy) {
+            const T up = j + 1 < ny ? u(id + sy) : T(0);
+            T gx, gy, gz;
+            if (ii == 0) gx = (u(id + sx) - uc) * idx;
+            else if (ii == nx - 1) gx = (uc - u(id - sx)) * idx;
+            else gx = (u(id + sx) - u(id - sx)) * (T(0.5) * idx);
+            if (j == 0) gy = (up - uc) * idy;
+            else if (j == ny - 1) gy = (uc - um) * idy;
+            else gy = (up - um) * (T(0.5) * idy);
+            if (k == 0) gz = (u(id + 1) - uc) * idz;
+            else if (k == nz - 1) gz = (uc - u(id - 1)) * idz;
+            else gz = (u(id + 1) - u(id - 1)) * (T(0.5) * idz);
+            const long long i = (prot ? 0 : g.G) + id;
+            if constexpr (sizeof(T) == 4) {
+                reinterpret_cast<float4 *>(F4)[i] = make_float4(-gx, -gy, -gz, 0.0f);
+            } else {
+                T *o = F4 + 4 * i;
+                o[0] = -gx;
+                o[1] = -gy;
+                o[2] = -gz;
+                o[3] = T(0);
+            }
+            um = uc;
+            uc = up;
         }
     }
 }
 
-// k_forces_f4's launch: one block per (y row, x plane, species), threads along z
-inline dim3 forces_grid(const Geom &g) { return dim3((unsigned)g.ny, (unsigned)g.nx, 2u); }
+// k_forces_f4's launch: one block per (group of kForceRows y rows, x plane,
+// species), threads along z
+inline dim3 forces_grid(const Geom &g) {
+    return dim3((unsigned)((g.ny + kForceRows - 1) / kForceRows), (unsigned)g.nx, 2u);
+}
 inline dim3 forces_block(const Geom &g) { return dim3((unsigned)std::min(128, (g.nz + 31) / 32 * 32)); }
 
 template <typename T>
@@ -566,8 +605,8 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     const hv_skyrme &sk = p.skyrme;
     {
         ProfScope ps(c, HV_K_SKYRME);
-        k_skyrme_fast<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C), T(sk.gamma), s.rho,
-                                                                s.U);
+        k_skyrme_fast<T><<<nblk(skyrme_threads<T>(g.G), 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C),
+                                                                                   T(sk.gamma), s.rho, s.U);
     }
     HV_CUDA(cudaGetLastError());
     return HV_OK;
@@ -638,7 +677,8 @@ hv_status initial_typed(hv_ctx *c) {
     else
         HV_TRY(launch_smooth<T>(c, s.rho_raw, s.rho));
     const hv_skyrme &sk = p.skyrme;
-    k_skyrme_fast<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C), T(sk.gamma), s.rho, s.U);
+    k_skyrme_fast<T><<<nblk(skyrme_threads<T>(g.G), 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C),
+                                                                               T(sk.gamma), s.rho, s.U);
     HV_CUDA(cudaGetLastError());
     if (!c->boundary_set) {
         HV_CUDA(cudaMemsetAsync(f.phi64, 0, sizeof(double) * g.G, c->stream));
