@@ -680,13 +680,17 @@ hv_status initial_typed(hv_ctx *c) {
     k_skyrme_fast<T><<<nblk(skyrme_threads<T>(g.G), 256), 256, 0, c->stream>>>(g.G, T(sk.A), T(sk.B), T(sk.C),
                                                                                T(sk.gamma), s.rho, s.U);
     HV_CUDA(cudaGetLastError());
+    // the boundary counts as set only once the solve has succeeded: a solve
+    // that gave up leaves phi64 unfinished and the plain phi without the
+    // monopole boundary, so the next attempt must start from the boundary again
+    bool set_boundary = false;
     if (!c->boundary_set) {
         HV_CUDA(cudaMemsetAsync(f.phi64, 0, sizeof(double) * g.G, c->stream));
         HV_TRY(launch_boundary<double>(c, f.phi64));
         const double R = 1.2 * std::cbrt((double)(c->params.z + c->params.n));
         k_sphere_guess<<<dim3((unsigned)g.ny, (unsigned)g.nx), 128, 0, c->stream>>>(g, c->params.z, R, f.phi64);
         HV_CUDA(cudaGetLastError());
-        c->boundary_set = true;
+        set_boundary = true;
     } else {
         k_widen<T><<<nblk(g.G, 256), 256, 0, c->stream>>>(g.G, s.phi, f.phi64);
     }
@@ -707,6 +711,7 @@ hv_status initial_typed(hv_ctx *c) {
         set_last_error("SOR: a bounded device-side wait timed out");
         return HV_ERR_TIMEOUT;
     }
+    if (set_boundary) c->boundary_set = true;
     // f of the initial positions; the plain buffers get the same fields
     if (c->total > 0)
         k_close_kick<T><<<nblk(c->total, 256), 256, 0, c->stream>>>(g, c->protons, c->total, s.x, s.y, s.z, s.kx, s.ky,
@@ -778,6 +783,10 @@ hv_status run_rows(hv_ctx *c, int s0, int k, hv_observables *obs) {
     HV_CUDA(cudaStreamSynchronize(c->stream));
     prof_collect(c);
     if (status[0]) {
+        // the steps ran on an unfinished potential: the next run solves the
+        // fields of the current positions again
+        c->fields_valid = false;
+        fused_invalidate(c);
         set_last_error("SOR: a bounded device-side wait timed out");
         return HV_ERR_TIMEOUT;
     }

@@ -5,7 +5,8 @@ grids 32^3..96^3 at h = 0.5 fm, jittered Skyrme parameters and boosts), with
 at most 100 test particles per nucleon to keep the test short.  Tolerance:
 D(t) of every instance within 1e-4 of its largest |D| against the instance's
 own fused run (the float atomic deposit makes two runs of one instance differ
-at ~1e-6), SOR iteration counts within one residual check (256)."""
+at ~1e-6); with the instances' own plans, SOR iteration counts within one
+residual check (256)."""
 from __future__ import annotations
 
 from dataclasses import replace
@@ -52,7 +53,10 @@ def test_batch_matches_individual_runs(hv, cap):
         d = np.abs(a["dipole"]).max()
         assert d > 0
         assert np.max(np.abs(obs[i]["dipole"] - a["dipole"])) <= 1e-4 * d, ws[i].name
-        assert np.all(np.abs(obs[i]["sor_iterations"] - a["sor_iterations"]) <= 256)
+        if cap == 0:
+            # the instances' own plans: the same solver as their lone runs (a
+            # cap can force the generic sweep, whose plain cycles take more)
+            assert np.all(np.abs(obs[i]["sor_iterations"] - a["sor_iterations"]) <= 256)
         assert not np.any(obs[i]["flags"] & 1)
         assert np.allclose(obs[i]["t"], a["t"])
 

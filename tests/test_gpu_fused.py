@@ -475,8 +475,9 @@ def test_coarse_grid_correction_keeps_the_stopping_rule(hv, wname, n):
     every solve at the same FP64 stopping rule as plain SOR cycles: D(t) and
     the Coulomb potential agree within 1e-6 relative (the tolerance of each
     solve), the particles to float rounding, and the iterations per step fall
-    well below the plain cycles' (coarse factors 8, 4, 2 and a non-cubic grid,
-    8 on each axis)."""
+    below the plain cycles' -- to under 0.6 of them on the cubic grids of 64
+    nodes and more (coarse factors 8, 4, 2, and a non-cubic grid with 8 on
+    each axis, whose coarse grid has only 3 interior nodes along y)."""
     w = hv.WORKLOADS[wname]
     world = _world(n, w.h)
     p = hv.workload_particles(w, np.float32)
@@ -494,7 +495,8 @@ def test_coarse_grid_correction_keeps_the_stopping_rule(hv, wname, n):
     assert max_rel(c1, c0) < 1e-6, max_rel(c1, c0)
     assert all(np.max(np.abs(a - b)) < 1e-4 for a, b in zip(p0, p1))
     its0, its1 = o0["sor_iterations"][2:].mean(), o1["sor_iterations"][2:].mean()
-    if n[0] >= 64:
+    assert its1 < its0, (its1, its0)
+    if n[0] == n[1] == n[2] and n[0] >= 64:
         assert its1 < 0.6 * its0, (its1, its0)
 
 
