@@ -348,13 +348,28 @@ __global__ void k_close_kick(Geom g, int protons, int total, const T *__restrict
 }
 
 // Skyrme potential (include/physics.hpp:272-281, physics_formulas.hpp:70-77).
+// In float, t^gamma is CUDA's fast power intrinsic (exp2 of gamma log2 t on
+// the special-function units) and the divisions by rho0 are products by its
+// reciprocal: the accurate pow and two divisions made this kernel compute-
+// bound (58 % SM, 11 % DRAM in ncu).  The results move by float rounding;
+// the FP32 form's accuracy is checked on D(t).  The double form (the fused
+// FP64 path) keeps pow and the divisions.
 template <typename T>
 __device__ __forceinline__ void skyrme_node(T A, T B, T C, T gamma, T rp, T rn, T &up, T &un) {
-    const T t = (rp + rn) / T(0.16);
-    const T base = A * t + B * pow(t, gamma);
-    const T iso = T(2.0) * C * ((rn - rp) / T(0.16));
-    up = base - iso;
-    un = base + iso;
+    if constexpr (sizeof(T) == 4) {
+        const float inv_rho0 = 1.0f / 0.16f;
+        const float t = (rp + rn) * inv_rho0;
+        const float base = A * t + B * __powf(t, gamma);
+        const float iso = 2.0f * C * ((rn - rp) * inv_rho0);
+        up = base - iso;
+        un = base + iso;
+    } else {
+        const T t = (rp + rn) / T(0.16);
+        const T base = A * t + B * pow(t, gamma);
+        const T iso = T(2.0) * C * ((rn - rp) / T(0.16));
+        up = base - iso;
+        un = base + iso;
+    }
 }
 
 template <typename T>

@@ -88,7 +88,7 @@ struct SorArgs {
     // coarse-grid correction (staged float form): coarsening factor F, interior
     // extents of the coarse grid (its nodes sit at every F-th fine node, with
     // zero corrections at 0 and n / F), red+black iterations per cycle, and
-    // the two restriction stages' buffers t1 [nx][ny][cmz], t2 [nx][cmy][cmz]
+    // the restriction's buffers t1 [nx][ny][cmz] and t2 [cmx][cmy][cmz]
     int coarse, cf, cmx, cmy, cmz, csweeps;
     float *t1, *t2;
     double hx, hy, hz;      // fine grid spacings
@@ -730,8 +730,9 @@ __device__ __forceinline__ void sweep_scalar(const SorArgs<T, S> &a, const Block
 // (S_jk = sin(pi (j+1)(k+1) / (m+1)), S S = (m+1)/2 I), redundantly in every
 // block's shared memory, so that no block waits for another to solve it.
 // Restriction is separable: stage 1 filters each block's own z rows (its
-// residual source is in shared memory), stage 2 the y direction (all blocks,
-// after a grid barrier), stage 3 the x direction (every block, after another).
+// residual source is in shared memory); after a grid barrier, all blocks
+// share the y and x filters of the interior coarse nodes; after another,
+// every block reads the restricted residual.
 constexpr int kCoarseMax = 15;
 
 struct Coarse {
@@ -801,23 +802,47 @@ __device__ void coarse_stage1(const SorArgs<T, S> &a, const Block &B, const S *s
     }
 }
 
-// Stage 2 (every block's share of the outputs): the filter along y, into t2.
+// Stages 2 and 3 (every block's share of the outputs): the filters along y
+// and x of t1 at each interior coarse node, into t2[I][J][K].  A group of
+// lanes (the power of two covering the 2F - 1 taps) shares a node: lane l
+// sums its tap x = F (I + 1) + l - (F - 1) over the 2F - 1 y taps with all
+// loads issued together, and the group adds its lanes with shuffles.
 template <typename T, typename S>
-__device__ void coarse_stage2(const SorArgs<T, S> &a, int b) {
-    const int F = a.cf, my = a.cmy, mz = a.cmz, ny = a.ny;
-    const float w0 = 1.0f / (float)(F * F);
-    const long long total = (long long)(a.nx - 2) * my * mz;
-    const long long stride = (long long)a.nblocks * blockDim.x;
-    for (long long o = (long long)b * blockDim.x + threadIdx.x; o < total; o += stride) {
-        const int K = (int)(o % mz), J = (int)((o / mz) % my), x = 1 + (int)(o / ((long long)my * mz));
-        const int yc = F * (J + 1);
+__device__ void coarse_stage23(const SorArgs<T, S> &a, int b) {
+    const int F = a.cf, my = a.cmy, mz = a.cmz, nx = a.nx, ny = a.ny, taps = 2 * F - 1;
+    int lanes = 1;
+    while (lanes < taps) lanes <<= 1;
+    const int M = a.cmx * my * mz;
+    const float w0 = 1.0f / ((float)F * F * F * F);
+    const int lane = threadIdx.x & 31, sub = lane & (lanes - 1);
+    const long long groups_per_warp = 32 / lanes;
+    const long long gw = ((long long)b * blockDim.x + threadIdx.x) / 32;  // this warp's index
+    const long long warps = (long long)a.nblocks * (blockDim.x / 32);
+    for (long long g0 = gw * groups_per_warp; g0 < M; g0 += warps * groups_per_warp) {
+        const long long o = g0 + lane / lanes;  // this lane's coarse node
         float acc = 0.0f;
-        for (int d = 1 - F; d < F; d++) {
-            const int y = yc + d;
-            if (y < 1 || y > ny - 2) continue;
-            acc = fmaf((float)(F - abs(d)), __ldcg(a.t1 + ((long long)x * ny + y) * mz + K), acc);
+        if (o < M && sub < taps) {
+            const int K = (int)(o % mz), J = (int)((o / mz) % my), I = (int)(o / ((long long)my * mz));
+            const int dx = sub - (F - 1), x = F * (I + 1) + dx;
+            if (x >= 1 && x <= nx - 2) {
+                const int yc = F * (J + 1);
+                const float *col = a.t1 + (long long)x * ny * mz + K;
+                // eight taps' loads at a time, issued before their sums
+                for (int q0 = 0; q0 < taps; q0 += 8) {
+                    float v[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int y = yc + q0 + q - (F - 1);
+                        v[q] = (q0 + q < taps && y >= 1 && y <= ny - 2) ? __ldcg(col + (long long)y * mz) : 0.0f;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 8; q++) acc = fmaf((float)max(F - abs(q0 + q - (F - 1)), 0), v[q], acc);
+                }
+                acc *= (float)(F - abs(dx));
+            }
         }
-        __stcg(a.t2 + ((long long)x * my + J) * mz + K, acc * w0);
+        for (int off = lanes / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (sub == 0 && o < M) __stcg(a.t2 + o, acc * w0);
     }
 }
 
@@ -847,24 +872,14 @@ __device__ __forceinline__ void dst_pass(const float *in, float *out, const floa
     }
 }
 
-// Stage 3 and the coarse solve: the filter along x of t2 (every block reads
-// all of it), scaled back from the pre-scaled residual to r, then
+// The coarse solve: the restricted residual (t2, every block reads all of
+// it), scaled back from the pre-scaled residual to r, then
 // e = S_x S_y S_z (-(S_x S_y S_z R r) / (lam_x + lam_y + lam_z)) 8 / ((mx+1)(my+1)(mz+1)).
 template <typename T, typename S>
 __device__ void coarse_solve(const SorArgs<T, S> &a, const Coarse &cs) {
-    const int F = a.cf, mx = a.cmx, my = a.cmy, mz = a.cmz, M = mx * my * mz;
-    const float w0 = (float)(1.0 / ((double)F * F * a.src_scale));
-    for (int o = threadIdx.x; o < M; o += blockDim.x) {
-        const int K = o % mz, J = (o / mz) % my, I = o / (my * mz);
-        const int xc = F * (I + 1);
-        float acc = 0.0f;
-        for (int d = 1 - F; d < F; d++) {
-            const int x = xc + d;
-            if (x < 1 || x > a.nx - 2) continue;
-            acc = fmaf((float)(F - abs(d)), __ldcg(a.t2 + ((long long)x * my + J) * mz + K), acc);
-        }
-        cs.ec[o] = acc * w0;
-    }
+    const int mx = a.cmx, my = a.cmy, mz = a.cmz, M = mx * my * mz;
+    const float w0 = (float)(1.0 / a.src_scale);
+    for (int o = threadIdx.x; o < M; o += blockDim.x) cs.ec[o] = __ldcg(a.t2 + o) * w0;
     __syncthreads();
     dst_pass(cs.ec, cs.tmp, cs.sz, mz, 2, mx, my, mz);
     __syncthreads();
@@ -1377,7 +1392,7 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
             if (a.coarse) {
                 // restriction stages 2 and 3, the coarse solve and its
                 // prolongation, which the sweeps below start from
-                coarse_stage2(a, b);
+                coarse_stage23(a, b);
                 if (!grid_barrier(a.bar, a.nblocks, err, a.max_spin)) return;
                 coarse_solve(a, cs);
                 coarse_prolong<T>(a, B, cs, sd, st.gbuf, st.gsrc, ng_rows);
@@ -1488,7 +1503,10 @@ static hv_status plan_for(hv_ctx *c, int max_blocks, int rank = 0) {
     // factor F that divides every axis and leaves at most kCoarseMax interior
     // coarse nodes per axis (at least one)
     int cf = 0, cm[3] = {0, 0, 0};
-    if (sizeof(S) == 4) {
+    // grids of fewer nodes converge in a few dozen plain iterations, less than
+    // the correction's fixed cost per cycle repays
+    const long long coarse_min_nodes = 48ll * 48 * 48;
+    if (sizeof(S) == 4 && g.G >= coarse_min_nodes) {
         const int n3[3] = {g.nx, g.ny, g.nz};
         for (int F = 2; F <= 256 && !cf; F *= 2) {
             bool ok = true;

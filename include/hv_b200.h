@@ -342,9 +342,10 @@ typedef struct hv_fast_options {
                              solve starts its correction from the correction
                              equation solved exactly on a coarse grid (every
                              F-th node, F the smallest power of two leaving at
-                             most 15 interior coarse nodes per axis; grids
-                             whose axes F does not divide, double solves, the
-                             max-update rule and batched runs go without), and
+                             most 15 interior coarse nodes per axis; grids of
+                             fewer than 48^3 nodes or whose axes F does not
+                             divide, double solves, the max-update rule and
+                             batched waves of generic sweeps go without), and
                              runs sor_coarse_sweeps red+black iterations after
                              it; 0: plain SOR cycles.  The stopping rule is
                              unchanged, so only the iterations per solve
