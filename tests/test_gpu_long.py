@@ -10,13 +10,16 @@ The test-particle dynamics amplify any rounding difference by about ten
 every 250 steps: two FP64 runs that differ only in the order of the atomic
 deposit's additions go from 1e-16 to 2e-10 over the 2000 steps, and the FP32
 run's difference, starting from float rounding, passes 1e-3 of max|D| near
-step 1500 and ends near 5e-3 (the same growth from plain SOR cycles and
-per-particle atomics).  So the test asserts what holds: the strength function
-S(E) of the whole series (detrended, cos^2-windowed FFT, the reference's
-post-processing, scripts/programs.py:82-122) within 1e-3 of the FP64 run's
-largest value; D(t) within 1e-3 over the first 1400 steps and within 1e-2
-over all 2000; and an FP64 run with the atomic deposit within 1e-8 of the
-sorted one over all 2000 (the growth is the dynamics', not the FP32 form's).
+step 1500 and ends between 5e-3 and 1.2e-2, depending on the atomic
+deposit's summation order (the same growth from plain SOR cycles and
+per-particle atomics).  Both runs here use the deterministic sort-by-cell
+deposit, so the comparison measures the FP32 form alone and repeats exactly.
+The test asserts what holds: the strength function S(E) of the whole series
+(detrended, cos^2-windowed FFT, the reference's post-processing,
+scripts/programs.py:82-122) within 1e-3 of the FP64 run's largest value;
+D(t) within 1e-3 over the first 1400 steps and within 1e-2 over all 2000;
+and an FP64 run with the atomic deposit within 1e-8 of the sorted one over
+all 2000 (the growth is the dynamics', not the FP32 form's).
 The plain FP64 path itself is pinned over 200 steps of the same workload to
 the double oracle (the C restatement of the reference), D(t) within 1e-7.
 """
@@ -48,7 +51,7 @@ def test_fp32_fused_tracks_fp64_over_2000_steps_of_208pb_104k(hv):
     p64 = [p.astype(np.float64) for p in p32]
     obs64 = _plain_f64(hv, replace(w, deposit_mode=hv.HV_DEPOSIT_SORTED), steps, p64)
     obs64a = _plain_f64(hv, w, steps, p64)
-    with hv.Session.from_workload(w, hv.HV_F32) as s:
+    with hv.Session.from_workload(replace(w, deposit_mode=hv.HV_DEPOSIT_SORTED), hv.HV_F32) as s:
         s.upload_particles(*p32)
         s.initial_solve()
         obs32 = s.run(steps, hv.HV_PATH_FUSED)
