@@ -780,25 +780,30 @@ __device__ void coarse_tables(const SorArgs<T, S> &a, const Coarse &cs) {
 }
 
 // Stage 1: the triangle filter along z of the block's own rows of the
-// pre-scaled residual (shared memory), at the coarse z nodes, into t1.
+// pre-scaled residual (shared memory), at the coarse z nodes, into t1.  A
+// half-warp takes a row (no index division per element), lane K its coarse
+// node.
 template <typename T, typename S>
 __device__ void coarse_stage1(const SorArgs<T, S> &a, const Block &B, const S *ss) {
     const int F = a.cf, mz = a.cmz, nz2 = a.nz2, nz = a.nz, ny = a.ny;
     const float w0 = 1.0f / (float)(F * F);
-    for (int o = threadIdx.x; o < B.np * B.nr * mz; o += blockDim.x) {
-        const int K = o % mz, l = o / mz, p = l / B.nr, j = l - p * B.nr;
-        const int x = B.x0 + p, y = B.y0 + j;
+    const int lane = threadIdx.x & 15, half = threadIdx.x >> 4, halves = blockDim.x >> 4;
+    const int rows = B.np * B.nr;
+    for (int r = half; r < rows; r += halves) {
+        const int p = r / B.nr, j = r - p * B.nr, x = B.x0 + p, y = B.y0 + j;
+        if (lane >= mz) continue;
         float acc = 0.0f;
         if (y >= 1 && y <= ny - 2) {
-            const int kc = F * (K + 1);
+            const int kc = F * (lane + 1);
+            const S *row0 = ss + ((p * 2) * B.nr + j) * nz2, *row1 = row0 + B.nr * nz2;
             for (int d = 1 - F; d < F; d++) {
                 const int k = kc + d;
                 if (k < 1 || k > nz - 2) continue;
-                const int c0 = (x + y + k) & 1;
-                acc = fmaf((float)(F - abs(d)), (float)ss[((p * 2 + c0) * B.nr + j) * nz2 + (k >> 1)], acc);
+                const S *row = ((x + y + k) & 1) ? row1 : row0;
+                acc = fmaf((float)(F - abs(d)), (float)row[k >> 1], acc);
             }
         }
-        __stcg(a.t1 + ((long long)x * ny + y) * mz + K, acc * w0);
+        __stcg(a.t1 + ((long long)x * ny + y) * mz + lane, acc * w0);
     }
 }
 
@@ -846,29 +851,28 @@ __device__ void coarse_stage23(const SorArgs<T, S> &a, int b) {
     }
 }
 
-// out = S applied along one axis of in ([mx][my][mz], z fastest): thread
-// (k, g) keeps row k of S in registers and produces element k of lines g,
-// g + G, ...
+// out = S applied along one axis of in ([mx][my][mz], z fastest).  A
+// half-warp takes a line: lane k keeps row k of S in registers and produces
+// element k, every lane reading the same input element at a time (a shared-
+// memory broadcast), so a line costs m loads and m multiply-adds per lane.
 __device__ __forceinline__ void dst_pass(const float *in, float *out, const float *Sm, int m, int axis, int mx, int my,
                                          int mz) {
-    const int G = blockDim.x / m, t = threadIdx.x;
-    if (t >= G * m) return;
-    const int k = t % m, g = t / m;
+    const int k = threadIdx.x & 15, half = threadIdx.x >> 4, halves = blockDim.x >> 4;
     float srow[kCoarseMax];
 #pragma unroll
-    for (int j = 0; j < kCoarseMax; j++) srow[j] = j < m ? Sm[k * m + j] : 0.0f;
-    const int L = mx * my * mz / m;
+    for (int j = 0; j < kCoarseMax; j++) srow[j] = (k < m && j < m) ? Sm[k * m + j] : 0.0f;
     const int stride = axis == 2 ? 1 : axis == 1 ? mz : my * mz;
-    for (int line = g; line < L; line += G) {
+    const int L = axis == 2 ? mx * my : axis == 1 ? mx * mz : my * mz;
+    for (int line = half; line < L; line += halves) {
         int base;
         if (axis == 2) base = line * mz;
-        else if (axis == 1) base = (line / mz) * my * mz + line % mz;
+        else if (axis == 1) base = (line / mz) * (my * mz) + line % mz;
         else base = line;
         float acc = 0.0f;
 #pragma unroll
         for (int j = 0; j < kCoarseMax; j++)
             if (j < m) acc = fmaf(srow[j], in[base + j * stride], acc);
-        out[base + k * stride] = acc;
+        if (k < m) out[base + k * stride] = acc;
     }
 }
 
@@ -911,55 +915,65 @@ __device__ __forceinline__ float coarse_at(const Coarse &cs, int mx, int my, int
 // correction (both colours, every node; zero on the Dirichlet rows and
 // z ends) and into the ghost buffer (the other blocks' black values across
 // the block's faces, read by the cycle's first red sweep).  Separable: the
-// (x, y) interpolation of each row's coarse z profile first, then z.
+// (x, y) interpolation of each row's coarse z profile first (a warp per row,
+// a lane per coarse z node), then z (a warp per row and colour, lanes along
+// the half-row; F is a power of two, so no division per node).
 template <typename T>
 __device__ void coarse_prolong(const SorArgs<T, float> &a, const Block &B, const Coarse &cs, float *sd, float *gbuf,
                                const unsigned *gsrc, int ng) {
     const int F = a.cf, mx = a.cmx, my = a.cmy, mz = a.cmz, ny = a.ny, nz = a.nz, nz2 = a.nz2;
     const int own_rows = B.np * B.nr, rows = own_rows + ng, pw = mz + 2;
+    const int lf = __ffs(F) - 1;
     const float inv = 1.0f / (float)F;
-    for (int o = threadIdx.x; o < rows * pw; o += blockDim.x) {
-        const int r = o / pw, Kp = o - r * pw;
-        int x, y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    auto row_xy = [&](int r, int &x, int &y) {
         if (r < own_rows) {
-            x = B.x0 + r / B.nr;
-            y = B.y0 + r % B.nr;
+            const int p = r / B.nr;
+            x = B.x0 + p;
+            y = B.y0 + (r - p * B.nr);
         } else {
             const unsigned g = gsrc[r - own_rows];
             y = (int)((g / (unsigned)nz2) % (unsigned)ny);
             x = (int)(g / (unsigned)(2 * ny * nz2));
         }
+    };
+    for (int r = warp; r < rows; r += warps) {
+        int x, y;
+        row_xy(r, x, y);
+        if (lane >= pw) continue;
         float v = 0.0f;
         if (y >= 1 && y <= ny - 2) {
-            const int I = x / F, J = y / F;
-            const float tx = (float)(x - I * F) * inv, ty = (float)(y - J * F) * inv;
+            const int I = x >> lf, J = y >> lf, Kp = lane;
+            const float tx = (float)(x & (F - 1)) * inv, ty = (float)(y & (F - 1)) * inv;
             v = (1.0f - tx) * ((1.0f - ty) * coarse_at(cs, mx, my, mz, I, J, Kp) +
                                ty * coarse_at(cs, mx, my, mz, I, J + 1, Kp)) +
                 tx * ((1.0f - ty) * coarse_at(cs, mx, my, mz, I + 1, J, Kp) +
                       ty * coarse_at(cs, mx, my, mz, I + 1, J + 1, Kp));
         }
-        cs.prof[o] = v;
+        cs.prof[r * pw + lane] = v;
     }
     __syncthreads();
-    auto zval = [&](int r, int k) -> float {
+    // z: value at node k of row r
+    auto zval = [&](const float *pr, int k) -> float {
         if (k < 1 || k > nz - 2) return 0.0f;
-        const int K = k / F;
-        const float t = (float)(k - K * F) * inv;
-        const float *pr = cs.prof + r * pw;
+        const int K = k >> lf;
+        const float t = (float)(k & (F - 1)) * inv;
         return (1.0f - t) * pr[K] + t * pr[K + 1];
     };
-    for (int o = threadIdx.x; o < own_rows * 2 * nz2; o += blockDim.x) {
-        const int kh = o % nz2, rc = o / nz2, c = rc & 1, r = rc >> 1;
+    for (int task = warp; task < own_rows * 2; task += warps) {
+        const int r = task >> 1, c = task & 1;
         const int p = r / B.nr, j = r - p * B.nr, x = B.x0 + p, y = B.y0 + j;
-        const int k = ((c - x - y) & 1) + 2 * kh;
-        sd[((p * 2 + c) * B.nr + j) * nz2 + kh] = zval(r, k);
+        const int kc = (c - x - y) & 1;
+        const float *pr = cs.prof + r * pw;
+        float *row = sd + ((p * 2 + c) * B.nr + j) * nz2;
+        for (int kh = lane; kh < nz2; kh += 32) row[kh] = zval(pr, kc + 2 * kh);
     }
-    for (int o = threadIdx.x; o < ng * nz2; o += blockDim.x) {
-        const int kh = o % nz2, g = o / nz2;
-        const unsigned gs = gsrc[g];
-        const int y = (int)((gs / (unsigned)nz2) % (unsigned)ny), x = (int)(gs / (unsigned)(2 * ny * nz2));
-        const int k = ((1 - x - y) & 1) + 2 * kh;
-        gbuf[g * nz2 + kh] = zval(own_rows + g, k);
+    for (int g = warp; g < ng; g += warps) {
+        int x, y;
+        row_xy(own_rows + g, x, y);
+        const int kc = (1 - x - y) & 1;
+        const float *pr = cs.prof + (own_rows + g) * pw;
+        for (int kh = lane; kh < nz2; kh += 32) gbuf[g * nz2 + kh] = zval(pr, kc + 2 * kh);
     }
     __syncthreads();
 }
