@@ -740,9 +740,10 @@ struct Coarse {
     float *sx, *sy, *sz;   // sine matrices [m][m]
     float *lam;            // [mx + my + mz] eigenvalues of the 1-D coarse operators
     float *prof;           // [rows][mz + 2] z-profiles of own and ghost rows
+    float *den;            // [mx][my][mz]: -8 / ((mx+1)(my+1)(mz+1) (lam_x + lam_y + lam_z)) per mode
     __host__ __device__ static size_t bytes(int mx, int my, int mz, int rows) {
         const size_t M = (size_t)mx * my * mz;
-        return 4 * (2 * M + (size_t)mx * mx + (size_t)my * my + (size_t)mz * mz + mx + my + mz +
+        return 4 * (3 * M + (size_t)mx * mx + (size_t)my * my + (size_t)mz * mz + mx + my + mz +
                     (size_t)rows * (mz + 2)) + 64;
     }
     __device__ Coarse(void *base, int mx, int my, int mz) {
@@ -755,7 +756,10 @@ struct Coarse {
         sz = sy + my * my;
         lam = sz + mz * mz;
         prof = lam + mx + my + mz;
+        den = prof;  // set by coarse_tables' caller: after the profiles (see bytes)
     }
+    // the mode factors follow the profiles of `rows` rows
+    __device__ void place_den(int mz, int rows) { den = prof + (size_t)rows * (mz + 2); }
 };
 
 // Sine matrices and the eigenvalues (2 cos(pi (j+1) / (m+1)) - 2) / H^2 of
@@ -777,6 +781,14 @@ __device__ void coarse_tables(const SorArgs<T, S> &a, const Coarse &cs) {
             cs.lam[loff + j] = (float)((2.0 * cospi((double)(j + 1) / (double)(m + 1)) - 2.0) / (H * H));
         loff += m;
     }
+    __syncthreads();
+    // the solve's per-mode factor: e^ = -f^ 8 / ((mx+1)(my+1)(mz+1)) / (lam_x + lam_y + lam_z)
+    const int mx = a.cmx, my = a.cmy, mz = a.cmz;
+    const float norm = 8.0f / (float)((mx + 1) * (my + 1) * (mz + 1));
+    for (int o = threadIdx.x; o < mx * my * mz; o += blockDim.x) {
+        const int K = o % mz, J = (o / mz) % my, I = o / (my * mz);
+        cs.den[o] = -norm / (cs.lam[I] + cs.lam[mx + J] + cs.lam[mx + my + K]);
+    }
 }
 
 // Stage 1: the triangle filter along z of the block's own rows of the
@@ -796,11 +808,16 @@ __device__ void coarse_stage1(const SorArgs<T, S> &a, const Block &B, const S *s
         if (y >= 1 && y <= ny - 2) {
             const int kc = F * (lane + 1);
             const S *row0 = ss + ((p * 2) * B.nr + j) * nz2, *row1 = row0 + B.nr * nz2;
-            for (int d = 1 - F; d < F; d++) {
-                const int k = kc + d;
-                if (k < 1 || k > nz - 2) continue;
-                const S *row = ((x + y + k) & 1) ? row1 : row0;
-                acc = fmaf((float)(F - abs(d)), (float)row[k >> 1], acc);
+            for (int d0 = 1 - F; d0 < F; d0 += 8) {
+                float v[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int d = d0 + q, k = kc + d;
+                    const S *row = ((x + y + k) & 1) ? row1 : row0;
+                    v[q] = (d < F && k >= 1 && k <= nz - 2) ? (float)row[k >> 1] : 0.0f;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q++) acc = fmaf((float)max(F - abs(d0 + q), 0), v[q], acc);
             }
         }
         __stcg(a.t1 + ((long long)x * ny + y) * mz + lane, acc * w0);
@@ -851,28 +868,45 @@ __device__ void coarse_stage23(const SorArgs<T, S> &a, int b) {
     }
 }
 
-// out = S applied along one axis of in ([mx][my][mz], z fastest).  A
-// half-warp takes a line: lane k keeps row k of S in registers and produces
-// element k, every lane reading the same input element at a time (a shared-
-// memory broadcast), so a line costs m loads and m multiply-adds per lane.
+// out = S applied along one axis of in ([mx][my][mz], z fastest), times
+// scale[element] when scale is given.  Eight threads take a line: thread k
+// keeps rows k and k + 8 of S in registers and produces elements k and k + 8,
+// so each input element loaded (the eight read the same one: a shared-memory
+// broadcast) feeds two multiply-adds.  (Measured against two threads per
+// line with eight outputs each, whose 450 threads left each pass latency-
+// bound at twice the time, and one thread per output and line, at 1.3x.)
 __device__ __forceinline__ void dst_pass(const float *in, float *out, const float *Sm, int m, int axis, int mx, int my,
-                                         int mz) {
-    const int k = threadIdx.x & 15, half = threadIdx.x >> 4, halves = blockDim.x >> 4;
-    float srow[kCoarseMax];
+                                         int mz, const float *scale) {
+    const int k0 = threadIdx.x & 7, k1 = k0 + 8, lg = threadIdx.x >> 3, lgs = blockDim.x >> 3;
+    float s0[kCoarseMax], s1[kCoarseMax];
 #pragma unroll
-    for (int j = 0; j < kCoarseMax; j++) srow[j] = (k < m && j < m) ? Sm[k * m + j] : 0.0f;
+    for (int j = 0; j < kCoarseMax; j++) {
+        s0[j] = (k0 < m && j < m) ? Sm[k0 * m + j] : 0.0f;
+        s1[j] = (k1 < m && j < m) ? Sm[k1 * m + j] : 0.0f;
+    }
     const int stride = axis == 2 ? 1 : axis == 1 ? mz : my * mz;
     const int L = axis == 2 ? mx * my : axis == 1 ? mx * mz : my * mz;
-    for (int line = half; line < L; line += halves) {
+    for (int line = lg; line < L; line += lgs) {
         int base;
         if (axis == 2) base = line * mz;
         else if (axis == 1) base = (line / mz) * (my * mz) + line % mz;
         else base = line;
-        float acc = 0.0f;
+        float a0 = 0.0f, a1 = 0.0f;
 #pragma unroll
         for (int j = 0; j < kCoarseMax; j++)
-            if (j < m) acc = fmaf(srow[j], in[base + j * stride], acc);
-        if (k < m) out[base + k * stride] = acc;
+            if (j < m) {
+                const float v = in[base + j * stride];
+                a0 = fmaf(s0[j], v, a0);
+                a1 = fmaf(s1[j], v, a1);
+            }
+        if (k0 < m) {
+            const int e = base + k0 * stride;
+            out[e] = scale ? a0 * scale[e] : a0;
+        }
+        if (k1 < m) {
+            const int e = base + k1 * stride;
+            out[e] = scale ? a1 * scale[e] : a1;
+        }
     }
 }
 
@@ -885,23 +919,17 @@ __device__ void coarse_solve(const SorArgs<T, S> &a, const Coarse &cs) {
     const float w0 = (float)(1.0 / a.src_scale);
     for (int o = threadIdx.x; o < M; o += blockDim.x) cs.ec[o] = __ldcg(a.t2 + o) * w0;
     __syncthreads();
-    dst_pass(cs.ec, cs.tmp, cs.sz, mz, 2, mx, my, mz);
+    dst_pass(cs.ec, cs.tmp, cs.sz, mz, 2, mx, my, mz, nullptr);
     __syncthreads();
-    dst_pass(cs.tmp, cs.ec, cs.sy, my, 1, mx, my, mz);
+    dst_pass(cs.tmp, cs.ec, cs.sy, my, 1, mx, my, mz, nullptr);
     __syncthreads();
-    dst_pass(cs.ec, cs.tmp, cs.sx, mx, 0, mx, my, mz);
+    dst_pass(cs.ec, cs.tmp, cs.sx, mx, 0, mx, my, mz, cs.den);  // with the per-mode factor
     __syncthreads();
-    const float norm = 8.0f / (float)((mx + 1) * (my + 1) * (mz + 1));
-    for (int o = threadIdx.x; o < M; o += blockDim.x) {
-        const int K = o % mz, J = (o / mz) % my, I = o / (my * mz);
-        cs.tmp[o] *= -norm / (cs.lam[I] + cs.lam[mx + J] + cs.lam[mx + my + K]);
-    }
+    dst_pass(cs.tmp, cs.ec, cs.sz, mz, 2, mx, my, mz, nullptr);
     __syncthreads();
-    dst_pass(cs.tmp, cs.ec, cs.sz, mz, 2, mx, my, mz);
+    dst_pass(cs.ec, cs.tmp, cs.sy, my, 1, mx, my, mz, nullptr);
     __syncthreads();
-    dst_pass(cs.ec, cs.tmp, cs.sy, my, 1, mx, my, mz);
-    __syncthreads();
-    dst_pass(cs.tmp, cs.ec, cs.sx, mx, 0, mx, my, mz);
+    dst_pass(cs.tmp, cs.ec, cs.sx, mx, 0, mx, my, mz, nullptr);
     __syncthreads();
 }
 
@@ -1007,7 +1035,8 @@ __device__ __forceinline__ void sor_body(const SorArgs<T, S> &a, const int b) {
     const Staged st(sd + (size_t)a.P * 2 * a.R * nz2 * (a.src_smem ? 2 : 1), a.P, a.R);
     unsigned *order = st.order;
     // coarse-grid correction: its arrays follow the ghost buffer
-    const Coarse cs(st.gbuf + (size_t)2 * (a.P + a.R) * nz2, a.cmx, a.cmy, a.cmz);
+    Coarse cs(st.gbuf + (size_t)2 * (a.P + a.R) * nz2, a.cmx, a.cmy, a.cmz);
+    cs.place_den(a.cmz, a.P * a.R + 2 * (a.P + a.R));
     int ng_rows = 0;  // ghost rows listed in st.gsrc (staged sweeps)
     auto SD = [&](int p, int c, int j, int t) -> S & { return sd[((p * 2 + c) * nr + j) * nz2 + t]; };
     unsigned my_phase = 0;
