@@ -253,15 +253,27 @@ struct PArgs {
 // One particle of one step: gather f_n, the closing kick/2 of the previous
 // step, observables of x_n, the excitation, the opening kick/2 and the drift;
 // returns x_{n+1} and the particle's species offset in the stacked grids.
+// The state (x_n, k) of one particle, loaded ahead of its update.
 template <typename T>
-__device__ __forceinline__ void particle_update(const PArgs<T> &a, int i, bool close, bool excite, T dmx, T dmy,
-                                                T dmz, double (&v)[6], T &px, T &py, T &pz, long long &off) {
+struct PState {
+    T px, py, pz, qx, qy, qz;
+};
+
+template <typename T>
+__device__ __forceinline__ PState<T> load_state(const PArgs<T> &a, int i) {
+    return PState<T>{a.x[i], a.y[i], a.z[i], a.kx[i], a.ky[i], a.kz[i]};
+}
+
+template <typename T>
+__device__ __forceinline__ void particle_update(const PArgs<T> &a, int i, const PState<T> &st, bool close, bool excite,
+                                                T dmx, T dmy, T dmz, double (&v)[6], T &px, T &py, T &pz,
+                                                long long &off) {
     const int s = i < a.protons ? 0 : 1;
     off = s ? a.g.G : 0;
-    px = a.x[i];
-    py = a.y[i];
-    pz = a.z[i];
-    T qx = a.kx[i], qy = a.ky[i], qz = a.kz[i];
+    px = st.px;
+    py = st.py;
+    pz = st.pz;
+    T qx = st.qx, qy = st.qy, qz = st.qz;
     T fx, fy, fz;
     gather_at<T>(a.g, a.F4, off, px, py, pz, fx, fy, fz);
     if (close) {  // closing kick/2 of the previous step (physics.hpp:248-258)
@@ -298,14 +310,21 @@ __global__ void __launch_bounds__(kB) k_particle_step(PArgs<T> a) {
     const bool excite = a.ctl[CTL_EXCITE] == step;
     const T dmx = T(a.g.dmx), dmy = T(a.g.dmy), dmz = T(a.g.dmz);
     double v[6] = {0, 0, 0, 0, 0, 0};
-    // warp-uniform trip count (the aggregated deposit needs every lane)
+    // warp-uniform trip count (the aggregated deposit needs every lane); the
+    // next particle's state is loaded before this one's gathers and atomics,
+    // so that its memory round trip overlaps them
     const int stride = gridDim.x * blockDim.x;
+    const int i_first = blockIdx.x * blockDim.x + threadIdx.x;
+    PState<T> next{};
+    if (i_first < a.total) next = load_state(a, i_first);
     for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < a.total; i0 += stride) {
         const int i = i0 + (threadIdx.x & 31);
         const bool valid = i < a.total;
+        const PState<T> cur = next;
+        if (i + stride < a.total) next = load_state(a, i + stride);
         T px = T(0), py = T(0), pz = T(0);
         long long off = 0;
-        if (valid) particle_update<T>(a, i, close, excite, dmx, dmy, dmz, v, px, py, pz, off);
+        if (valid) particle_update<T>(a, i, cur, close, excite, dmx, dmy, dmz, v, px, py, pz, off);
         if (!a.deposit) continue;
         if constexpr (sizeof(T) == 4) {
             if (a.aggregate) {
@@ -784,15 +803,54 @@ hv_status run_begin(hv_ctx *c, int n_steps, int *exc_out) {
 
 // After k steps that started at step s0: their observable rows (obs[0..k)),
 // and the SOR status; synchronous.
+// The rows of k steps from step s0 into host memory (pinned for an
+// asynchronous copy): k x 8 doubles, then the solver's per-step iteration
+// ring (kRing ints); stream-ordered, no synchronisation.
+hv_status rows_enqueue(hv_ctx *c, int s0, int k, double *rows, int *its) {
+    Fused &f = c->fused;
+    k_reduce_rows<<<k, 32, 0, c->stream>>>(f.obs_partials, f.obs_blocks, s0, k, f.obs_rows_dev);
+    HV_CUDA(cudaGetLastError());
+    HV_CUDA(cudaMemcpyAsync(rows, f.obs_rows_dev, sizeof(double) * 8 * k, cudaMemcpyDeviceToHost, c->stream));
+    HV_CUDA(cudaMemcpyAsync(its, f.sor_its, sizeof(int) * kRing, cudaMemcpyDeviceToHost, c->stream));
+    return HV_OK;
+}
+
+// Decodes k rows copied by rows_enqueue (the stream synchronised since).
+template <typename T>
+void rows_decode(hv_ctx *c, int s0, int k, const double *rows, const int *its, hv_observables *obs) {
+    const double zz = c->params.z, nn = c->params.n;
+    for (int r = 0; r < k; r++) {
+        hv_observables &o = obs[r];
+        const double *v = &rows[(size_t)r * 8];
+        std::memset(&o, 0, sizeof(o));
+        o.t = (double)(T(s0 + r) * T(c->params.dt));
+        o.zcm_p = v[0] / (double)c->protons;
+        o.zcm_n = v[1] / (double)c->neutrons;
+        o.rms_p = std::sqrt(v[2] / v[4]);
+        o.rms_n = std::sqrt(v[3] / v[5]);
+        o.dipole = (nn * zz) / (nn + zz) * (o.zcm_p - o.zcm_n);
+        const int it = its[(s0 + r) % kRing];
+        o.sor_iterations = it < 0 ? -it : it;
+        if (it < 0) o.flags |= HV_OBS_SOR_NOT_CONVERGED;
+    }
+}
+
+// A timed-out solve (the sticky error word): the steps ran on an unfinished
+// potential, and the next run solves the fields of the current positions again.
+hv_status rows_status(hv_ctx *c, int status0) {
+    if (!status0) return HV_OK;
+    c->fields_valid = false;
+    fused_invalidate(c);
+    set_last_error("SOR: a bounded device-side wait timed out");
+    return HV_ERR_TIMEOUT;
+}
+
 template <typename T>
 hv_status run_rows(hv_ctx *c, int s0, int k, hv_observables *obs) {
     Fused &f = c->fused;
     std::vector<double> rows((size_t)k * 8);
     std::vector<int> its(kRing);
-    k_reduce_rows<<<k, 32, 0, c->stream>>>(f.obs_partials, f.obs_blocks, s0, k, f.obs_rows_dev);
-    HV_CUDA(cudaGetLastError());
-    HV_CUDA(cudaMemcpyAsync(rows.data(), f.obs_rows_dev, sizeof(double) * 8 * k, cudaMemcpyDeviceToHost, c->stream));
-    HV_CUDA(cudaMemcpyAsync(its.data(), f.sor_its, sizeof(int) * kRing, cudaMemcpyDeviceToHost, c->stream));
+    HV_TRY(rows_enqueue(c, s0, k, rows.data(), its.data()));
     int status[3] = {0, 0, 0};
     HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
     HV_CUDA(cudaStreamSynchronize(c->stream));
@@ -835,8 +893,30 @@ hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
     HV_TRY(run_begin<T>(c, n_steps, &exc));
     const int chunk = c->fast.graph_steps > 0 ? std::min(c->fast.graph_steps, kRing) : std::min(8, kRing);
     int done = 0;
-    std::vector<double> rows;
-    std::vector<int> its(kRing);
+    // the rows go to the context's pinned staging memory chunk by chunk
+    // without a synchronisation per chunk (profiled runs synchronise per
+    // chunk to read their events)
+    const bool async_rows = !c->prof.on;
+    const int max_chunks = (n_steps + chunk - 1) / chunk;
+    double *host_rows = nullptr;
+    int *host_its = nullptr;
+    int nchunk = 0;
+    std::vector<int> chunk_start;
+    if (async_rows) {
+        const size_t need = sizeof(double) * 8 * (size_t)n_steps + sizeof(int) * ((size_t)max_chunks * kRing + 4);
+        if (c->staging_bytes < need) {
+            // room for runs of 4096 steps at least, so that the pinned buffer
+            // is not reallocated run after run
+            const size_t least = sizeof(double) * 8 * 4096 + sizeof(int) * ((size_t)4096 * kRing + 4);
+            if (c->staging) cudaFreeHost(c->staging);
+            c->staging = nullptr;
+            c->staging_bytes = 0;
+            HV_CUDA(cudaMallocHost(&c->staging, std::max(need, least)));
+            c->staging_bytes = std::max(need, least);
+        }
+        host_rows = static_cast<double *>(c->staging);
+        host_its = reinterpret_cast<int *>(host_rows + (size_t)8 * n_steps);
+    }
     while (done < n_steps) {
         const int k = std::min(chunk, n_steps - done);
         // slot re-sort by cell every sort_every steps (at most once per
@@ -874,8 +954,27 @@ hv_status run_typed(hv_ctx *c, int n_steps, hv_observables *obs) {
             }
         }
         if (!launched) HV_TRY(enqueue_steps<T>(c, k));
-        HV_TRY(run_rows<T>(c, c->step_index + done, k, obs ? obs + done : nullptr));
+        if (async_rows) {
+            HV_TRY(rows_enqueue(c, c->step_index + done, k, host_rows + (size_t)done * 8, host_its + (size_t)nchunk * kRing));
+            chunk_start.push_back(done);
+            nchunk++;
+        } else {
+            HV_TRY(run_rows<T>(c, c->step_index + done, k, obs ? obs + done : nullptr));
+        }
         done += k;
+    }
+    if (async_rows) {
+        // one synchronisation for the whole run: the rows, then the error word
+        int *status = host_its + (size_t)nchunk * kRing;
+        HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        HV_CUDA(cudaStreamSynchronize(c->stream));
+        HV_TRY(rows_status(c, *status));
+        if (obs)
+            for (int q = 0; q < nchunk; q++) {
+                const int d0 = chunk_start[q], kk = (q + 1 < nchunk ? chunk_start[q + 1] : n_steps) - d0;
+                rows_decode<T>(c, c->step_index + d0, kk, host_rows + (size_t)d0 * 8, host_its + (size_t)q * kRing,
+                               obs + d0);
+            }
     }
     return run_end<T>(c, n_steps, exc);
 }
