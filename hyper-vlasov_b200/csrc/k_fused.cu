@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kPBlock = 256;      // default threads per block of the particle step
 constexpr int kPBlockMax = 512;   // largest of the autotuner's candidates
-constexpr int kPGridMax = 8;      // most blocks per SM of the particle step
+constexpr int kPGridMax = 16;     // most blocks per SM of the particle step
 constexpr int kForceRows = 8;     // y rows per thread of the forces kernel
 constexpr int kRing = 64;  // observable rows kept on the device
 
@@ -56,16 +56,48 @@ __device__ __forceinline__ void load_f4<double>(const double *F4, long long node
     fz = b.x;
 }
 
+// Grid coordinates of a position, (n / 2) (p / d_max + 1) per axis
+// (include/tools.hpp:35-96 and :98-168).  In float the division is a product
+// by the axis's reciprocal d_max, formed once per launch: the particle step
+// would otherwise make six IEEE divisions per particle.  A coordinate then
+// moves by at most about an ulp; a particle that lies on a cell face may land
+// in the neighbouring cell with a weight of ~0 there, which the continuity of
+// the CIC weights makes harmless.  The double form keeps the division.
+template <typename T>
+struct CellMap {
+    T hx, hy, hz;  // n / 2
+    T ix, iy, iz;  // 1 / d_max (float form)
+    T dx, dy, dz;  // d_max (double form)
+};
+
+template <typename T>
+__device__ __forceinline__ CellMap<T> cell_map(const Geom &g) {
+    return CellMap<T>{g.nx / T(2.0),      g.ny / T(2.0),      g.nz / T(2.0), T(1.0) / T(g.dmx), T(1.0) / T(g.dmy),
+                      T(1.0) / T(g.dmz), T(g.dmx),           T(g.dmy),      T(g.dmz)};
+}
+
+template <typename T>
+__device__ __forceinline__ void cell_coords(const CellMap<T> &m, T px, T py, T pz, T &cx, T &cy, T &cz) {
+    if constexpr (sizeof(T) == 4) {
+        cx = m.hx * (px * m.ix + T(1.0));
+        cy = m.hy * (py * m.iy + T(1.0));
+        cz = m.hz * (pz * m.iz + T(1.0));
+    } else {
+        cx = m.hx * (px / m.dx + T(1.0));
+        cy = m.hy * (py / m.dy + T(1.0));
+        cz = m.hz * (pz / m.dz + T(1.0));
+    }
+}
+
 // CIC force gather at (px,py,pz) (distribute_forces_to_particles_cic,
 // include/tools.hpp:98-168; corner order and corner drop as there).
 template <typename T>
-__device__ __forceinline__ void gather_at(const Geom &g, const T *F4, long long off, T px, T py, T pz, T &ax, T &ay,
-                                          T &az) {
+__device__ __forceinline__ void gather_at(const Geom &g, const CellMap<T> &m, const T *F4, long long off, T px, T py,
+                                          T pz, T &ax, T &ay, T &az) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     ax = ay = az = T(0);
-    T cx = (nx / T(2.0)) * (px / T(g.dmx) + T(1.0));
-    T cy = (ny / T(2.0)) * (py / T(g.dmy) + T(1.0));
-    T cz = (nz / T(2.0)) * (pz / T(g.dmz) + T(1.0));
+    T cx, cy, cz;
+    cell_coords<T>(m, px, py, pz, cx, cy, cz);
     if (cx < T(0) || cy < T(0) || cz < T(0) || cx >= nx || cy >= ny || cz >= nz) return;
     int x0 = (int)cx, y0 = (int)cy, z0 = (int)cz;
     T dx = cx - x0, dy = cy - y0, dz = cz - z0;
@@ -96,11 +128,11 @@ __device__ __forceinline__ void gather_at(const Geom &g, const T *F4, long long 
 // CIC deposit of one particle (distribute_volumetric_particles_cic,
 // include/tools.hpp:35-96), atomically.
 template <typename T>
-__device__ __forceinline__ void deposit_at(const Geom &g, T *rho, long long off, T px, T py, T pz) {
+__device__ __forceinline__ void deposit_at(const Geom &g, const CellMap<T> &m, T *rho, long long off, T px, T py,
+                                           T pz) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    T cx = (nx / T(2.0)) * (px / T(g.dmx) + T(1.0));
-    T cy = (ny / T(2.0)) * (py / T(g.dmy) + T(1.0));
-    T cz = (nz / T(2.0)) * (pz / T(g.dmz) + T(1.0));
+    T cx, cy, cz;
+    cell_coords<T>(m, px, py, pz, cx, cy, cz);
     if (cx < T(0) || cy < T(0) || cz < T(0) || cx >= nx || cy >= ny || cz >= nz) return;
     int x0 = (int)cx, y0 = (int)cy, z0 = (int)cz;
     T dx = cx - x0, dy = cy - y0, dz = cz - z0;
@@ -189,13 +221,12 @@ __device__ __forceinline__ void add_corners(const Geom &g, float *rho, long long
 // issues the atomics (distribute_volumetric_particles_cic,
 // include/tools.hpp:35-96: the same cells, weights and corner drops; only the
 // order of the float additions differs).
-__device__ __forceinline__ void deposit_warp(const Geom &g, float *rho, long long off, float px, float py, float pz,
-                                             bool valid) {
+__device__ __forceinline__ void deposit_warp(const Geom &g, const CellMap<float> &m, float *rho, long long off,
+                                             float px, float py, float pz, bool valid) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int lane = threadIdx.x & 31;
-    const float cx = (nx / 2.0f) * (px / (float)g.dmx + 1.0f);
-    const float cy = (ny / 2.0f) * (py / (float)g.dmy + 1.0f);
-    const float cz = (nz / 2.0f) * (pz / (float)g.dmz + 1.0f);
+    float cx, cy, cz;
+    cell_coords<float>(m, px, py, pz, cx, cy, cz);
     const bool in = valid && !(cx < 0.0f || cy < 0.0f || cz < 0.0f || cx >= nx || cy >= ny || cz >= nz);
     int x0 = 0, y0 = 0, z0 = 0;
     float w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -264,10 +295,18 @@ __device__ __forceinline__ PState<T> load_state(const PArgs<T> &a, int i) {
     return PState<T>{a.x[i], a.y[i], a.z[i], a.kx[i], a.ky[i], a.kz[i]};
 }
 
+// The observable sums of one thread, per species (v[s], v[2 + s], v[4 + s]
+// with s the species): indexed by constants only, so that they stay in
+// registers (an index by the particle's species put them in local memory).
+struct ObsSums {
+    double z0, z1, r0, r1;
+    int n0, n1;  // counts, exact in an int
+};
+
 template <typename T>
-__device__ __forceinline__ void particle_update(const PArgs<T> &a, int i, const PState<T> &st, bool close, bool excite,
-                                                T dmx, T dmy, T dmz, double (&v)[6], T &px, T &py, T &pz,
-                                                long long &off) {
+__device__ __forceinline__ void particle_update(const PArgs<T> &a, const CellMap<T> &m, int i, const PState<T> &st,
+                                                bool close, bool excite, T dmx, T dmy, T dmz, ObsSums &v, T &px,
+                                                T &py, T &pz, long long &off) {
     const int s = i < a.protons ? 0 : 1;
     off = s ? a.g.G : 0;
     px = st.px;
@@ -275,17 +314,28 @@ __device__ __forceinline__ void particle_update(const PArgs<T> &a, int i, const 
     pz = st.pz;
     T qx = st.qx, qy = st.qy, qz = st.qz;
     T fx, fy, fz;
-    gather_at<T>(a.g, a.F4, off, px, py, pz, fx, fy, fz);
+    gather_at<T>(a.g, m, a.F4, off, px, py, pz, fx, fy, fz);
     if (close) {  // closing kick/2 of the previous step (physics.hpp:248-258)
         qx += a.h * fx;
         qy += a.h * fy;
         qz += a.h * fz;
     }
     // observables of x_n (tools.hpp:302-338)
-    v[s] += (double)pz;
-    if (!(px < -dmx || px > dmx || py < -dmy || py > dmy || pz < -dmz || pz > dmz)) {
-        v[2 + s] += (double)(px * px + py * py + pz * pz);
-        v[4 + s] += 1.0;
+    const bool inside = !(px < -dmx || px > dmx || py < -dmy || py > dmy || pz < -dmz || pz > dmz);
+    const double zd = (double)pz;
+    const double r2 = inside ? (double)(px * px + py * py + pz * pz) : 0.0;
+    if (s == 0) {
+        v.z0 += zd;
+        if (inside) {
+            v.r0 += r2;
+            v.n0 += 1;
+        }
+    } else {
+        v.z1 += zd;
+        if (inside) {
+            v.r1 += r2;
+            v.n1 += 1;
+        }
     }
     if (excite) qz += s ? -a.dn : a.dp;  // physics.hpp:236-246
     qx += a.h * fx;                      // opening kick/2
@@ -303,42 +353,55 @@ __device__ __forceinline__ void particle_update(const PArgs<T> &a, int i, const 
 }
 
 // One step of every particle; observables of x_n into the ring row of step n.
+// Float: at most 64 registers a thread (1024 threads resident per SM), with
+// no spills; the step is bound by the latency of its gathers, so resident
+// warps count.  The double form would spill under that bound and is left
+// unbounded (its step is dominated by the double solve).
 template <typename T, int kB>
-__global__ void __launch_bounds__(kB) k_particle_step(PArgs<T> a) {
+__global__ void __launch_bounds__(kB, sizeof(T) == 4 ? 1024 / kB : 1) k_particle_step(PArgs<T> a) {
     const int step = a.ctl[CTL_STEP];
     const bool close = a.ctl[CTL_CLOSE] != 0;
     const bool excite = a.ctl[CTL_EXCITE] == step;
     const T dmx = T(a.g.dmx), dmy = T(a.g.dmy), dmz = T(a.g.dmz);
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    // warp-uniform trip count (the aggregated deposit needs every lane); the
-    // next particle's state is loaded before this one's gathers and atomics,
-    // so that its memory round trip overlaps them
-    const int stride = gridDim.x * blockDim.x;
-    const int i_first = blockIdx.x * blockDim.x + threadIdx.x;
+    const CellMap<T> m = cell_map<T>(a.g);
+    ObsSums v{0.0, 0.0, 0.0, 0.0, 0, 0};
+    // Each block takes one contiguous chunk of the slots (a multiple of 32):
+    // the slots are sorted by cell every few steps, so a block's particles
+    // lie in a few rows of cells and their force gathers hit in L1.  Warp-
+    // uniform trip count (the aggregated deposit needs every lane); the next
+    // particle's state is loaded before this one's gathers and atomics, so
+    // that its memory round trip overlaps them.
+    const int chunk = (int)((((long long)a.total + gridDim.x - 1) / gridDim.x + 31) & ~31ll);
+    const int begin = (int)min((long long)blockIdx.x * chunk, (long long)a.total);
+    const int end = (int)min((long long)begin + chunk, (long long)a.total);
+    const int stride = blockDim.x;
+    const int i_first = begin + threadIdx.x;
     PState<T> next{};
-    if (i_first < a.total) next = load_state(a, i_first);
-    for (int i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); i0 < a.total; i0 += stride) {
+    if (i_first < end) next = load_state(a, i_first);
+    for (int i0 = begin + (threadIdx.x & ~31); i0 < end; i0 += stride) {
         const int i = i0 + (threadIdx.x & 31);
-        const bool valid = i < a.total;
+        const bool valid = i < end;
         const PState<T> cur = next;
-        if (i + stride < a.total) next = load_state(a, i + stride);
+        if (i + stride < end) next = load_state(a, i + stride);
         T px = T(0), py = T(0), pz = T(0);
         long long off = 0;
-        if (valid) particle_update<T>(a, i, cur, close, excite, dmx, dmy, dmz, v, px, py, pz, off);
+        if (valid) particle_update<T>(a, m, i, cur, close, excite, dmx, dmy, dmz, v, px, py, pz, off);
         if (!a.deposit) continue;
         if constexpr (sizeof(T) == 4) {
             if (a.aggregate) {
-                deposit_warp(a.g, reinterpret_cast<float *>(a.rho_raw), off, px, py, pz, valid);
+                deposit_warp(a.g, m, reinterpret_cast<float *>(a.rho_raw), off, px, py, pz, valid);
                 continue;
             }
         }
-        if (valid) deposit_at<T>(a.g, a.rho_raw, off, px, py, pz);
+        if (valid) deposit_at<T>(a.g, m, a.rho_raw, off, px, py, pz);
     }
     // deterministic block reduction of the six sums
     __shared__ double sh[6][kB / 32];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const double vs[6] = {v.z0, v.z1, v.r0, v.r1, (double)v.n0, (double)v.n1};
+#pragma unroll
     for (int c = 0; c < 6; c++) {
-        double u = v[c];
+        double u = vs[c];
         for (int o = 16; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
         if (l == 0) sh[c][w] = u;
     }
@@ -357,7 +420,7 @@ __global__ void k_close_kick(Geom g, int protons, int total, const T *__restrict
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     T ax, ay, az;
-    gather_at<T>(g, F4, i < protons ? 0 : g.G, x[i], y[i], z[i], ax, ay, az);
+    gather_at<T>(g, cell_map<T>(g), F4, i < protons ? 0 : g.G, x[i], y[i], z[i], ax, ay, az);
     kx[i] += h * ax;
     ky[i] += h * ay;
     kz[i] += h * az;
@@ -1105,7 +1168,7 @@ hv_status fused_autotune(hv_ctx *c, int trial, hv_autotune_report *rep) {
     Fused &f = c->fused;
     int count = 0;
     double best_ms = 0.0, ms = 0.0;
-    const int blocks[3] = {128, 256, 512}, grids[3] = {2, 4, 8};
+    const int blocks[3] = {128, 256, 512}, grids[4] = {2, 4, 8, 16};
     int best_b = f.pblock, best_g = f.obs_blocks;
     for (int pb : blocks)
         for (int pg : grids) {
