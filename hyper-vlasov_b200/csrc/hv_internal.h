@@ -123,6 +123,7 @@ struct SmoothFast {
     // FFT form (power-of-two axes up to 128): the circular convolution by the
     // stencil's spectrum, exact while no density lies within (A, B, W) of a face
     bool fft = false;
+    bool fft128 = false;       // 128^3: the register-transform kernels (khat in natural z order)
     void *fwork = nullptr;     // nx ny nz complex floats: both species' transform
     float *khat = nullptr;     // nx ny nz: the stencil's spectrum x term / (nx ny nz)
     void *tw = nullptr;        // 64 complex twiddles exp(-2 pi i m / 128)

@@ -435,15 +435,208 @@ __global__ void __launch_bounds__(kFThreads) k_fft_plane_inv(const __grid_consta
 }
 
 // khat(kx, ky, zrev(kz)) = sum_a cx[a][kx] Y_a(ky, kz): the last sum of the
-// stencil's spectrum, one node per thread, in double.
-__global__ void k_fft_khat(int nx, int P, int nz, int lz, int na, const double *cx, const double *ya, float *khat) {
+// stencil's spectrum, one node per thread, in double.  zrev = 0 keeps z in
+// natural order (the 128^3 form below).
+__global__ void k_fft_khat(int nx, int P, int nz, int lz, int na, const double *cx, const double *ya, float *khat,
+                           int zrev) {
     const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (id >= (long long)nx * P) return;
     const int kx = (int)(id / P), q = (int)(id - (long long)kx * P);
     double acc = 0.0;
     for (int a = 0; a < na; a++) acc += cx[a * nx + kx] * ya[(size_t)a * P + q];
     const int ky = q >> lz, kz = q & (nz - 1);
-    khat[(long long)kx * P + ((long long)ky << lz) + bit_reverse(kz, lz)] = (float)acc;
+    khat[(long long)kx * P + ((long long)ky << lz) + (zrev ? bit_reverse(kz, lz) : kz)] = (float)acc;
+}
+
+// ---- The 128^3 form: 128-point transforms as 16 x 8 in registers ----------
+//
+// A block transforms 128 lines of 128 points, eight threads a line (thread j
+// of a line holds points j + 8c, c = 0..15).  With n = 8a + b and
+// k = k1 + 16 k2 (a, k1 < 16; b, k2 < 8):
+//   X[k1 + 16 k2] = sum_b W8^(b k2) W128^(b k1) sum_a x[8a + b] W16^(a k1).
+// Thread j computes the inner 16-point transform of its points in registers
+// and multiplies by W128^(j k1); the 16 x 8 values of a line then cross once
+// through shared memory (position 8 k1 + b), and thread j takes k1 = j and
+// j + 8 for two 8-point transforms over b.  It ends holding X[j + 8c], the
+// layout it started from, so a forward and an inverse transform chain in
+// registers.  The warps of a block hold 32 consecutive lines each (thread
+// index = j * 128 + line), so a warp's 32 accesses of any step go to 32
+// lines: consecutive addresses along a column, or rows 129 complex apart,
+// which spreads them over every bank.  An inverse is conj(forward(conj(.))).
+// Per kernel the plane crosses shared memory four times (twice per axis)
+// instead of once per radix-4 stage.
+constexpr int kF128 = 128;
+constexpr int kFRow = 129;  // row stride of a shared plane, in complex elements
+constexpr size_t kF128Smem = sizeof(float2) * kF128 * kFRow;
+
+__host__ __device__ constexpr int brev4(int i) { return ((i & 1) << 3) | ((i & 2) << 1) | ((i & 4) >> 1) | ((i & 8) >> 3); }
+__host__ __device__ constexpr int brev3(int i) { return ((i & 1) << 2) | (i & 2) | ((i & 4) >> 2); }
+
+// v W16^e for e in [0, 8): W16 = exp(-2 pi i / 16); cos and sin of pi/8,
+// pi/4 and 3 pi/8
+__device__ __forceinline__ float2 mul_w16(float2 v, int e) {
+    constexpr float c1 = 0.923879532511286756f, s1 = 0.382683432365089772f, r2 = 0.707106781186547524f;
+    switch (e) {
+        case 1: return make_float2(c1 * v.x + s1 * v.y, c1 * v.y - s1 * v.x);
+        case 2: return make_float2(r2 * (v.x + v.y), r2 * (v.y - v.x));
+        case 3: return make_float2(s1 * v.x + c1 * v.y, s1 * v.y - c1 * v.x);
+        case 4: return make_float2(v.y, -v.x);
+        case 5: return make_float2(c1 * v.y - s1 * v.x, -s1 * v.y - c1 * v.x);
+        case 6: return make_float2(r2 * (v.y - v.x), -r2 * (v.x + v.y));
+        case 7: return make_float2(s1 * v.y - c1 * v.x, -c1 * v.y - s1 * v.x);
+        default: return v;
+    }
+}
+
+// In-place decimation-in-frequency transform of N = 16 or 8 points in
+// registers (natural in, bit-reversed out); every index and twiddle exponent
+// is a constant once unrolled.
+template <int N>
+__device__ __forceinline__ void dft_regs(float2 (&a)[N]) {
+#pragma unroll
+    for (int h = N / 2; h >= 1; h >>= 1) {
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if (i & h) continue;
+            const float2 u = a[i], v = a[i + h];
+            a[i] = cadd(u, v);
+            a[i + h] = mul_w16(csub(u, v), (i & (h - 1)) * (8 / h));
+        }
+    }
+}
+
+// The 128-point transform of one line (see above): r holds points j + 8c in,
+// X[j + 8c] out.  xb[p * ps] is the line's exchange area (p < 128), tw the
+// 128 powers of W128.  Every thread of the block calls it at once.
+__device__ __forceinline__ void fft128_line(float2 (&r)[16], int j, float2 *xb, int ps, const float2 *tw) {
+    dft_regs<16>(r);  // r[brev4(k1)] = sum_a x[8a + j] W16^(a k1)
+#pragma unroll
+    for (int k1 = 1; k1 < 16; k1++) r[brev4(k1)] = cmul(r[brev4(k1)], tw[(j * k1) & 127]);
+    __syncthreads();  // the exchange area may still hold inputs being read
+#pragma unroll
+    for (int k1 = 0; k1 < 16; k1++) xb[(8 * k1 + j) * ps] = r[brev4(k1)];
+    __syncthreads();
+    float2 e0[8], e1[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        e0[b] = xb[(8 * j + b) * ps];
+        e1[b] = xb[(64 + 8 * j + b) * ps];
+    }
+    dft_regs<8>(e0);  // e0[brev3(k2)] = X[j + 16 k2]
+    dft_regs<8>(e1);  // e1[brev3(k2)] = X[j + 8 + 16 k2]
+#pragma unroll
+    for (int k2 = 0; k2 < 8; k2++) {
+        r[2 * k2] = e0[brev3(k2)];
+        r[2 * k2 + 1] = e1[brev3(k2)];
+    }
+}
+
+__device__ __forceinline__ float2 cconj(float2 v) { return make_float2(v.x, -v.y); }
+
+__device__ __forceinline__ void load_tw128(const float2 *tw64, float2 *tw) {
+    if (threadIdx.x < 64) {
+        const float2 w = tw64[threadIdx.x];
+        tw[threadIdx.x] = w;
+        tw[threadIdx.x + 64] = make_float2(-w.x, -w.y);  // W128^(m + 64) = -W128^m
+    }
+}
+
+// Pass 1 at 128^3, per x plane: forward along y (lines are z columns, loaded
+// straight from the densities: consecutive lanes, consecutive z), then along
+// z (lines are rows of the shared plane), stored through the plane so that
+// the store is coalesced.  Flags density within the stencil of a face.
+__global__ void __launch_bounds__(kFThreads, 1) k_fft128_plane_fwd(const __grid_constant__ FftArgs a) {
+    extern __shared__ __align__(16) float2 fs[];  // 128 rows of kFRow
+    __shared__ float2 tw[kF128];
+    const int x = blockIdx.x, tid = threadIdx.x, line = tid & 127, j = tid >> 7, P = kF128 * kF128;
+    load_tw128(a.tw, tw);
+    const float *sp = a.src + (long long)x * P, *sn = sp + a.G;
+    const bool zx_edge = x < a.A || x >= kF128 - a.A || line < a.W || line >= kF128 - a.W;
+    int edge = 0;
+    float2 r[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+        const int y = j + 8 * c;
+        const float rp = __ldg(sp + y * kF128 + line), rn = __ldg(sn + y * kF128 + line);
+        if ((rp != 0.0f || rn != 0.0f) && (zx_edge || y < a.B || y >= kF128 - a.B)) edge = 1;
+        r[c] = make_float2(rp, rn);
+    }
+    edge = __syncthreads_or(edge);  // also publishes tw
+    if (tid == 0) a.edge[x] = edge;
+    fft128_line(r, j, fs + line, kFRow, tw);  // r[c] = V[ky = j + 8c][z = line]
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; c++) fs[(j + 8 * c) * kFRow + line] = r[c];
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; c++) r[c] = fs[line * kFRow + j + 8 * c];
+    fft128_line(r, j, fs + line * kFRow, 1, tw);  // r[c] = Z[ky = line][kz = j + 8c]
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; c++) fs[line * kFRow + j + 8 * c] = r[c];
+    __syncthreads();
+    float2 *out = a.work + (long long)x * P;
+    for (int e = tid; e < P; e += kFThreads) out[e] = fs[(e >> 7) * kFRow + (e & 127)];
+}
+
+// Pass 2 at 128^3, per y: forward along x (lines are z columns, loaded and
+// stored straight: consecutive lanes, consecutive z), the product by the
+// spectrum (natural order), and the inverse along x.
+__global__ void __launch_bounds__(kFThreads, 1) k_fft128_columns(const __grid_constant__ FftArgs a) {
+    extern __shared__ __align__(16) float2 fs[];
+    __shared__ float2 tw[kF128];
+    const int y = blockIdx.x, tid = threadIdx.x, line = tid & 127, j = tid >> 7, P = kF128 * kF128;
+    load_tw128(a.tw, tw);
+    float2 *col = a.work + (long long)y * kF128 + line;
+    const float *kh = a.khat + (long long)y * kF128 + line;
+    float2 r[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) r[c] = col[(long long)(j + 8 * c) * P];
+    __syncthreads();  // tw
+    fft128_line(r, j, fs + line, kFRow, tw);  // r[c] = F[kx = j + 8c]
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+        const float k = __ldg(kh + (long long)(j + 8 * c) * P);
+        r[c] = cconj(make_float2(r[c].x * k, r[c].y * k));
+    }
+    fft128_line(r, j, fs + line, kFRow, tw);
+#pragma unroll
+    for (int c = 0; c < 16; c++) col[(long long)(j + 8 * c) * P] = cconj(r[c]);
+}
+
+// Pass 3 at 128^3, per x plane: inverse along y (lines are z columns, loaded
+// straight), then along z (rows), both species stored through the plane,
+// scaled and clamped at 0.
+__global__ void __launch_bounds__(kFThreads, 1) k_fft128_plane_inv(const __grid_constant__ FftArgs a) {
+    extern __shared__ __align__(16) float2 fs[];
+    __shared__ float2 tw[kF128];
+    const int x = blockIdx.x, tid = threadIdx.x, line = tid & 127, j = tid >> 7, P = kF128 * kF128;
+    load_tw128(a.tw, tw);
+    const float2 *in = a.work + (long long)x * P + line;
+    float2 r[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) r[c] = cconj(in[(j + 8 * c) * kF128]);
+    __syncthreads();  // tw
+    fft128_line(r, j, fs + line, kFRow, tw);  // r[c]: y = j + 8c, z = line (conjugated domain)
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; c++) fs[(j + 8 * c) * kFRow + line] = r[c];
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; c++) r[c] = fs[line * kFRow + j + 8 * c];
+    fft128_line(r, j, fs + line * kFRow, 1, tw);  // r[c]: y = line, z = j + 8c
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 16; c++) fs[line * kFRow + j + 8 * c] = r[c];
+    __syncthreads();
+    float *dp = a.dst + (long long)x * P, *dn = dp + a.G;
+    for (int e = tid; e < P; e += kFThreads) {
+        const float2 v = cconj(fs[(e >> 7) * kFRow + (e & 127)]);
+        // the exact sum is non-negative; rounding must not leave negative
+        // densities, where rho^gamma has no value
+        dp[e] = fmaxf(v.x * a.post, 0.0f);
+        dn[e] = fmaxf(v.y * a.post, 0.0f);
+    }
 }
 
 int log2_exact(int n) {
@@ -558,6 +751,7 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     //   Z_w(kz)     = sum_{|c| <= w} g(c) cos(2 pi c kz / nz),
     // m = 1 at 0 and 2 elsewhere; scaled by term / G (the inverse transform's 1/G).
     const int nx = gg.nx, ny = gg.ny, nz = gg.nz, P = ny * nz;
+    f.fft128 = nx == kF128 && ny == kF128 && nz == kF128;
     std::vector<double> gxd(A + 1), gyd(B + 1), gzd(W + 1);
     auto g1d = [&](int axis, int off) {
         const int n = wd.n[axis], ctr = n / 2;
@@ -626,7 +820,7 @@ hv_status smooth_fast_plan(hv_ctx *c) {
             ce = cudaMemcpyAsync(dya, ya.data(), sizeof(double) * ya.size(), cudaMemcpyHostToDevice, c->stream);
         if (ce == cudaSuccess) {
             k_fft_khat<<<(unsigned)((gg.G + 255) / 256), 256, 0, c->stream>>>(nx, P, nz, lz, A + 1, dcx, dya,
-                                                                             f.khat);
+                                                                             f.khat, f.fft128 ? 0 : 1);
             ce = cudaGetLastError();
         }
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(c->stream);
@@ -637,6 +831,9 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     const size_t plane = sizeof(float2) * (size_t)std::max(P, nx * nz);
     for (const void *k : {(const void *)k_fft_plane_fwd, (const void *)k_fft_columns, (const void *)k_fft_plane_inv})
         HV_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plane));
+    for (const void *k :
+         {(const void *)k_fft128_plane_fwd, (const void *)k_fft128_columns, (const void *)k_fft128_plane_inv})
+        HV_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kF128Smem));
     f.fft = true;
     return HV_OK;
 }
@@ -696,10 +893,16 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho) {
         q.tw = reinterpret_cast<const float2 *>(f.tw);
         q.edge = f.edge;
         q.post = (float)(term / f.fft_term);
-        const size_t plane = sizeof(float2) * (size_t)g.ny * g.nz, slab = sizeof(float2) * (size_t)g.nx * g.nz;
-        k_fft_plane_fwd<<<g.nx, kFThreads, plane, c->stream>>>(q);
-        k_fft_columns<<<g.ny, kFThreads, slab, c->stream>>>(q);
-        k_fft_plane_inv<<<g.nx, kFThreads, plane, c->stream>>>(q);
+        if (f.fft128) {
+            k_fft128_plane_fwd<<<kF128, kFThreads, kF128Smem, c->stream>>>(q);
+            k_fft128_columns<<<kF128, kFThreads, kF128Smem, c->stream>>>(q);
+            k_fft128_plane_inv<<<kF128, kFThreads, kF128Smem, c->stream>>>(q);
+        } else {
+            const size_t plane = sizeof(float2) * (size_t)g.ny * g.nz, slab = sizeof(float2) * (size_t)g.nx * g.nz;
+            k_fft_plane_fwd<<<g.nx, kFThreads, plane, c->stream>>>(q);
+            k_fft_columns<<<g.ny, kFThreads, slab, c->stream>>>(q);
+            k_fft_plane_inv<<<g.nx, kFThreads, plane, c->stream>>>(q);
+        }
         HV_CUDA(cudaGetLastError());
         a.edge = f.edge;
     }
