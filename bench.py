@@ -333,12 +333,13 @@ def adjoint_cases(args, local):
     10-25 MeV with respect to (t0, t3, sigma, a_sym), for 40Ca with 1000 test
     particles per nucleon (32^3, h = 1 fm) and 208Pb with 500 (64^3, h =
     0.5 fm), dt = 0.5 fm/c, args.adjoint_steps steps (1000), checkpoints every
-    50 steps, FP64 plain path with the deterministic deposit.  Per case: the
-    plain forward run, the checkpointed forward and the backward pass (host
-    wall time around the synchronous calls), their ratio -- the cost against
-    a forward run of the same precision and path -- and the same against the
-    fused FP32 forward of that case.  For 208Pb, a central-difference check
-    (relative step 1e-3, SOR to 1e-12 so that its stopping rule adds no
+    50 steps, FP64 with the deterministic deposit, on both paths.  Per case
+    and path: the forward run, the checkpointed forward and the backward pass
+    (host wall time around the synchronous calls) and their ratio -- the cost
+    against a forward run of the same precision and path; the fused FP64
+    adjoint's gradient against the plain one's, and both against the fused
+    FP32 forward of that case.  For 208Pb, central-difference checks of both
+    paths (relative step 1e-3, SOR to 1e-12 so that its stopping rule adds no
     noise) over args.adjoint_fd_steps steps."""
     from dataclasses import replace
 
@@ -383,12 +384,42 @@ def adjoint_cases(args, local):
             J, dJ = objective_grad(obs, w, steps)
             grad, _ = s.adjoint_backward(dJ, theta)
             t2 = time.perf_counter()
+            _, plain_adj_its, _ = s.adjoint_stats()
+        # the fused FP64 path: its forward, then its adjoint
+        with hv.Session.from_workload(w, hv.HV_F64, device=local) as s:
+            s.upload_particles(*parts)
+            s.run(1, hv.HV_PATH_FUSED)
+            t0f = time.perf_counter()
+            s.run(steps, hv.HV_PATH_FUSED)
+            fused64 = time.perf_counter() - t0f
+        with hv.Session.from_workload(w, hv.HV_F64, device=local) as s:
+            s.upload_particles(*parts)
+            s.run(0, hv.HV_PATH_FUSED)
+            t3 = time.perf_counter()
+            obs_f = s.adjoint_forward(steps, every, hv.HV_PATH_FUSED)
+            t4 = time.perf_counter()
+            Jf, dJf = objective_grad(obs_f, w, steps)
+            grad_f, _ = s.adjoint_backward(dJf, theta)
+            t5 = time.perf_counter()
+            _, fused_adj_its, fused_unconv = s.adjoint_stats()
+        gscale = float(np.max(np.abs(grad)))
         out[key] = {"workload": f"{w.Z + w.N} nucleons x {w.ppn} test particles ({w.particles}), {w.n}^3 at "
                                 f"h {w.h} fm, dt {w.dt} fm/c",
                     "objective_value": J, "plain_forward_s": plain, "checkpointed_forward_s": t1 - t0,
                     "backward_s": t2 - t1, "gradient_over_forward": (t2 - t0) / plain,
+                    "adjoint_sor_iterations_per_step": plain_adj_its / steps,
                     "fused_f32_forward_s": fused, "gradient_over_fused_f32_forward": (t2 - t0) / fused,
-                    "grad_t0_t3_sigma_asym": [float(v) for v in grad]}
+                    "grad_t0_t3_sigma_asym": [float(v) for v in grad],
+                    "fused_f64": {
+                        "objective_value": Jf, "forward_s": fused64, "checkpointed_forward_s": t4 - t3,
+                        "backward_s": t5 - t4, "gradient_over_forward": (t5 - t3) / fused64,
+                        "gradient_over_fused_f32_forward": (t5 - t3) / fused,
+                        "speedup_over_plain_gradient": (t2 - t0) / (t5 - t3),
+                        "adjoint_sor_iterations_per_step": fused_adj_its / steps,
+                        "adjoint_sor_unconverged": fused_unconv,
+                        "grad_t0_t3_sigma_asym": [float(v) for v in grad_f],
+                        "max_abs_diff_from_plain_gradient_over_max": (float(np.max(np.abs(grad_f - grad))) / gscale
+                                                                      if gscale > 0 else None)}}
     # central differences on 208Pb over fewer steps
     fd_steps = args.adjoint_fd_steps
     if fd_steps > 0:
@@ -396,29 +427,31 @@ def adjoint_cases(args, local):
         w = replace(cases["pb208_104k_64"], sor_tol=1e-12)
         parts = hv.workload_particles(w, np.float64)
         theta = np.array([w.t0, w.t3, w.sigma, w.a_sym])
-        run = AdjointRun(w, parts, fd_steps, checkpoint_every=every, device=local)
 
         def fn(dd):
             d = torch.tensor(dd, dtype=torch.float64)
             return float(power_in_band(d, np.arange(fd_steps) * w.dt, fd_steps * w.dt, w.dt))
-        try:
-            run.forward(theta)
-            _, dJ = objective_grad(run.obs, w, fd_steps)
-            g_adj = run.backward(dJ)
-            g_fd = np.zeros(4)
-            for i in range(4):
-                hstep = 1e-3 * abs(theta[i])
-                tp, tm = theta.copy(), theta.copy()
-                tp[i] += hstep
-                tm[i] -= hstep
-                g_fd[i] = (run.objective(tp, fn) - run.objective(tm, fn)) / (2 * hstep)
-        finally:
-            run.close()
-        scale = float(np.max(np.abs(g_fd)))
-        out["pb208_104k_64_central_differences"] = {
-            "steps": fd_steps, "relative_step": 1e-3, "sor_tol": 1e-12, "adjoint": [float(v) for v in g_adj],
-            "finite_differences": [float(v) for v in g_fd],
-            "max_abs_diff_over_max_abs_fd": float(np.max(np.abs(g_adj - g_fd))) / scale if scale > 0 else None}
+        for name, path in (("pb208_104k_64_central_differences", hv.HV_PATH_PLAIN),
+                           ("pb208_104k_64_central_differences_fused_f64", hv.HV_PATH_FUSED)):
+            run = AdjointRun(w, parts, fd_steps, checkpoint_every=every, device=local, path=path)
+            try:
+                run.forward(theta)
+                _, dJ = objective_grad(run.obs, w, fd_steps)
+                g_adj = run.backward(dJ)
+                g_fd = np.zeros(4)
+                for i in range(4):
+                    hstep = 1e-3 * abs(theta[i])
+                    tp, tm = theta.copy(), theta.copy()
+                    tp[i] += hstep
+                    tm[i] -= hstep
+                    g_fd[i] = (run.objective(tp, fn) - run.objective(tm, fn)) / (2 * hstep)
+            finally:
+                run.close()
+            scale = float(np.max(np.abs(g_fd)))
+            out[name] = {
+                "steps": fd_steps, "relative_step": 1e-3, "sor_tol": 1e-12, "adjoint": [float(v) for v in g_adj],
+                "finite_differences": [float(v) for v in g_fd],
+                "max_abs_diff_over_max_abs_fd": float(np.max(np.abs(g_adj - g_fd))) / scale if scale > 0 else None}
     return out
 
 

@@ -78,11 +78,13 @@ __global__ void k_adj_gather_field(Geom g, int protons, int total, const double 
 
 // Position adjoint of the CIC weights of gather and deposit:
 // lam_x(p) += sum_c grad w_c(x_p) [ F(c) . lam_f(p) + lam_raw(c) ].
+// The force field is read at Fx[fs id] (fs 1: separate arrays; 4: the fused
+// path's interleaved (Fx, Fy, Fz, 0) per node).
 __global__ void k_adj_weights(Geom g, int protons, int total, const double *__restrict__ x,
                               const double *__restrict__ y, const double *__restrict__ z,
                               const double *__restrict__ lfx, const double *__restrict__ lfy,
                               const double *__restrict__ lfz, const double *__restrict__ Fx,
-                              const double *__restrict__ Fy, const double *__restrict__ Fz,
+                              const double *__restrict__ Fy, const double *__restrict__ Fz, long long fs,
                               const double *__restrict__ lraw, double *lx, double *ly, double *lz) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -105,7 +107,7 @@ __global__ void k_adj_weights(Geom g, int protons, int total, const double *__re
             for (int cc = 0; cc < 2; cc++) {
                 if (x0 + a >= nx || y0 + b >= ny || z0 + cc >= nz) continue;
                 const long long id = off + (x0 + a) * sx + (y0 + b) * sy + z0 + cc;
-                const double v = Fx[id] * fx + Fy[id] * fy + Fz[id] * fz + lraw[id];
+                const double v = Fx[fs * id] * fx + Fy[fs * id] * fy + Fz[fs * id] * fz + lraw[id];
                 ax += gxw[a] * wy[b] * wz[cc] * v;
                 ay += wx[a] * gyw[b] * wz[cc] * v;
                 az += wx[a] * wy[b] * gzw[cc] * v;
@@ -221,11 +223,17 @@ __global__ void k_scale3d(int total, double f, double *a0, double *a1, double *a
 // Device buffers and checkpoints of one adjoint run.
 struct Adjoint {
     int steps = 0, every = 0, nseg = 0, cap_steps = 0, cap_every = 0;
-    // checkpoints: [nseg + 1] x (9 N particle state + G phi); the last is the final state
+    hv_step_path path = HV_PATH_PLAIN, cap_path = HV_PATH_PLAIN;  // the forward's path; the buffers' layout
+    // checkpoints: [nseg + 1] x (9 N particle state + G phi) on the plain path;
+    // the fused path adds phi's two earlier solutions (the extrapolated start),
+    // the interleaved force field (8 G) and the smoothed density (2 G); the
+    // last checkpoint is the final state
     double *ckpt = nullptr;
-    std::vector<int> ck_step;
+    int *ck_ctl = nullptr;   // fused path: [nseg + 1] x the fused control words
+    std::vector<int> ck_step, ck_mhint;
     std::vector<char> ck_excited, ck_boundary;
-    // per-step data of a recomputed segment: [every] x (3 N positions + 6 G forces + 2 G density)
+    // per-step data of a recomputed segment: [every] x (3 N positions + the
+    // force field (6 G separate, or 8 G interleaved on the fused path) + 2 G density)
     double *seg = nullptr;
     // adjoints of the particle state (9 N: x, k, f) and grid work arrays
     double *lam = nullptr;
@@ -235,39 +243,52 @@ struct Adjoint {
     double *Lraw = nullptr;  // 2G
     double *src = nullptr;   // G
     double *mu = nullptr;    // G, zero on the boundary
+    double *mu_hist = nullptr;  // fused path: 2 G, mu's two earlier solutions
+    int *actl = nullptr;     // fused path: the transposed solves' control words (8) and counts (2)
     double *partials = nullptr;
     double *acc = nullptr;   // 4: dJ/d(A, B, gamma, C)
     // the slot-to-caller permutation of the checkpointed particle state (the
-    // plain steps of a forward run keep the slot order, so one copy serves all
+    // steps of a forward run keep the slot order, so one copy serves all
     // checkpoints); restored with them, since a fused run between forward and
     // backward may re-sort the slots
     int *perm = nullptr;
     bool permuted = false;
     int nb_sky = 0;
     int adj_sor_its = 0;     // iterations of the transposed solves of the last backward pass
+    int adj_sor_unconverged = 0;  // of those solves, the ones that stopped at max_iter
     bool ready = false;      // a forward run's checkpoints are held
 };
 
 void adjoint_release(hv_ctx *c) {
     Adjoint *a = c->adjoint;
     if (!a) return;
-    double *bufs[] = {a->ckpt, a->seg, a->lam, a->LF, a->LU, a->Lrho, a->Lraw, a->src, a->mu, a->partials, a->acc};
+    double *bufs[] = {a->ckpt, a->seg, a->lam, a->LF, a->LU, a->Lrho, a->Lraw, a->src, a->mu, a->mu_hist,
+                      a->partials, a->acc};
     for (double *p : bufs)
         if (p) cudaFree(p);
-    if (a->perm) cudaFree(a->perm);
+    int *ibufs[] = {a->perm, a->ck_ctl, a->actl};
+    for (int *p : ibufs)
+        if (p) cudaFree(p);
     delete a;
     c->adjoint = nullptr;
 }
 
 namespace {
 
-size_t ck_stride(const hv_ctx *c) { return (size_t)9 * c->total + (size_t)c->geom.G; }
-size_t seg_stride(const hv_ctx *c) { return (size_t)3 * c->total + (size_t)8 * c->geom.G; }
+bool fused_layout(hv_step_path p) { return p == HV_PATH_FUSED; }
+size_t ck_stride(const hv_ctx *c, hv_step_path p) {
+    return (size_t)9 * c->total + (size_t)(fused_layout(p) ? 13 : 1) * c->geom.G;
+}
+size_t seg_stride(const hv_ctx *c, hv_step_path p) {
+    return (size_t)3 * c->total + (size_t)(fused_layout(p) ? 10 : 8) * c->geom.G;
+}
 
-hv_status adjoint_alloc(hv_ctx *c, int steps, int every) {
+hv_status adjoint_alloc(hv_ctx *c, int steps, int every, hv_step_path path) {
     const int nseg = (steps + every - 1) / every;
     Adjoint *a = c->adjoint;
-    if (a && a->cap_every >= every && (a->cap_steps + a->cap_every - 1) / a->cap_every >= nseg) return HV_OK;
+    if (a && a->cap_path == path && a->cap_every >= every &&
+        (a->cap_steps + a->cap_every - 1) / a->cap_every >= nseg)
+        return HV_OK;
     adjoint_release(c);
     a = c->adjoint = new Adjoint();
     const size_t N = c->total, G = c->geom.G;
@@ -278,8 +299,15 @@ hv_status adjoint_alloc(hv_ctx *c, int steps, int every) {
         }
         return HV_OK;
     };
-    HV_TRY(alloc(&a->ckpt, ck_stride(c) * (nseg + 1)));
-    HV_TRY(alloc(&a->seg, seg_stride(c) * every));
+    auto alloci = [&](int **p, size_t n) -> hv_status {
+        if (cudaMalloc((void **)p, sizeof(int) * (n > 0 ? n : 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return HV_ERR_OOM;
+        }
+        return HV_OK;
+    };
+    HV_TRY(alloc(&a->ckpt, ck_stride(c, path) * (nseg + 1)));
+    HV_TRY(alloc(&a->seg, seg_stride(c, path) * every));
     HV_TRY(alloc(&a->lam, 9 * N));
     HV_TRY(alloc(&a->LF, 6 * G));
     HV_TRY(alloc(&a->LU, 2 * G));
@@ -290,31 +318,53 @@ hv_status adjoint_alloc(hv_ctx *c, int steps, int every) {
     a->nb_sky = 2 * c->sm_count;
     HV_TRY(alloc(&a->partials, 4 * (size_t)a->nb_sky));
     HV_TRY(alloc(&a->acc, 4));
-    if (cudaMalloc((void **)&a->perm, sizeof(int) * (N > 0 ? N : 1)) != cudaSuccess) {
-        cudaGetLastError();
-        return HV_ERR_OOM;
+    HV_TRY(alloci(&a->perm, N));
+    if (fused_layout(path)) {
+        HV_TRY(alloc(&a->mu_hist, 2 * G));
+        HV_TRY(alloci(&a->ck_ctl, (size_t)fused_ctl_words() * (nseg + 1)));
+        HV_TRY(alloci(&a->actl, 10));
     }
     a->cap_steps = steps;
     a->cap_every = every;
+    a->cap_path = path;
     return HV_OK;
 }
 
-// Particle state (x..kz, fx..fz) and phi to / from checkpoint slot s.
+// Particle state (x..kz, fx..fz) and phi to / from checkpoint slot s; on the
+// fused path also phi's history, the interleaved forces, the smoothed density
+// and the control words, so that a recomputed segment repeats the forward's
+// steps.
 hv_status save_ckpt(hv_ctx *c, int s) {
     Adjoint *a = c->adjoint;
     State<double> &st = c->d64;
     const size_t N = c->total, G = c->geom.G;
-    double *dst = a->ckpt + ck_stride(c) * s;
+    const bool fz = fused_layout(a->path);
+    double *dst = a->ckpt + ck_stride(c, a->path) * s;
     double *src[9] = {st.x, st.y, st.z, st.kx, st.ky, st.kz, st.fx, st.fy, st.fz};
     for (int k = 0; k < 9; k++)
         if (N) HV_CUDA(cudaMemcpyAsync(dst + k * N, src[k], sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
-    HV_CUDA(cudaMemcpyAsync(dst + 9 * N, st.phi, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+    double *g = dst + 9 * N;
+    if (!fz) {
+        HV_CUDA(cudaMemcpyAsync(g, st.phi, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        const Fused &f = c->fused;
+        HV_CUDA(cudaMemcpyAsync(g, f.phi64, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(g + G, f.phi64_prev, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(g + 2 * G, f.phi64_prev2, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(g + 3 * G, f.F4, sizeof(double) * 8 * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(g + 11 * G, st.rho, sizeof(double) * 2 * G, cudaMemcpyDeviceToDevice, c->stream));
+        const int nw = fused_ctl_words();
+        HV_CUDA(cudaMemcpyAsync(a->ck_ctl + (size_t)nw * s, fused_ctl(c), sizeof(int) * nw, cudaMemcpyDeviceToDevice,
+                                c->stream));
+    }
     if ((int)a->ck_step.size() <= s) {
         a->ck_step.resize(s + 1);
+        a->ck_mhint.resize(s + 1);
         a->ck_excited.resize(s + 1);
         a->ck_boundary.resize(s + 1);
     }
     a->ck_step[s] = c->step_index;
+    a->ck_mhint[s] = c->fused.m_hint;
     a->ck_excited[s] = c->excited;
     a->ck_boundary[s] = c->boundary_set;
     return HV_OK;
@@ -324,11 +374,29 @@ hv_status load_ckpt(hv_ctx *c, int s) {
     Adjoint *a = c->adjoint;
     State<double> &st = c->d64;
     const size_t N = c->total, G = c->geom.G;
-    const double *src = a->ckpt + ck_stride(c) * s;
+    const bool fz = fused_layout(a->path);
+    const double *src = a->ckpt + ck_stride(c, a->path) * s;
     double *dst[9] = {st.x, st.y, st.z, st.kx, st.ky, st.kz, st.fx, st.fy, st.fz};
     for (int k = 0; k < 9; k++)
         if (N) HV_CUDA(cudaMemcpyAsync(dst[k], src + k * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
-    HV_CUDA(cudaMemcpyAsync(st.phi, src + 9 * N, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+    const double *g = src + 9 * N;
+    if (!fz) {
+        HV_CUDA(cudaMemcpyAsync(st.phi, g, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        Fused &f = c->fused;
+        HV_CUDA(cudaMemcpyAsync(f.phi64, g, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(f.phi64_prev, g + G, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(f.phi64_prev2, g + 2 * G, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(f.F4, g + 3 * G, sizeof(double) * 8 * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(st.rho, g + 11 * G, sizeof(double) * 2 * G, cudaMemcpyDeviceToDevice, c->stream));
+        // the plain view of phi, as a fused run's end leaves it
+        HV_CUDA(cudaMemcpyAsync(st.phi, g, sizeof(double) * G, cudaMemcpyDeviceToDevice, c->stream));
+        const int nw = fused_ctl_words();
+        HV_CUDA(cudaMemcpyAsync(fused_ctl(c), a->ck_ctl + (size_t)nw * s, sizeof(int) * nw, cudaMemcpyDeviceToDevice,
+                                c->stream));
+        f.f4_current = true;
+        f.m_hint = a->ck_mhint[s];
+    }
     if (N) HV_CUDA(cudaMemcpyAsync(c->perm, a->perm, sizeof(int) * N, cudaMemcpyDeviceToDevice, c->stream));
     c->permuted = a->permuted;
     c->step_index = a->ck_step[s];
@@ -340,11 +408,18 @@ hv_status load_ckpt(hv_ctx *c, int s) {
 // Positions, forces and smoothed density after a step, into segment slot j.
 hv_status save_slot(hv_ctx *c, int j) {
     State<double> &st = c->d64;
+    const hv_step_path path = c->adjoint->path;
     const size_t N = c->total, G = c->geom.G;
-    double *d = c->adjoint->seg + seg_stride(c) * j;
+    double *d = c->adjoint->seg + seg_stride(c, path) * j;
     const double *src3[3] = {st.x, st.y, st.z};
     for (int k = 0; k < 3; k++)
         if (N) HV_CUDA(cudaMemcpyAsync(d + k * N, src3[k], sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+    if (fused_layout(path)) {
+        HV_CUDA(cudaMemcpyAsync(d + 3 * N, c->fused.F4, sizeof(double) * 8 * G, cudaMemcpyDeviceToDevice, c->stream));
+        HV_CUDA(cudaMemcpyAsync(d + 3 * N + 8 * G, st.rho, sizeof(double) * 2 * G, cudaMemcpyDeviceToDevice,
+                                c->stream));
+        return HV_OK;
+    }
     const double *srcF[4] = {st.Fx, st.Fy, st.Fz, st.rho};
     for (int k = 0; k < 4; k++)
         HV_CUDA(cudaMemcpyAsync(d + 3 * N + k * 2 * G, srcF[k], sizeof(double) * 2 * G, cudaMemcpyDeviceToDevice,
@@ -354,13 +429,28 @@ hv_status save_slot(hv_ctx *c, int j) {
 
 // lam_x += dforce(x)^T lam_f at the point stored in slot j; the parameter
 // derivatives are added to acc.
+// After a transposed solve on the persistent kernel: its iterations and
+// whether it stopped unconverged, added to cnt[0] and cnt[1] (status words:
+// [1] iterations, [2] converged).
+__global__ void k_adj_sor_count(const int *__restrict__ status, int *cnt) {
+    if (threadIdx.x == 0) {
+        cnt[0] += status[1];
+        cnt[1] += status[2] ? 0 : 1;
+    }
+}
+
 hv_status force_adjoint(hv_ctx *c, int j) {
     Adjoint *a = c->adjoint;
     const Geom &g = c->geom;
     const size_t N = c->total, G = g.G;
-    const double *d = a->seg + seg_stride(c) * j;
+    const bool fz = fused_layout(a->path);
+    const double *d = a->seg + seg_stride(c, a->path) * j;
     const double *x = d, *y = d + N, *z = d + 2 * N;
-    const double *Fx = d + 3 * N, *Fy = Fx + 2 * G, *Fz = Fy + 2 * G, *rho = Fz + 2 * G;
+    // the force field: separate arrays, or (Fx, Fy, Fz, 0) per node
+    const double *F = d + 3 * N;
+    const double *Fx = F, *Fy = fz ? F + 1 : F + 2 * G, *Fz = fz ? F + 2 : F + 4 * G;
+    const long long fs = fz ? 4 : 1;
+    const double *rho = fz ? F + 8 * G : F + 6 * G;
     double *lx = a->lam, *ly = lx + N, *lz = ly + N;
     const double *lf = a->lam + 6 * N;
     double *LFx = a->LF, *LFy = LFx + 2 * G, *LFz = LFy + 2 * G;
@@ -381,19 +471,83 @@ hv_status force_adjoint(hv_ctx *c, int j) {
     const double cc = 4.0 * kPi * kE2;
     k_adj_coulomb_src<<<nblocks(G), kBlock, 0, c->stream>>>((long long)G, 1.0 / cc, a->LU, a->src);
     HV_CUDA(cudaGetLastError());
-    int its = 0;
-    double metric = 0.0;
-    hv_status st = launch_sor_plain<double>(c, a->mu, a->src, &its, &metric);
-    if (st != HV_OK && st != HV_ERR_NOT_CONVERGED) return st;
-    a->adj_sor_its += its;
+    if (fz) {
+        // on the persistent kernel, started from the extrapolation of the
+        // previous reversed steps' mu; counted on the device
+        HV_TRY(sor_fast_launch_adjoint(c, a->src, a->mu, a->mu_hist, a->mu_hist + G, a->actl));
+        k_adj_sor_count<<<1, 32, 0, c->stream>>>(sor_fast_status_words(c), a->actl + 8);
+    } else {
+        int its = 0;
+        double metric = 0.0;
+        hv_status st = launch_sor_plain<double>(c, a->mu, a->src, &its, &metric);
+        if (st != HV_OK && st != HV_ERR_NOT_CONVERGED) return st;
+        a->adj_sor_its += its;
+        if (st == HV_ERR_NOT_CONVERGED) a->adj_sor_unconverged++;
+    }
     k_adj_coulomb_add<<<nblocks(G), kBlock, 0, c->stream>>>((long long)G, cc, a->mu, a->Lrho);
     // smoothing^T = smoothing
     HV_TRY(launch_smooth<double>(c, a->Lrho, a->Lraw));
     // deposit^T and gather^T in the positions
     if (N)
         k_adj_weights<<<nblocks(N), kBlock, 0, c->stream>>>(g, c->protons, c->total, x, y, z, lf, lf + N, lf + 2 * N,
-                                                           Fx, Fy, Fz, a->Lraw, lx, ly, lz);
+                                                           Fx, Fy, Fz, fs, a->Lraw, lx, ly, lz);
     HV_CUDA(cudaGetLastError());
+    return HV_OK;
+}
+
+// Slot re-sorting paused while an adjoint pass runs fused steps: the adjoint
+// state is indexed by particle slot, so every step of a forward run and of its
+// backward pass must see one slot order.
+struct SortPause {
+    hv_ctx *c;
+    int saved;
+    explicit SortPause(hv_ctx *c_) : c(c_), saved(c_->fast.sort_every) { c->fast.sort_every = 0; }
+    ~SortPause() { c->fast.sort_every = saved; }
+};
+
+// The persistent solver's error word after a stretch of fused steps and
+// transposed solves (synchronous): a bounded wait that ran out leaves the
+// fused copies and the fields stale.
+hv_status fused_pass_status(hv_ctx *c) {
+    int st0 = 0;
+    HV_CUDA(cudaMemcpyAsync(&st0, sor_fast_status_words(c), sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HV_CUDA(cudaStreamSynchronize(c->stream));
+    if (!st0) return HV_OK;
+    c->fields_valid = false;
+    fused_invalidate(c);
+    set_last_error("SOR: a bounded device-side wait timed out");
+    return HV_ERR_TIMEOUT;
+}
+
+// The forward run on the fused FP64 path: one hv_run(HV_PATH_FUSED) per
+// segment, with a checkpoint before each and the final state after the last.
+hv_status forward_fused(hv_ctx *c, int n_steps, hv_observables *obs) {
+    Adjoint *a = c->adjoint;
+    // forces and phi into the fused buffers, the solution history cleared
+    HV_TRY(fused_adjoint_begin(c, 0));
+    for (int sgi = 0; sgi < a->nseg; sgi++) {
+        const int s0 = sgi * a->every, k = std::min(a->every, n_steps - s0);
+        HV_TRY(save_ckpt(c, sgi));
+        HV_TRY(fused_run(c, k, obs ? obs + s0 : nullptr));
+    }
+    return save_ckpt(c, a->nseg);
+}
+
+// Recomputes steps s0..s1-1 from the checkpoint the context holds, keeping
+// what the reversed steps need.
+hv_status recompute_segment(hv_ctx *c, int s0, int s1) {
+    if (fused_layout(c->adjoint->path)) {
+        HV_TRY(fused_adjoint_begin(c, s1 - s0));
+        for (int n = s0; n < s1; n++) {
+            HV_TRY(fused_adjoint_step(c));
+            HV_TRY(save_slot(c, n - s0));
+        }
+        return HV_OK;
+    }
+    for (int n = s0; n < s1; n++) {
+        HV_TRY(plain_step_f64(c, nullptr));
+        HV_TRY(save_slot(c, n - s0));
+    }
     return HV_OK;
 }
 
@@ -404,31 +558,54 @@ using namespace hv;
 
 extern "C" {
 
-hv_status hv_adjoint_forward(hv_ctx *c, int n_steps, int checkpoint_every, hv_observables *obs) {
+hv_status hv_adjoint_forward_path(hv_ctx *c, int path, int n_steps, int checkpoint_every, hv_observables *obs) {
     if (!c || n_steps < 1 || checkpoint_every < 1) return HV_ERR_BAD_ARG;
+    if (path != HV_PATH_PLAIN && path != HV_PATH_FUSED) return HV_ERR_BAD_ARG;
     if (c->prec != HV_F64) return HV_ERR_UNSUPPORTED;
     HV_CUDA(cudaSetDevice(c->device));
-    if (!c->fields_valid) HV_TRY(hv_initial_solve(c, nullptr));
+    const hv_step_path p = (hv_step_path)path;
+    if (p == HV_PATH_FUSED) {
+        // the fused path solves missing fields with its own kernels
+        if (!c->fields_valid) HV_TRY(fused_run(c, 0, nullptr));
+        hv_status st = fused_prepare(c);
+        if (st != HV_OK) {
+            fused_release(c);
+            return st;
+        }
+    } else if (!c->fields_valid) {
+        HV_TRY(hv_initial_solve(c, nullptr));
+    }
     fused_invalidate(c);
     const int every = checkpoint_every < n_steps ? checkpoint_every : n_steps;
-    HV_TRY(adjoint_alloc(c, n_steps, every));
+    if (c->adjoint) c->adjoint->ready = false;
+    HV_TRY(adjoint_alloc(c, n_steps, every, p));
     Adjoint *a = c->adjoint;
     a->ready = false;
+    a->path = p;
     a->steps = n_steps;
     a->every = every;
     a->nseg = (n_steps + every - 1) / every;
     if (c->total) HV_CUDA(cudaMemcpyAsync(a->perm, c->perm, sizeof(int) * c->total, cudaMemcpyDeviceToDevice, c->stream));
     a->permuted = c->permuted;
-    for (int n = 0; n < n_steps; n++) {
-        if (n % every == 0) HV_TRY(save_ckpt(c, n / every));
-        hv_observables *row = obs ? &obs[n] : nullptr;
-        if (row) std::memset(row, 0, sizeof(*row));
-        HV_TRY(plain_step_f64(c, row));
+    if (p == HV_PATH_FUSED) {
+        SortPause pause(c);
+        HV_TRY(forward_fused(c, n_steps, obs));
+    } else {
+        for (int n = 0; n < n_steps; n++) {
+            if (n % every == 0) HV_TRY(save_ckpt(c, n / every));
+            hv_observables *row = obs ? &obs[n] : nullptr;
+            if (row) std::memset(row, 0, sizeof(*row));
+            HV_TRY(plain_step_f64(c, row));
+        }
+        HV_TRY(save_ckpt(c, a->nseg));  // the final state, restored after a backward pass
     }
-    HV_TRY(save_ckpt(c, a->nseg));  // the final state, restored after a backward pass
     HV_CUDA(cudaStreamSynchronize(c->stream));
     a->ready = true;
     return HV_OK;
+}
+
+hv_status hv_adjoint_forward(hv_ctx *c, int n_steps, int checkpoint_every, hv_observables *obs) {
+    return hv_adjoint_forward_path(c, HV_PATH_PLAIN, n_steps, checkpoint_every, obs);
 }
 
 hv_status hv_adjoint_backward(hv_ctx *c, const double *dJ_dD, const double theta[4], double grad_theta[4],
@@ -438,6 +615,8 @@ hv_status hv_adjoint_backward(hv_ctx *c, const double *dJ_dD, const double theta
     Adjoint *a = c->adjoint;
     if (!a || !a->ready) return HV_ERR_BAD_ARG;
     HV_CUDA(cudaSetDevice(c->device));
+    const bool fz = fused_layout(a->path);
+    SortPause pause(c);
     fused_invalidate(c);
     const size_t N = c->total, G = c->geom.G;
     const double dt = c->params.dt;
@@ -448,16 +627,22 @@ hv_status hv_adjoint_backward(hv_ctx *c, const double *dJ_dD, const double theta
     HV_CUDA(cudaMemsetAsync(a->lam, 0, sizeof(double) * 9 * (N ? N : 1), c->stream));
     HV_CUDA(cudaMemsetAsync(a->mu, 0, sizeof(double) * G, c->stream));
     HV_CUDA(cudaMemsetAsync(a->acc, 0, sizeof(double) * 4, c->stream));
+    if (fz) {
+        // the transposed solves' control words: no earlier solution held, a
+        // first cycle of 8 iterations; their iteration and unconverged counts
+        const int h_ctl[10] = {0, 8, 0, 0, 0, 0, 0, 0, 0, 0};
+        HV_CUDA(cudaMemsetAsync(a->mu_hist, 0, sizeof(double) * 2 * G, c->stream));
+        HV_CUDA(cudaMemcpyAsync(a->actl, h_ctl, sizeof(h_ctl), cudaMemcpyHostToDevice, c->stream));
+        HV_CUDA(cudaStreamSynchronize(c->stream));
+    }
     a->adj_sor_its = 0;
+    a->adj_sor_unconverged = 0;
     const int nbp = nblocks(N);
     for (int sgi = a->nseg - 1; sgi >= 0; sgi--) {
         const int s0 = sgi * a->every, s1 = std::min(s0 + a->every, a->steps);
         // recompute the segment, keeping what the reversed steps need
         HV_TRY(load_ckpt(c, sgi));
-        for (int n = s0; n < s1; n++) {
-            HV_TRY(plain_step_f64(c, nullptr));
-            HV_TRY(save_slot(c, n - s0));
-        }
+        HV_TRY(recompute_segment(c, s0, s1));
         for (int n = s1 - 1; n >= s0; n--) {
             if (!N) continue;
             k_axpy3d<<<nbp, kBlock, 0, c->stream>>>(c->total, ka, lfx, lfy, lfz, lkx, lky, lkz);
@@ -469,20 +654,34 @@ hv_status hv_adjoint_backward(hv_ctx *c, const double *dJ_dD, const double theta
             k_scale3d<<<nbp, kBlock, 0, c->stream>>>(c->total, ka, lfx, lfy, lfz, lkx, lky, lkz);
             HV_CUDA(cudaGetLastError());
         }
+        if (fz) HV_TRY(fused_pass_status(c));
     }
     // the forces of the starting state were solved from theta too
     HV_TRY(load_ckpt(c, 0));
-    int its = 0;
-    hv_status st = plain_fields_f64(c, &its);
-    if (st != HV_OK && st != HV_ERR_NOT_CONVERGED) return st;
-    HV_TRY(save_slot(c, 0));
+    if (fz) {
+        // checkpoint 0 holds the forces and smoothed density of x_0
+        HV_TRY(save_slot(c, 0));
+    } else {
+        int its = 0;
+        hv_status st = plain_fields_f64(c, &its);
+        if (st != HV_OK && st != HV_ERR_NOT_CONVERGED) return st;
+        HV_TRY(save_slot(c, 0));
+    }
     if (N) HV_TRY(force_adjoint(c, 0));
     double acc[4];
+    int cnt[2] = {0, 0};
     HV_CUDA(cudaMemcpyAsync(acc, a->acc, sizeof(acc), cudaMemcpyDeviceToHost, c->stream));
+    if (fz) HV_CUDA(cudaMemcpyAsync(cnt, a->actl + 8, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    if (fz) HV_TRY(fused_pass_status(c));
     // back to the state the forward run ended in
     HV_TRY(load_ckpt(c, a->nseg));
     HV_CUDA(cudaStreamSynchronize(c->stream));
+    if (fz) {
+        a->adj_sor_its = cnt[0];
+        a->adj_sor_unconverged = cnt[1];
+    }
     c->fields_valid = false;
+    fused_invalidate(c);
     // (A, B, gamma, C) -> (t0, t3, sigma, a_sym), the map of hv_skyrme_from_t0t3
     const double t3 = theta[1], sg = theta[2];
     const double r0s = std::pow(kRho0, sg + 1.0);
@@ -496,6 +695,15 @@ hv_status hv_adjoint_backward(hv_ctx *c, const double *dJ_dD, const double theta
         grad_skyrme[2] = acc[3];
         grad_skyrme[3] = acc[2];
     }
+    return HV_OK;
+}
+
+hv_status hv_adjoint_stats(const hv_ctx *c, int *path, int *adjoint_sor_iterations, int *adjoint_sor_unconverged) {
+    if (!c || !c->adjoint) return HV_ERR_BAD_ARG;
+    const Adjoint *a = c->adjoint;
+    if (path) *path = a->path;
+    if (adjoint_sor_iterations) *adjoint_sor_iterations = a->adj_sor_its;
+    if (adjoint_sor_unconverged) *adjoint_sor_unconverged = a->adj_sor_unconverged;
     return HV_OK;
 }
 

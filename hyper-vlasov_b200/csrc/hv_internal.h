@@ -280,6 +280,24 @@ hv_status fused_batch_rows(hv_ctx *c, cudaStream_t s, int s0, int k, hv_observab
 hv_status fused_batch_end(hv_ctx *c, int n_steps, int exc);
 void fused_batch_sor_inputs(hv_ctx *c, const float **rho, int **ctl, int **its_ring, int *ring);
 void adjoint_release(hv_ctx *c);
+// fused FP64 steps one at a time for the adjoint (k_fused.cu): the control
+// words set for n_steps steps from the context's step (forces and phi packed
+// from the plain buffers first when stale; synchronous), then one step per
+// call (stream-ordered).  fused_ctl: the device control words, fused_ctl_words
+// of them.
+hv_status fused_adjoint_begin(hv_ctx *c, int n_steps);
+hv_status fused_adjoint_step(hv_ctx *c);
+int *fused_ctl(hv_ctx *c);
+int fused_ctl_words();
+// A double solve of lap mu = -4 pi e^2 src with mu's boundary nodes held (the
+// adjoint's transposed Coulomb solve), on the persistent SOR kernel with the
+// context's SOR settings, warm-started from mu and its history mu_prev,
+// mu_prev2 as the context's warm-start rule says; ctl: its own control words
+// ([1] iterations of the previous solve, [2] solutions held).  The outcome is
+// left in the solver's status words (sor_fast_status_words).
+hv_status sor_fast_launch_adjoint(hv_ctx *c, const double *src, double *mu, double *mu_prev, double *mu_prev2,
+                                  int *ctl);
+const int *sor_fast_status_words(hv_ctx *c);
 // compute_particle_densities of N particles (protons first) given by device
 // positions, into dp / dn at the same indices (pdens.cu; stream-ordered)
 template <typename T>

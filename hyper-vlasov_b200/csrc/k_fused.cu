@@ -1260,6 +1260,16 @@ void fused_batch_sor_inputs(hv_ctx *c, const float **rho, int **ctl, int **its_r
     *ring = kRing;
 }
 
+// ---- adjoint support (adjoint.cu): fused FP64 steps one at a time
+hv_status fused_adjoint_begin(hv_ctx *c, int n_steps) {
+    if (c->prec != HV_F64) return HV_ERR_UNSUPPORTED;
+    int exc = -1;
+    return run_begin<double>(c, n_steps, &exc);
+}
+hv_status fused_adjoint_step(hv_ctx *c) { return enqueue_step<double>(c); }
+int *fused_ctl(hv_ctx *c) { return ctl_of(c); }
+int fused_ctl_words() { return CTL_N; }
+
 // Marks the fused copies stale after the plain path or an upload changed the state.
 void fused_invalidate(hv_ctx *c) {
     c->fused.f4_current = false;

@@ -1839,6 +1839,24 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
     return HV_OK;
 }
 
+hv_status sor_fast_launch_adjoint(hv_ctx *c, const double *src, double *mu, double *mu_prev, double *mu_prev2,
+                                  int *ctl) {
+    if (c->prec != HV_F64) return HV_ERR_UNSUPPORTED;
+    SorFast &f = c->fused.sor;
+    SorArgs<double, double> a;
+    const int form = sor_fast_args<double>(c, src, ctl, nullptr, 0, a);
+    a.phi64 = mu;
+    a.phi64_prev = mu_prev;
+    a.phi64_prev2 = mu_prev2;
+    if (form == 0) HV_CUDA(cudaMemsetAsync(f.phase, 0, sizeof(unsigned) * (f.nblocks + 2), c->stream));
+    void *args[] = {&a};
+    HV_CUDA(cudaLaunchCooperativeKernel(sor_kernel<double, false>(form), dim3(f.nblocks), dim3(f.threads), args,
+                                        f.smem, c->stream));
+    return HV_OK;
+}
+
+const int *sor_fast_status_words(hv_ctx *c) { return c->fused.sor.status; }
+
 // ---- several float solves in one cooperative launch ------------------------
 
 hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std::vector<const float *> &rho,

@@ -180,6 +180,8 @@ SIGNATURES = {
     "hv_simulate_release": (_S, []),
     "hv_adjoint_forward": (_S, [_P, _I, _I, _P]),
     "hv_adjoint_backward": (_S, [_P, _P, _P, _P, _P]),
+    "hv_adjoint_forward_path": (_S, [_P, _I, _I, _I, _P]),
+    "hv_adjoint_stats": (_S, [_P, _P, _P, _P]),
     "hv_particle_densities": (_S, [_P, _P, _P]),
     "hv_init_params_default": (None, [_P]),
     "hv_initialize_particles": (_S, [_P, _P, _P, _P, _P, _P, _P]),

@@ -13,7 +13,10 @@ respect to theta = (t0, t3, sigma, a_sym):
     J = power_in_band(d, t, t_f, dt_row)
     J.backward()                                      # the adjoint run; theta.grad
 
-Everything runs in FP64 on the plain path (one kernel per reference routine).
+Everything runs in FP64: on the plain path (one kernel per reference routine,
+the default) or, with path=HV_PATH_FUSED, on the fused kernels (the fused
+particle step, the persistent SOR for the forward and the transposed Poisson
+solves).
 """
 from __future__ import annotations
 
@@ -31,12 +34,15 @@ class AdjointRun:
     runs the FP64 forward from the initial state with checkpoints and returns
     D(t) per step, backward(dJ/dD) the gradient at that theta."""
 
-    def __init__(self, workload: Workload, particles, steps: int, checkpoint_every: int = 50, device: int = -1):
+    def __init__(self, workload: Workload, particles, steps: int, checkpoint_every: int = 50, device: int = -1,
+                 path: int = L.HV_PATH_PLAIN, fast_options: dict | None = None):
         self.w = workload
         self.parts = [np.ascontiguousarray(p, dtype=np.float64) for p in particles]
         self.steps = int(steps)
         self.every = int(checkpoint_every)
         self.device = device
+        self.path = int(path)
+        self.fast_options = dict(fast_options or {})
         self.session = None
         self.theta = None
         self.obs = None
@@ -50,9 +56,12 @@ class AdjointRun:
         w = self.workload_at(theta)
         self.theta = np.array([w.t0, w.t3, w.sigma, w.a_sym], dtype=np.float64)
         s = Session.from_workload(w, L.HV_F64, self.device)
+        if self.fast_options:
+            s.set_fast_options(**self.fast_options)
         s.upload_particles(*self.parts)
-        s.initial_solve()
-        self.obs = s.adjoint_forward(self.steps, self.every)
+        if self.path == L.HV_PATH_PLAIN:
+            s.initial_solve()  # the fused path solves the first fields with its own kernels
+        self.obs = s.adjoint_forward(self.steps, self.every, self.path)
         self.session = s
         return self.obs["dipole"].copy()
 

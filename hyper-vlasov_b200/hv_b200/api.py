@@ -313,13 +313,22 @@ class Session:
         return obs
 
     # -- adjoint ---------------------------------------------------------------
-    def adjoint_forward(self, steps, checkpoint_every):
-        """hv_adjoint_forward: `steps` plain FP64 steps with checkpoints every
-        `checkpoint_every` steps; returns the observable rows."""
+    def adjoint_forward(self, steps, checkpoint_every, path=L.HV_PATH_PLAIN):
+        """hv_adjoint_forward_path: `steps` FP64 steps on `path` (plain or
+        fused) with checkpoints every `checkpoint_every` steps; returns the
+        observable rows."""
         obs = np.zeros(steps, L.OBS_DTYPE)
-        L.check(self.lib.hv_adjoint_forward(self._ctx, steps, checkpoint_every, C.c_void_p(obs.ctypes.data)),
-                "hv_adjoint_forward")
+        L.check(self.lib.hv_adjoint_forward_path(self._ctx, path, steps, checkpoint_every,
+                                                 C.c_void_p(obs.ctypes.data)),
+                "hv_adjoint_forward_path")
         return obs
+
+    def adjoint_stats(self):
+        """hv_adjoint_stats: (path, iterations of the last backward pass's
+        transposed Poisson solves, how many stopped at the iteration cap)."""
+        p, it, un = C.c_int(0), C.c_int(0), C.c_int(0)
+        L.check(self.lib.hv_adjoint_stats(self._ctx, C.byref(p), C.byref(it), C.byref(un)), "hv_adjoint_stats")
+        return p.value, it.value, un.value
 
     def adjoint_backward(self, dJ_dD, theta):
         """hv_adjoint_backward: (dJ/d(t0, t3, sigma, a_sym), dJ/d(A, B, C, gamma))

@@ -575,6 +575,29 @@ HV_API hv_status hv_adjoint_forward(hv_ctx *ctx, int n_steps, int checkpoint_eve
 HV_API hv_status hv_adjoint_backward(hv_ctx *ctx, const double *dJ_dD, const double theta[4],
                                      double grad_theta[4], double grad_skyrme[4]);
 
+/* hv_adjoint_forward on a chosen path (no counterpart in the reference).
+ * HV_PATH_PLAIN is hv_adjoint_forward.  HV_PATH_FUSED runs the forward as
+ * fused FP64 steps (hv_run(HV_PATH_FUSED) per segment; missing fields are
+ * solved with the fused kernels), and the following hv_adjoint_backward
+ * recomputes its segments with the same steps and runs each transposed
+ * Poisson solve on the persistent SOR kernel, started from the extrapolation
+ * of the previous reversed steps' solutions as the fused forward starts phi.
+ * Slot re-sorting (hv_fast_options.sort_every) is paused during both passes,
+ * since the adjoint state is indexed by slot.  Device memory: (n / K + 1)
+ * (9 N + 13 G) doubles for the checkpoints (phi and its two earlier
+ * solutions, the interleaved forces and the smoothed density besides the
+ * particle state), K (3 N + 10 G) for a recomputed segment.  A bounded wait of
+ * the solver that runs out returns HV_ERR_TIMEOUT with the fields marked
+ * stale. */
+HV_API hv_status hv_adjoint_forward_path(hv_ctx *ctx, int path, int n_steps, int checkpoint_every,
+                                         hv_observables *obs);
+
+/* After hv_adjoint_backward: the path of the forward run, the iterations of
+ * all transposed Poisson solves of the backward pass, and how many of them
+ * stopped at the iteration cap (no counterpart in the reference). */
+HV_API hv_status hv_adjoint_stats(const hv_ctx *ctx, int *path, int *adjoint_sor_iterations,
+                                  int *adjoint_sor_unconverged);
+
 /* ---- batched runs -------------------------------------------------------
  * No counterpart in the reference, which runs one nucleus per process: many
  * independent runs (own nucleus, test particles, grid and parameters, each an

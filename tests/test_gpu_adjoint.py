@@ -185,3 +185,64 @@ def test_adjoint_backward_after_a_resorting_fused_run_keeps_the_caller_order(hv)
         after_backward = s.download_particles()
     for a, b in zip(after_backward, after_forward):
         assert a.tobytes() == b.tobytes()
+
+
+def test_fused_adjoint_matches_the_plain_adjoint_and_central_differences(hv):
+    """hv_adjoint_forward_path(HV_PATH_FUSED): the forward as fused FP64 steps
+    and the backward's transposed Poisson solves on the persistent SOR kernel.
+    Its D(t) is the plain forward's within 1e-8 of max|D| (both solves to a
+    relative residual of 1e-12), its gradient the plain adjoint's within 1e-5
+    and central differences of fused forward runs within 1e-3, each relative to
+    the largest component."""
+    from hv_b200.adjoint import AdjointRun
+    steps = 40
+    w, parts, theta = _setup(hv, steps)
+    wts = np.random.default_rng(5).standard_normal(steps)
+    fn = lambda d: float(wts @ d)
+    plain = AdjointRun(w, parts, steps, checkpoint_every=10)
+    fused = AdjointRun(w, parts, steps, checkpoint_every=10, path=hv.HV_PATH_FUSED)
+    try:
+        d_p = plain.forward(theta)
+        g_p = plain.backward(wts)
+        d_f = fused.forward(theta)
+        g_f = fused.backward(wts)
+        path, its, unconverged = fused.session.adjoint_stats()
+        g_fd = _central_differences(fused, theta, fn)
+    finally:
+        plain.close()
+        fused.close()
+    assert path == hv.HV_PATH_FUSED and its > 0 and unconverged == 0
+    assert np.max(np.abs(d_f - d_p)) <= 1e-8 * np.abs(d_p).max()
+    scale = np.abs(g_p).max()
+    assert np.all(np.abs(g_f - g_p) <= 1e-5 * scale), (g_f, g_p)
+    scale = np.abs(g_fd).max()
+    assert np.all(np.abs(g_f - g_fd) <= 1e-3 * scale), (g_f, g_fd)
+
+
+def test_fused_adjoint_independent_of_checkpoint_spacing_and_restores_state(hv):
+    """The fused backward recomputes each segment from a checkpoint that holds
+    phi's history, the forces, the smoothed density and the control words, so
+    the gradient does not depend on the spacing; the context ends in the
+    forward's final state, and slot re-sorting stays off during both passes
+    (the default sort_every would otherwise re-sort inside a segment)."""
+    from hv_b200.adjoint import AdjointRun
+    steps = 30
+    w, parts, theta = _setup(hv, steps)
+    wts = np.random.default_rng(6).standard_normal(steps)
+    grads, finals = [], []
+    for every in (1, 7, 30):
+        run = AdjointRun(w, parts, steps, checkpoint_every=every, path=hv.HV_PATH_FUSED,
+                         fast_options={"sort_every": 4})
+        try:
+            d = run.forward(theta)
+            end = run.session.download_particles()
+            grads.append(run.backward(wts))
+            after = run.session.download_particles()
+            assert all(np.array_equal(a, b) for a, b in zip(end, after))
+            finals.append(d)
+        finally:
+            run.close()
+    for g in grads[1:]:
+        assert np.max(np.abs(g - grads[0])) <= 1e-9 * np.abs(grads[0]).max()
+    for d in finals[1:]:
+        assert np.array_equal(d, finals[0])
