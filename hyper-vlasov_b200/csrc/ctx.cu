@@ -113,8 +113,10 @@ hv_status alloc_state(hv_ctx *c) {
     }
     T **grids[] = {&s.rho_raw, &s.rho, &s.U, &s.Fx, &s.Fy, &s.Fz};
     for (T **p : grids) {
-        HV_CUDA(cudaMalloc((void **)p, G2 * sizeof(T)));
-        HV_CUDA(cudaMemsetAsync(*p, 0, G2 * sizeof(T), c->stream));
+        // rho_raw: 4 more values, the wrap list's count (State)
+        const size_t len = G2 + (p == &s.rho_raw ? 4 : 0);
+        HV_CUDA(cudaMalloc((void **)p, len * sizeof(T)));
+        HV_CUDA(cudaMemsetAsync(*p, 0, len * sizeof(T), c->stream));
     }
     HV_CUDA(cudaMalloc((void **)&s.phi, (size_t)c->geom.G * sizeof(T)));
     HV_CUDA(cudaMemsetAsync(s.phi, 0, (size_t)c->geom.G * sizeof(T), c->stream));

@@ -60,7 +60,9 @@ struct State {
     T *x = nullptr, *y = nullptr, *z = nullptr;
     T *kx = nullptr, *ky = nullptr, *kz = nullptr;
     T *fx = nullptr, *fy = nullptr, *fz = nullptr;
-    // fields
+    // fields; rho_raw holds 2G values and then 4 more, the first of which is,
+    // as an int, the count of the FFT smoothing's wrap list (zeroed with the
+    // raw density by each fused step)
     T *rho_raw = nullptr, *rho = nullptr, *U = nullptr, *phi = nullptr;
     T *Fx = nullptr, *Fy = nullptr, *Fz = nullptr;
     T *taps_w = nullptr;
@@ -111,6 +113,9 @@ struct SorFast {
 
 // Decomposed smoothing plan (k_smooth_fast.cu).
 constexpr int kSmoothMaxR = 16;  // largest |a|, |b| or z half-width handled
+// Capacity of the FFT smoothing's wrap list: particles that deposit within the
+// stencil of a face in one step (more: the direct form recomputes the field).
+constexpr int kWrapParticles = 65536;
 struct SmoothFast {
     bool ok = false;           // tap table is symmetric with contiguous runs
     int A = 0, B = 0, W = 0;   // max |a|, |b|, z half-width
@@ -121,13 +126,16 @@ struct SmoothFast {
     int per = 0;               // R = max(A, B, W): the kernel instantiation
     int xsplit = 1;            // x segments per column tile (the plan's choice)
     // FFT form (power-of-two axes up to 128): the circular convolution by the
-    // stencil's spectrum, exact while no density lies within (A, B, W) of a face
+    // stencil's spectrum, exact while no density lies within (A, B, W) of a
+    // face, and made exact otherwise by subtracting the wrapped pairs
     bool fft = false;
     bool fft128 = false;       // 128^3: the register-transform kernels (khat in natural z order)
     void *fwork = nullptr;     // nx ny nz complex floats: both species' transform
     float *khat = nullptr;     // nx ny nz: the stencil's spectrum x term / (nx ny nz)
     void *tw = nullptr;        // 64 complex twiddles exp(-2 pi i m / 128)
-    int *edge = nullptr;       // [nx]: density found within the stencil of a face
+    int *edge = nullptr;       // [nx]: nonzero densities found within the stencil of a face
+    void *wlist = nullptr;     // kWrapParticles float4: the particles depositing within the
+                               // stencil of a face (grid coordinates, species), from the particle step
     double fft_term = 0.0;     // the term folded into khat
 };
 

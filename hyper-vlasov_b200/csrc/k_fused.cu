@@ -25,7 +25,8 @@ hv_status sor_fast_launch(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int 
 hv_status sor_fast_clear_error(hv_ctx *c);
 hv_status smooth_fast_plan(hv_ctx *c);
 void smooth_fast_release(hv_ctx *c);
-hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho);
+hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho, const int *wcount);
+bool smooth_fft_runs(const hv_ctx *c);
 
 namespace {
 
@@ -277,9 +278,43 @@ struct PArgs {
     T h, fd, dp, dn;
     int deposit;  // 1: atomic CIC deposit of x_{n+1} here; 0: the sorted deposit follows
     int aggregate;  // float atomic deposit aggregated over warp runs of equal base nodes
+    // the FFT smoothing's wrap list (null: not kept): particles whose deposit
+    // reaches within the stencil half-widths wA, wB, wW of a face
+    float4 *wlist;
+    int *wcount;
+    int wcap, wA, wB, wW;
     const int *ctl;
     double *obs;  // [kRing][blocks][6]
 };
+
+// Lists the particles whose CIC corners reach within the FFT smoothing's
+// stencil of a face, where the circular convolution wraps their deposit
+// around: grid coordinates (as the deposit forms them) and species, a warp's
+// entries appended with one atomic.  Every lane calls it; past the list's
+// capacity entries are counted but not stored (the smoothing then takes the
+// direct form).
+__device__ __forceinline__ void list_wrap(const PArgs<float> &a, const CellMap<float> &m, float px, float py,
+                                          float pz, long long off, bool valid) {
+    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+    float cx, cy, cz;
+    cell_coords<float>(m, px, py, pz, cx, cy, cz);
+    bool want = false;
+    if (valid && !(cx < 0.0f || cy < 0.0f || cz < 0.0f || cx >= nx || cy >= ny || cz >= nz)) {
+        const int x0 = (int)cx, y0 = (int)cy, z0 = (int)cz;
+        want = x0 < a.wA || x0 >= nx - a.wA - 1 || y0 < a.wB || y0 >= ny - a.wB - 1 || z0 < a.wW ||
+               z0 >= nz - a.wW - 1;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (!mask) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(a.wcount, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) {
+        const int pos = base + __popc(mask & ((1u << lane) - 1u));
+        if (pos < a.wcap) a.wlist[pos] = make_float4(cx, cy, cz, off ? 1.0f : 0.0f);
+    }
+}
 
 // One particle of one step: gather f_n, the closing kick/2 of the previous
 // step, observables of x_n, the excitation, the opening kick/2 and the drift;
@@ -388,6 +423,7 @@ __global__ void __launch_bounds__(kB, sizeof(T) == 4 ? 1024 / kB : 1) k_particle
         if (valid) particle_update<T>(a, m, i, cur, close, excite, dmx, dmy, dmz, v, px, py, pz, off);
         if (!a.deposit) continue;
         if constexpr (sizeof(T) == 4) {
+            if (a.wlist) list_wrap(a, m, px, py, pz, off, valid);
             if (a.aggregate) {
                 deposit_warp(a.g, m, reinterpret_cast<float *>(a.rho_raw), off, px, py, pz, valid);
                 continue;
@@ -454,16 +490,29 @@ __device__ __forceinline__ void skyrme_node(T A, T B, T C, T gamma, T rp, T rn, 
     }
 }
 
+// The smoothed density is also clamped at zero here, in place: the FFT
+// smoothing's wrap correction subtracts from the edge slabs after the
+// transform's own clamp, and may leave rounding-level negatives there (the
+// exact sum is non-negative; rho^gamma has no value below zero).  A node is
+// stored back only when it was negative.
+__device__ __forceinline__ bool clamp4(float4 &v) {
+    const bool neg = v.x < 0.0f || v.y < 0.0f || v.z < 0.0f || v.w < 0.0f;
+    if (neg) v = make_float4(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f), fmaxf(v.z, 0.0f), fmaxf(v.w, 0.0f));
+    return neg;
+}
+
 template <typename T>
-__global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__restrict__ rho, T *U) {
+__global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, T *rho, T *U) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if constexpr (sizeof(T) == 4) {
         // four nodes per thread with 16-byte loads and stores (G a multiple
         // of 4): enough bytes in flight per thread for the memory system
         if ((G & 3) == 0) {
             if (4 * i >= G) return;
-            const float4 p = __ldg(reinterpret_cast<const float4 *>(rho) + i);
-            const float4 n = __ldg(reinterpret_cast<const float4 *>(rho + G) + i);
+            float4 p = reinterpret_cast<const float4 *>(rho)[i];
+            float4 n = reinterpret_cast<const float4 *>(rho + G)[i];
+            if (clamp4(p)) reinterpret_cast<float4 *>(rho)[i] = p;
+            if (clamp4(n)) reinterpret_cast<float4 *>(rho + G)[i] = n;
             float4 up, un;
             skyrme_node<T>(A, B, C, gamma, p.x, n.x, up.x, un.x);
             skyrme_node<T>(A, B, C, gamma, p.y, n.y, up.y, un.y);
@@ -475,7 +524,10 @@ __global__ void k_skyrme_fast(long long G, T A, T B, T C, T gamma, const T *__re
         }
     }
     if (i >= G) return;
-    skyrme_node<T>(A, B, C, gamma, rho[i], rho[i + G], U[i], U[i + G]);
+    T p = rho[i], n = rho[i + G];
+    if (p < T(0)) rho[i] = p = T(0);
+    if (n < T(0)) rho[i + G] = n = T(0);
+    skyrme_node<T>(A, B, C, gamma, p, n, U[i], U[i + G]);
 }
 
 // threads of k_skyrme_fast: one per node, or one per four in float
@@ -652,7 +704,9 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     const hv_run_params &p = c->params;
     int *ctl = ctl_of(c);
     const bool sorted = p.deposit_mode == HV_DEPOSIT_SORTED;
-    if (!sorted) HV_CUDA(cudaMemsetAsync(s.rho_raw, 0, sizeof(T) * 2 * g.G, c->stream));
+    // the raw density and, after it, the wrap list's count
+    if (!sorted) HV_CUDA(cudaMemsetAsync(s.rho_raw, 0, sizeof(T) * (2 * g.G + 4), c->stream));
+    int *wcount = nullptr;
     PArgs<T> a;
     a.g = g;
     a.protons = c->protons;
@@ -672,6 +726,17 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     a.dn = e * zz / (zz + nn);
     a.deposit = sorted ? 0 : 1;
     a.aggregate = c->fast.deposit_aggregate;
+    a.wlist = nullptr;
+    a.wcount = nullptr;
+    a.wcap = kWrapParticles;
+    a.wA = f.smooth.A;
+    a.wB = f.smooth.B;
+    a.wW = f.smooth.W;
+    if (sizeof(T) == 4 && !sorted && smooth_fft_runs(c)) {
+        wcount = reinterpret_cast<int *>(s.rho_raw + 2 * g.G);
+        a.wlist = reinterpret_cast<float4 *>(f.smooth.wlist);
+        a.wcount = wcount;
+    }
     a.ctl = ctl;
     a.obs = f.obs_partials;
     if (c->total > 0) {
@@ -695,7 +760,8 @@ hv_status enqueue_phase_a(hv_ctx *c) {
     {
         ProfScope ps(c, HV_K_SMOOTH);
         if (sizeof(T) == 4 && f.smooth.ok)
-            HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho)));
+            HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho),
+                                      wcount));
         else
             HV_TRY(launch_smooth<T>(c, s.rho_raw, s.rho));
     }
@@ -769,8 +835,11 @@ hv_status initial_typed(hv_ctx *c) {
         HV_TRY(launch_deposit_sorted<T>(c, s.x, s.y, s.z, s.rho_raw));
     else
         HV_TRY(launch_deposit_atomic<T>(c, s.x, s.y, s.z, s.rho_raw));
+    // no wrap list here (the deposit is not the particle step's): density at
+    // a face takes the direct form
     if (sizeof(T) == 4 && f.smooth.ok)
-        HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho)));
+        HV_TRY(smooth_fast_launch(c, reinterpret_cast<const float *>(s.rho_raw), reinterpret_cast<float *>(s.rho),
+                                  nullptr));
     else
         HV_TRY(launch_smooth<T>(c, s.rho_raw, s.rho));
     const hv_skyrme &sk = p.skyrme;

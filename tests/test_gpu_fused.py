@@ -203,19 +203,79 @@ def test_fft_smoothing_matches_the_direct_form(hv, wname):
     assert d_fft.min() >= 0.0
 
 
-def test_fft_smoothing_falls_back_with_density_at_a_face(hv):
-    """Particles within the stencil of a face would wrap around in the
-    circular convolution; the first FFT pass flags them and the direct form
-    recomputes the whole field, so both options agree."""
-    w = hv.CA40_SMALL
+def _particles_at_faces(w, parts):
+    """Copies of the particles with some moved inside the grid next to faces,
+    an edge and a corner, where the circular convolution wraps around."""
+    p = [a.copy() for a in parts]
+    lo = -float(w.n) * w.h / 2.0
+    hi = -lo - 1.5 * w.h  # between the last two nodes
+    p[0][:40] = lo + 0.6 * w.h                       # protons at the x = min face
+    p[1][40:80] = hi                                 # protons at the y = max face
+    p[2][-40:] = lo + 0.3 * w.h                      # neutrons at the z = min face
+    p[0][80:90], p[1][80:90], p[2][80:90] = lo + 0.2 * w.h, hi, lo + 0.7 * w.h  # a corner
+    p[1][-60:-40], p[2][-60:-40] = hi, hi            # neutrons along the y = z = max edge
+    return p
+
+
+def _fft_and_direct_of_one_raw_density(hv, w, parts, deposit_mode):
+    """The fused FFT smoothing of one step's raw density, and the direct sum
+    (hv_smooth_density, the plain kernel) of the same raw density."""
+    wd = replace(w, deposit_mode=deposit_mode)
+    with hv.Session.from_workload(wd, hv.HV_F32) as s:
+        s.set_fast_options(smooth_fft=2)
+        s.upload_particles(*parts)
+        s.run(1, hv.HV_PATH_FUSED)
+        raw = s.download_field(hv.HV_FIELD_DENSITY_RAW)
+        d_fft = s.download_field(hv.HV_FIELD_DENSITY)
+        s.smooth()
+        d_dir = s.download_field(hv.HV_FIELD_DENSITY)
+    return raw, d_fft, d_dir
+
+
+@pytest.mark.parametrize("wname", ["40Ca-4k-32^3", "208Pb-20.8k-128^3"])
+def test_fft_smoothing_with_density_at_faces_keeps_the_truncated_sum(hv, wname):
+    """Density within the stencil of a face wraps around in the circular
+    convolution.  With the atomic deposit the transform's wrapped pairs are
+    subtracted (the wrap correction); the result is the reference's truncated
+    sum, as the direct kernel forms it from the same raw density, to the float
+    transform's rounding: 1e-5 of the maximum (a few 1e-6 at 128^3), for the
+    generic transform (32^3) and the 128^3 one, with density at three faces,
+    an edge and a corner.  Uncorrected, the wrapped density of the 40 moved
+    test particles would reach about a tenth of the maximum."""
+    w = hv.WORKLOADS[wname]
+    p32 = _particles_at_faces(w, hv.workload_particles(w, np.float32))
+    raw, d_fft, d_dir = _fft_and_direct_of_one_raw_density(hv, w, p32, hv.HV_DEPOSIT_ATOMIC)
+    r = raw.reshape(2, w.n, w.n, w.n)
+    assert r[0, :2].sum() > 0 and r[0, :, -2:].sum() > 0 and r[1, :, :, :2].sum() > 0  # density at the faces
+    assert max_rel(d_fft, d_dir) < 1e-5, max_rel(d_fft, d_dir)
+    assert d_fft.min() >= 0.0
+
+
+def test_fft_smoothing_with_more_face_particles_than_the_wrap_list_holds(hv):
+    """Past the wrap list's capacity (65536 particles near faces) the direct
+    march recomputes the field: 70,000 of 2.08 M particles moved to the faces,
+    the result still the truncated sum of the same raw density."""
+    w = hv.WORKLOADS["208Pb-2.08M-128^3"]
     p32 = [a.copy() for a in hv.workload_particles(w, np.float32)]
     lo = -float(w.n) * w.h / 2.0
-    # 40 protons moved next to the x = min face (inside the grid)
-    p32[0][:40] = lo + 0.6 * w.h
-    d_fft, raw_fft = _smoothed_after(hv, w, p32, 1, smooth_fft=2)
-    d_dir, raw_dir = _smoothed_after(hv, w, p32, 1, smooth_fft=0)
-    assert raw_fft.reshape(2, w.n, w.n, w.n)[0, :2].sum() > 0  # density in the x edge slab
-    assert max_rel(d_fft, d_dir) < 1e-6, max_rel(d_fft, d_dir)
+    rng = np.random.default_rng(7)
+    p32[0][:35000] = lo + rng.uniform(0.1, 1.5, 35000).astype(np.float32) * w.h
+    p32[2][-35000:] = -lo - rng.uniform(1.1, 2.5, 35000).astype(np.float32) * w.h
+    raw, d_fft, d_dir = _fft_and_direct_of_one_raw_density(hv, w, p32, hv.HV_DEPOSIT_ATOMIC)
+    assert raw.reshape(2, w.n, w.n, w.n)[0, :2].sum() > 0
+    assert max_rel(d_fft, d_dir) < 1e-5, max_rel(d_fft, d_dir)
+
+
+def test_fft_smoothing_at_faces_in_the_deterministic_mode_uses_the_direct_form(hv):
+    """The sort-by-cell deposit mode keeps the smoothing deterministic: with
+    density at a face the direct march recomputes the field instead of the
+    atomic wrap correction, and two runs agree bit for bit."""
+    w = hv.CA40_SMALL
+    p32 = _particles_at_faces(w, hv.workload_particles(w, np.float32))
+    raw, d_fft, d_dir = _fft_and_direct_of_one_raw_density(hv, w, p32, hv.HV_DEPOSIT_SORTED)
+    raw2, d_fft2, _ = _fft_and_direct_of_one_raw_density(hv, w, p32, hv.HV_DEPOSIT_SORTED)
+    assert np.array_equal(raw, raw2) and np.array_equal(d_fft, d_fft2)
+    assert max_rel(d_fft, d_dir) < 2e-6, max_rel(d_fft, d_dir)
 
 
 def test_fused_state_and_fields_match_oracle_on_final_positions(hv):
