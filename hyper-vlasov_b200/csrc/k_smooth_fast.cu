@@ -74,6 +74,7 @@ struct MarchArgs {
                                               // (null: always run)
     const int *wcount;                        // the wrap list's count (null: no list)
     int wcap;
+    const float4 *wlist;                      // the wrap list (particle step)
 };
 
 // Plane xi of the block's rho tile (y halo B, z halo W; zero outside the
@@ -91,6 +92,105 @@ __device__ __forceinline__ void load_plane(const MarchArgs &a, const float *src,
         v[i] = (e < rows * cols && xi >= 0 && xi < a.nx && y >= 0 && y < a.ny && z >= 0 && z < a.nz)
                    ? __ldg(plane + (long long)y * a.nz + z)
                    : 0.0f;
+    }
+}
+
+// The wrap correction of the FFT form, run by the march kernel's blocks after
+// the transform's last pass when it applies (wrap_active).  The circular
+// convolution adds, to nodes within the stencil of a face, the weights of
+// density near the opposite face whose offset wraps around the grid; the
+// reference's truncated sum (compute_volumetric_densities,
+// include/physics.hpp:202-234) has no such pairs.  The deposit of every
+// listed particle is taken again -- the same grid coordinates, weights and
+// corner drops -- and its wrapped pairs are subtracted from the output.  Work
+// items are (particle, x plane of the box its corners' stencils cover), a
+// warp each, its lanes over the plane's (y, z) targets that lie outside the
+// grid.  For such an unwrapped target T, the sum over the corners c whose
+// offset T - c is a tap of w_c g(a) g(b) g(c), times term, is subtracted at T
+// taken modulo the axes, where the transform put it: one atomic per target of
+// a particle.  The output may then dip below zero by the transform's
+// rounding; the Skyrme kernel, which reads it next, clamps it.  Each axis
+// holds at least twice its half-width plus two nodes (a plan condition), so a
+// target leaves the grid on one side of an axis at most, and one shift brings
+// it back.
+__device__ void wrap_correct(const MarchArgs &a) {
+    __shared__ float s_g[3][kMaxR + 1];
+    __shared__ int s_bm[kMaxR + 1], s_wt[(kMaxR + 1) * (kMaxR + 1)];
+    const int nx = a.nx, ny = a.ny, nz = a.nz;
+    for (int i = threadIdx.x; i <= kMaxR; i += blockDim.x) {
+        s_g[0][i] = a.gx[i];
+        s_g[1][i] = a.gy[i];
+        s_g[2][i] = a.gz[i];
+        s_bm[i] = a.bm[i];
+    }
+    for (int i = threadIdx.x; i < (kMaxR + 1) * (kMaxR + 1); i += blockDim.x) s_wt[i] = a.wt[i];
+    __syncthreads();
+    const int np = *a.wcount, bxn = 2 * a.A + 2, byn = 2 * a.B + 2, bzn = 2 * a.W + 2;
+    // q / bzn for q below byn bzn (at most 34^2) as a product: exact for divisors below 56
+    const unsigned inv_bzn = (65536u + bzn - 1) / bzn;
+    const int lane = threadIdx.x & 31;
+    const long long items = (long long)np * bxn, nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long it = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += nwarps) {
+        const int p = (int)(it / bxn), ix = (int)(it - (long long)p * bxn);
+        const float4 e = a.wlist[p];
+        const int x0 = (int)e.x, y0 = (int)e.y, z0 = (int)e.z;
+        const int X = x0 - a.A + ix;
+        const bool xout = X < 0 || X >= nx;
+        // no target of this x row lies outside the grid
+        if (!xout && y0 - a.B >= 0 && y0 + 1 + a.B < ny && z0 - a.W >= 0 && z0 + 1 + a.W < nz) continue;
+        const float dx = e.x - x0, dy = e.y - y0, dz = e.z - z0;
+        // the two x corners: tap extent in y, weight (a corner with an index
+        // equal to n is dropped, as by the deposit)
+        const int ua0 = abs(X - x0), ua1 = abs(X - x0 - 1);
+        const int bm0 = ua0 <= a.A ? s_bm[ua0] : -1, bm1 = (x0 + 1 < nx && ua1 <= a.A) ? s_bm[ua1] : -1;
+        if (bm0 < 0 && bm1 < 0) continue;
+        const float wx0 = bm0 >= 0 ? (1.0f - dx) * s_g[0][ua0] : 0.0f, wx1 = bm1 >= 0 ? dx * s_g[0][ua1] : 0.0f;
+        const int cyn = y0 + 1 < ny ? 2 : 1, czn = z0 + 1 < nz ? 2 : 1;
+        float *out = a.dst + (e.w != 0.0f ? a.G : 0);
+        const int Xt = X + (X < 0 ? nx : (X >= nx ? -nx : 0));
+        // the plane's targets outside the grid: every one when X is outside;
+        // otherwise the rows whose Y is outside (ylo below, yhi above), and
+        // in the other rows the z offsets whose Z is outside (zlo, zhi)
+        const int ylo = xout ? 0 : max(0, a.B - y0), yhi = xout ? 0 : max(0, y0 + 1 + a.B - (ny - 1));
+        const int zlo = xout ? 0 : max(0, a.W - z0), zhi = xout ? 0 : max(0, z0 + 1 + a.W - (nz - 1));
+        const int nrow = xout ? byn : ylo + yhi, nzo = zlo + zhi;
+        const int nfull = nrow * bzn, ntarget = nfull + (xout ? 0 : (byn - nrow) * nzo);
+        for (int q = lane; q < ntarget; q += 32) {
+            int iy, iz;
+            if (q < nfull) {
+                const int r = (int)(((unsigned)q * inv_bzn) >> 16);
+                iz = q - r * bzn;
+                iy = r < ylo || xout ? r : byn - yhi + (r - ylo);
+            } else {
+                const int qq = q - nfull, r = qq / nzo, c = qq - r * nzo;
+                iy = ylo + r;
+                iz = c < zlo ? c : bzn - zhi + (c - zlo);
+            }
+            const int Y = y0 - a.B + iy, Z = z0 - a.W + iz;
+            float v = 0.0f;
+#pragma unroll
+            for (int cb = 0; cb < 2; cb++) {
+                if (cb >= cyn) break;
+                const int ub = abs(Y - y0 - cb);
+                if (ub > a.B) continue;
+                const float wy = (cb ? dy : 1.0f - dy) * s_g[1][ub];
+#pragma unroll
+                for (int ca = 0; ca < 2; ca++) {
+                    if (ub > (ca ? bm1 : bm0)) continue;
+                    const int w = s_wt[(ca ? ua1 : ua0) * (kMaxR + 1) + ub];
+                    const float wxy = (ca ? wx1 : wx0) * wy;
+#pragma unroll
+                    for (int cc = 0; cc < 2; cc++) {
+                        if (cc >= czn) break;
+                        const int uc = abs(Z - z0 - cc);
+                        if (uc <= w) v += wxy * (cc ? dz : 1.0f - dz) * s_g[2][uc];
+                    }
+                }
+            }
+            if (v == 0.0f) continue;
+            const int Yt = Y + (Y < 0 ? ny : (Y >= ny ? -ny : 0)), Zt = Z + (Z < 0 ? nz : (Z >= nz ? -nz : 0));
+            atomicAdd(out + ((long long)Xt * ny + Yt) * nz + Zt, -v * a.term);
+        }
     }
 }
 
@@ -113,7 +213,11 @@ __global__ void __launch_bounds__(kMThreads) k_smooth_march(const __grid_constan
         // after the FFT form: needed only where neither the transform nor
         // its wrap correction is exact
         const int flags = edge_total(a.edge, a.nx);
-        if (flags == 0 || wrap_active(flags, a.wcount, a.wcap)) return;
+        if (flags == 0) return;
+        if (wrap_active(flags, a.wcount, a.wcap)) {
+            wrap_correct(a);
+            return;
+        }
     }
     const int A = a.A, ring = 2 * A + 1;
     float *s_rho = sm;                               // rows x cols
@@ -266,118 +370,7 @@ struct FftArgs {
     const float2 *tw;            // kFMaxN / 2 twiddles exp(-2 pi i m / kFMaxN)
     int *edge;                   // [nx]: nonzero densities within the stencil of a face, per x plane
     float post;                  // current term / the term folded into khat
-    // wrap correction: the particle step lists every particle that deposits
-    // within the stencil of a face (its grid coordinates and species) and
-    // counts them in *wcount; the correction kernel subtracts the wrapped pairs
-    // of their deposits from dst (wcount null: no list, the direct form instead)
-    const float4 *wlist;
-    const int *wcount;
-    int wcap;
-    float term;                                // the smoothing's prefactor
-    float gx[kMaxR + 1], gy[kMaxR + 1], gz[kMaxR + 1];  // the stencil's weights per axis
-    int bm[kMaxR + 1];                         // largest |b| with a tap for each |a| (-1: none)
-    int wt[(kMaxR + 1) * (kMaxR + 1)];         // z half-width w(|a|, |b|) (-1: none)
 };
-
-// The wrap correction of the FFT form, after its last pass.  The circular
-// convolution adds, to nodes within the stencil of a face, the weights of
-// density near the opposite face whose offset wraps around the grid; the
-// reference's truncated sum (compute_volumetric_densities,
-// include/physics.hpp:202-234) has no such pairs.  The deposit of every
-// listed particle is taken again -- the same grid coordinates, weights and
-// corner drops -- and its wrapped pairs are subtracted from the output.  Work
-// items are (particle, x plane of the box its corners' stencils cover), a
-// warp each, its lanes over the plane's (y, z) targets that lie outside the
-// grid.  For such an unwrapped target T, the sum over the corners c whose
-// offset T - c is a tap of w_c g(a) g(b) g(c), times term, is subtracted at T
-// taken modulo the axes, where the transform put it: one atomic per target of
-// a particle.  The output may then dip below zero by the transform's
-// rounding; the Skyrme kernel, which reads it next, clamps it.  Each axis
-// holds at least twice its half-width plus two nodes (a plan condition), so a
-// target leaves the grid on one side of an axis at most, and one shift brings
-// it back.
-constexpr int kWrapThreads = 256;
-__global__ void __launch_bounds__(kWrapThreads) k_fft_wrap(const __grid_constant__ FftArgs a) {
-    __shared__ float s_g[3][kMaxR + 1];
-    __shared__ int s_bm[kMaxR + 1], s_wt[(kMaxR + 1) * (kMaxR + 1)];
-    const int nx = a.nx, ny = a.ny, nz = a.nz;
-    if (!wrap_active(edge_total(a.edge, nx), a.wcount, a.wcap)) return;
-    for (int i = threadIdx.x; i <= kMaxR; i += blockDim.x) {
-        s_g[0][i] = a.gx[i];
-        s_g[1][i] = a.gy[i];
-        s_g[2][i] = a.gz[i];
-        s_bm[i] = a.bm[i];
-    }
-    for (int i = threadIdx.x; i < (kMaxR + 1) * (kMaxR + 1); i += blockDim.x) s_wt[i] = a.wt[i];
-    __syncthreads();
-    const int np = *a.wcount, bxn = 2 * a.A + 2, byn = 2 * a.B + 2, bzn = 2 * a.W + 2;
-    // q / bzn for q below byn bzn (at most 34^2) as a product: exact for divisors below 56
-    const unsigned inv_bzn = (65536u + bzn - 1) / bzn;
-    const int lane = threadIdx.x & 31;
-    const long long items = (long long)np * bxn, nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long it = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < items; it += nwarps) {
-        const int p = (int)(it / bxn), ix = (int)(it - (long long)p * bxn);
-        const float4 e = a.wlist[p];
-        const int x0 = (int)e.x, y0 = (int)e.y, z0 = (int)e.z;
-        const int X = x0 - a.A + ix;
-        const bool xout = X < 0 || X >= nx;
-        // no target of this x row lies outside the grid
-        if (!xout && y0 - a.B >= 0 && y0 + 1 + a.B < ny && z0 - a.W >= 0 && z0 + 1 + a.W < nz) continue;
-        const float dx = e.x - x0, dy = e.y - y0, dz = e.z - z0;
-        // the two x corners: tap extent in y, weight (a corner with an index
-        // equal to n is dropped, as by the deposit)
-        const int ua0 = abs(X - x0), ua1 = abs(X - x0 - 1);
-        const int bm0 = ua0 <= a.A ? s_bm[ua0] : -1, bm1 = (x0 + 1 < nx && ua1 <= a.A) ? s_bm[ua1] : -1;
-        if (bm0 < 0 && bm1 < 0) continue;
-        const float wx0 = bm0 >= 0 ? (1.0f - dx) * s_g[0][ua0] : 0.0f, wx1 = bm1 >= 0 ? dx * s_g[0][ua1] : 0.0f;
-        const int cyn = y0 + 1 < ny ? 2 : 1, czn = z0 + 1 < nz ? 2 : 1;
-        float *out = a.dst + (e.w != 0.0f ? a.G : 0);
-        const int Xt = X + (X < 0 ? nx : (X >= nx ? -nx : 0));
-        // the plane's targets outside the grid: every one when X is outside;
-        // otherwise the rows whose Y is outside (ylo below, yhi above), and
-        // in the other rows the z offsets whose Z is outside (zlo, zhi)
-        const int ylo = xout ? 0 : max(0, a.B - y0), yhi = xout ? 0 : max(0, y0 + 1 + a.B - (ny - 1));
-        const int zlo = xout ? 0 : max(0, a.W - z0), zhi = xout ? 0 : max(0, z0 + 1 + a.W - (nz - 1));
-        const int nrow = xout ? byn : ylo + yhi, nzo = zlo + zhi;
-        const int nfull = nrow * bzn, ntarget = nfull + (xout ? 0 : (byn - nrow) * nzo);
-        for (int q = lane; q < ntarget; q += 32) {
-            int iy, iz;
-            if (q < nfull) {
-                const int r = (int)(((unsigned)q * inv_bzn) >> 16);
-                iz = q - r * bzn;
-                iy = r < ylo || xout ? r : byn - yhi + (r - ylo);
-            } else {
-                const int qq = q - nfull, r = qq / nzo, c = qq - r * nzo;
-                iy = ylo + r;
-                iz = c < zlo ? c : bzn - zhi + (c - zlo);
-            }
-            const int Y = y0 - a.B + iy, Z = z0 - a.W + iz;
-            float v = 0.0f;
-#pragma unroll
-            for (int cb = 0; cb < 2; cb++) {
-                if (cb >= cyn) break;
-                const int ub = abs(Y - y0 - cb);
-                if (ub > a.B) continue;
-                const float wy = (cb ? dy : 1.0f - dy) * s_g[1][ub];
-#pragma unroll
-                for (int ca = 0; ca < 2; ca++) {
-                    if (ub > (ca ? bm1 : bm0)) continue;
-                    const int w = s_wt[(ca ? ua1 : ua0) * (kMaxR + 1) + ub];
-                    const float wxy = (ca ? wx1 : wx0) * wy;
-#pragma unroll
-                    for (int cc = 0; cc < 2; cc++) {
-                        if (cc >= czn) break;
-                        const int uc = abs(Z - z0 - cc);
-                        if (uc <= w) v += wxy * (cc ? dz : 1.0f - dz) * s_g[2][uc];
-                    }
-                }
-            }
-            if (v == 0.0f) continue;
-            const int Yt = Y + (Y < 0 ? ny : (Y >= ny ? -ny : 0)), Zt = Z + (Z < 0 ? nz : (Z >= nz ? -nz : 0));
-            atomicAdd(out + ((long long)Xt * ny + Yt) * nz + Zt, -v * a.term);
-        }
-    }
-}
 
 __device__ __forceinline__ int bit_reverse(int v, int l) { return (int)(__brev((unsigned)v) >> (32 - l)); }
 
@@ -1015,6 +1008,7 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho, const 
     a.edge = nullptr;
     a.wcount = nullptr;
     a.wcap = kWrapParticles;
+    a.wlist = nullptr;
     if (smooth_fft_runs(c)) {
         FftArgs q;
         q.nx = g.nx;
@@ -1034,21 +1028,12 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho, const 
         q.tw = reinterpret_cast<const float2 *>(f.tw);
         q.edge = f.edge;
         q.post = (float)(term / f.fft_term);
-        q.wlist = reinterpret_cast<const float4 *>(f.wlist);
-        // the deterministic deposit mode keeps a deterministic smoothing: the
-        // particle step lists nothing there, and the direct form recomputes
-        // the field instead of the atomic correction
-        q.wcount = p.deposit_mode == HV_DEPOSIT_SORTED ? nullptr : wcount;
-        q.wcap = kWrapParticles;
-        q.term = (float)term;
-        for (int i = 0; i <= kMaxR; i++) {
-            q.gx[i] = f.gx[i];
-            q.gy[i] = f.gy[i];
-            q.gz[i] = f.gz[i];
-            q.bm[i] = f.bm[i];
-        }
-        for (int i = 0; i < (kMaxR + 1) * (kMaxR + 1); i++) q.wt[i] = f.wt[i];
-        a.wcount = q.wcount;
+        a.edge = f.edge;
+        // the wrap correction (in the march kernel's launch): the particle
+        // step's list; none in the deterministic deposit mode, whose
+        // smoothing stays deterministic by the direct form
+        a.wcount = p.deposit_mode == HV_DEPOSIT_SORTED ? nullptr : wcount;
+        a.wlist = reinterpret_cast<const float4 *>(f.wlist);
         if (f.fft128) {
             k_fft128_plane_fwd<<<kF128, kFThreads, kF128Smem, c->stream>>>(q);
             k_fft128_columns<<<kF128, kFThreads, kF128Smem, c->stream>>>(q);
@@ -1059,9 +1044,7 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho, const 
             k_fft_columns<<<g.ny, kFThreads, slab, c->stream>>>(q);
             k_fft_plane_inv<<<g.nx, kFThreads, plane, c->stream>>>(q);
         }
-        k_fft_wrap<<<(unsigned)(8 * c->sm_count), kWrapThreads, 0, c->stream>>>(q);
         HV_CUDA(cudaGetLastError());
-        a.edge = f.edge;
     }
     const int tz = (g.nz + kMBK - 1) / kMBK, ty = (g.ny + kMBY - 1) / kMBY;
     void *args[] = {&a};
