@@ -202,18 +202,23 @@ def sor_checks(n_sor, sweeps_per_cycle):
     return math.ceil(n_sor / sweeps_per_cycle) + 1 if sweeps_per_cycle > 0 else 2
 
 
-def step_bytes(w, n_sor, wordsize=4, checks=2):
-    """Algorithmic bytes of one step, per kernel: 48 B per particle (x, k read
-    and written) and 4 G (24 + 3 n_sor) B of grid traffic (deposit 2 words per
-    node, smoothing 4, Skyrme 4, merge 2, FDM 8, gather 6 minus overlap, SOR 3
-    per iteration).  The solve also streams its FP64 state: the extrapolated
-    start (read phi and its two predecessors, write all three: 48 B per node)
-    and each residual check (read phi and the carried residual, write both:
-    32 B per node)."""
+def step_bytes(w, n_sor, wordsize=4, checks=2, touched=None):
+    """Algorithmic bytes of one step, per kernel.  The particle step: 48 B per
+    particle (x, k read and written) and, per grid node its particles touch
+    (`touched`, counted over both species' grids; all 2 G when not given), the
+    interleaved force read by the gather (4 words) and the raw density's
+    read-modify-write by the deposit (2 words).  The grid kernels: 4 G B per
+    word of traffic per node (smoothing 4, Skyrme 4, forces 10: the potential
+    and phi read with their neighbours, the interleaved force written; SOR 3
+    per red+black iteration).  The solve also streams its FP64 state: the
+    extrapolated start (read phi and its two predecessors, write all three:
+    48 B per node) and each residual check (read phi and the carried
+    residual, write both: 32 B per node)."""
     G, N = w.G, w.particles
     s = wordsize / 4.0
+    nodes = 2 * G if touched is None else touched
     return {
-        "particle": s * (48 * N + 4 * G * (2 + 6)),
+        "particle": s * (48 * N + 4 * nodes * (4 + 2)),
         "smooth": s * 4 * G * 4,
         "skyrme": s * 4 * G * 4,
         "sor": s * 4 * G * 3 * n_sor + G * (48 + 32 * checks),
@@ -807,15 +812,16 @@ def our_arm(args, world, rank, local):
     sess.set_fast_options(sor_warm_start=warm_mode, sor_exchange=hv.HV_SOR_EXCHANGE_FLAGS
                           if args.sor_exchange == "flags" else hv.HV_SOR_EXCHANGE_AUTO)
     sess.upload_particles(*parts)
-    # the launch configuration chosen by the project's autotuner (its trial
-    # steps advance the run), then the warm-up steps
-    tune = sess.autotune(args.autotune_steps) if args.autotune_steps > 0 else None
     stream = torch.cuda.ExternalStream(sess.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # the clock sampler starts before the warm-up steps, so that its start-up
-    # (about a second of nvidia-smi initialisation) leaves no idle gap on the
-    # GPU just before the timed steps; it samples through the timed region
+    # the clock sampler starts before the autotuner, so that its start-up
+    # (up to a second of nvidia-smi initialisation, with the GPU idle) is
+    # followed by the autotuner's trial steps and the warm-up steps rather than
+    # by the timed steps; it samples through the timed region
     with ClockSampler(local) as clk:
+        # the launch configuration chosen by the project's autotuner (its
+        # trial steps advance the run), then the warm-up steps
+        tune = sess.autotune(args.autotune_steps) if args.autotune_steps > 0 else None
         sess.run(W, hv.HV_PATH_FUSED)  # includes the initial field solve when not tuned
         barrier(world)
         torch.cuda.synchronize()
@@ -842,7 +848,11 @@ def our_arm(args, world, rank, local):
     fo = sess.fast_options()
     per_cycle = fo.sor_coarse_sweeps if (fo.sor_coarse and prec == hv.HV_F32) else 0
     ws_ = 4 if prec == hv.HV_F32 else 8
-    nbytes = step_bytes(w, its_p.mean(), ws_, float(np.mean([sor_checks(n, per_cycle) for n in its_p])))
+    # grid nodes the particle step's gathers and deposit touch: the nonzero
+    # nodes of the raw density its last launch deposited (both species)
+    touched = int(np.count_nonzero(sess.download_field(hv.HV_FIELD_DENSITY_RAW)))
+    nbytes = step_bytes(w, its_p.mean(), ws_, float(np.mean([sor_checks(n, per_cycle) for n in its_p])),
+                        touched=touched)
     tot_ms = sum(v[0] for v in kt.values())
     kernels = {}
     for k, (kms, n) in kt.items():
@@ -852,6 +862,8 @@ def our_arm(args, world, rank, local):
         b = nbytes[k]
         kernels[k] = {"launches": n, "avg_ms": per, "share": kms / tot_ms if tot_ms else None,
                       "algorithmic_bytes": b, "gbs": b / (per / 1e3) / 1e9}
+    if "particle" in kernels:
+        kernels["particle"]["touched_nodes"] = touched
     peak, peak_kind = peaks()
     sor_b = sum(step_bytes(w, n, ws_, sor_checks(n, per_cycle))["sor"] for n in its_p)
     sor_ms = kt["sor"][0]
