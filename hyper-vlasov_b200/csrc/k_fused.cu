@@ -539,9 +539,18 @@ inline long long skyrme_threads(long long G) {
 // -grad(U + phi_p) with the reference's one-sided faces
 // (compute_volumetric_forces_fdm, include/physics.hpp:159-200), the Coulomb
 // merge (include/tools.hpp:377-384) folded in, written as (Fx,Fy,Fz,0).
+//
+// raw (float steps): the raw CIC density of the positions the next gather
+// reads.  A gather weights the force at a node by the same CIC weight the
+// deposit of that position added to the node, so the only forces read with a
+// nonzero weight are those at nodes of nonzero raw density.  A block whose
+// rows hold no raw density (most of the grid: the nucleus covers about a
+// fifth of the rows of 208Pb on 128^3) leaves its forces as they were; the
+// gather multiplies any such finite value by a zero weight.  The end of a run
+// computes every row again for the plain-path view of the fields (raw null).
 template <typename T>
 __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U, const double *__restrict__ phi,
-                            T *F4, int *advance) {
+                            T *F4, int *advance, const T *__restrict__ raw) {
     // the step's last kernel also advances the step counter (advance: the
     // control words; null for the initial solve)
     if (advance && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) {
@@ -558,6 +567,13 @@ __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U
     const T *Us = U + (prot ? 0 : g.G);
     auto u = [&](long long q) { return prot ? Us[q] + (T)phi[q] : Us[q]; };
     const int j0 = blockIdx.x * kForceRows, j1 = min(j0 + kForceRows, ny);
+    if (raw) {
+        // the block's rows are contiguous: (j1 - j0) nz values of its species
+        const T *r = raw + (prot ? 0 : g.G) + (long long)ii * sx + (long long)j0 * sy;
+        int any = 0;
+        for (int e = threadIdx.x; e < (j1 - j0) * nz; e += blockDim.x) any |= r[e] != T(0);
+        if (!__syncthreads_or(any)) return;
+    }
     for (int k = threadIdx.x; k < nz; k += blockDim.x) {
         long long id = (long long)ii * sx + (long long)j0 * sy + k;
         T um = j0 > 0 ? u(id - sy) : T(0);
@@ -783,10 +799,16 @@ hv_status enqueue_phase_c(hv_ctx *c) {
     int *ctl = ctl_of(c);
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
+    // float steps with the particle step's own atomic deposit: forces only on
+    // the rows holding raw density.  The deterministic deposit forms its cells
+    // with the reference's division, which can put a particle on a cell face
+    // into the neighbouring cell of the gather's (a product by the reciprocal),
+    // so its steps compute every row.
+    const T *raw = (sizeof(T) == 4 && c->params.deposit_mode != HV_DEPOSIT_SORTED) ? s.rho_raw : nullptr;
     {
         ProfScope ps(c, HV_K_FORCES);
         k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
-                                                                  reinterpret_cast<T *>(f.F4), ctl);
+                                                                  reinterpret_cast<T *>(f.F4), ctl, raw);
     }
     HV_CUDA(cudaGetLastError());
     return HV_OK;
@@ -868,7 +890,8 @@ hv_status initial_typed(hv_ctx *c) {
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
     k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
-                                                                       reinterpret_cast<T *>(f.F4), nullptr);
+                                                                       reinterpret_cast<T *>(f.F4), nullptr,
+                                                                       nullptr);
     HV_CUDA(cudaGetLastError());
     int status[3] = {0, 0, 0};
     HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
@@ -1121,6 +1144,16 @@ hv_status run_end(hv_ctx *c, int n_steps, int exc) {
     if (exc >= 0) c->excited = true;
     c->step_index += n_steps;
     State<T> &S = st<T>(c);
+    if (sizeof(T) == 4 && n_steps > 0) {
+        // the float steps computed forces only where the next gather reads
+        // them: the plain-path view of the fields gets every row, from the
+        // same U and phi (before the merge below adds phi to U)
+        const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
+                idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
+        k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, S.U, f.phi64,
+                                                                           reinterpret_cast<T *>(f.F4), nullptr,
+                                                                           nullptr);
+    }
     if (c->total > 0)
         k_close_kick<T><<<nblk(c->total, 256), 256, 0, c->stream>>>(g, c->protons, c->total, S.x, S.y, S.z, S.kx, S.ky,
                                                                     S.kz, S.fx, S.fy, S.fz,

@@ -333,6 +333,41 @@ def test_fused_runs_continue_across_calls_and_paths(hv):
     assert np.allclose(np.concatenate([a["t"], b["t"], c["t"]]), np.arange(14) * w.dt)
 
 
+def test_forces_on_the_gathered_rows_only_keep_the_run(hv):
+    """A float step with the atomic deposit computes the forces only on the
+    row groups of the grid that hold raw density, the nodes its particles'
+    next gather reads with a nonzero weight (208Pb on 128^3: the nucleus
+    covers about a fifth of the rows); the end of a run computes every row
+    again for the plain-path view.  Twelve runs of one step each (every
+    gather reading forces computed on every row) and one run of twelve steps
+    give D(t) and particles equal to float rounding of the atomic deposit's
+    order, and the forces downloaded after the run match those the plain
+    path computes from the potential the run left."""
+    w = hv.PB208_20K_128
+    p32 = hv.workload_particles(w, np.float32)
+    opts = dict(sort_every=0)
+    obs1, out1 = _fused(hv, w, 12, hv.HV_F32, p32, **opts)
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        s.set_fast_options(**opts)
+        s.upload_particles(*p32)
+        s.initial_solve()
+        parts = [s.run(1, hv.HV_PATH_FUSED) for _ in range(12)]
+        out2 = s.download_particles()
+        fields = (hv.HV_FIELD_FORCE_X, hv.HV_FIELD_FORCE_Y, hv.HV_FIELD_FORCE_Z)
+        f_fused = [s.download_field(fld) for fld in fields]
+        # the plain path's forces of the potential the run left
+        s.forces()
+        f_plain = [s.download_field(fld) for fld in fields]
+    d = np.concatenate([o["dipole"] for o in parts])
+    assert np.allclose(np.concatenate([o["t"] for o in parts]), obs1["t"])
+    assert max_rel(d, obs1["dipole"]) < 1e-5, max_rel(d, obs1["dipole"])
+    for a, b in zip(out1[:6], out2[:6]):
+        assert np.max(np.abs(a - b)) <= 1e-5 * max(1.0, float(np.max(np.abs(a))))
+    for a, b in zip(f_fused, f_plain):
+        scale = float(np.max(np.abs(b)))
+        assert scale > 0 and np.max(np.abs(a - b)) <= 1e-5 * scale, (np.max(np.abs(a - b)), scale)
+
+
 def test_graph_and_direct_launch_agree(hv):
     w = hv.CA40_SMALL
     p = hv.workload_particles(w, np.float64)
