@@ -202,7 +202,7 @@ def sor_checks(n_sor, sweeps_per_cycle):
     return math.ceil(n_sor / sweeps_per_cycle) + 1 if sweeps_per_cycle > 0 else 2
 
 
-def step_bytes(w, n_sor, wordsize=4, checks=2, touched=None):
+def step_bytes(w, n_sor, wordsize=4, checks=2, touched=None, force_frac=None):
     """Algorithmic bytes of one step, per kernel.  The particle step: 48 B per
     particle (x, k read and written) and, per grid node its particles touch
     (`touched`, counted over both species' grids; all 2 G when not given), the
@@ -213,7 +213,11 @@ def step_bytes(w, n_sor, wordsize=4, checks=2, touched=None):
     per red+black iteration).  The solve also streams its FP64 state: the
     extrapolated start (read phi and its two predecessors, write all three:
     48 B per node) and each residual check (read phi and the carried
-    residual, write both: 32 B per node)."""
+    residual, write both: 32 B per node).  The float forces kernel with the
+    atomic deposit computes only the row groups holding raw density
+    (`force_frac` of them); it tests them by reading the raw density of every
+    row (1 word per node of both species), except at 128^3, where the FFT
+    smoothing's forward pass records the test while it reads that density."""
     G, N = w.G, w.particles
     s = wordsize / 4.0
     nodes = 2 * G if touched is None else touched
@@ -222,7 +226,7 @@ def step_bytes(w, n_sor, wordsize=4, checks=2, touched=None):
         "smooth": s * 4 * G * 4,
         "skyrme": s * 4 * G * 4,
         "sor": s * 4 * G * 3 * n_sor + G * (48 + 32 * checks),
-        "forces": s * 4 * G * 10,
+        "forces": s * 4 * G * 10 if force_frac is None else s * 4 * G * ((0 if w.n == 128 else 2) + 10 * force_frac),
     }
 
 
@@ -849,10 +853,17 @@ def our_arm(args, world, rank, local):
     per_cycle = fo.sor_coarse_sweeps if (fo.sor_coarse and prec == hv.HV_F32) else 0
     ws_ = 4 if prec == hv.HV_F32 else 8
     # grid nodes the particle step's gathers and deposit touch: the nonzero
-    # nodes of the raw density its last launch deposited (both species)
-    touched = int(np.count_nonzero(sess.download_field(hv.HV_FIELD_DENSITY_RAW)))
+    # nodes of the raw density its last launch deposited (both species); the
+    # forces kernel's row groups (4 y rows of one x plane and species in the
+    # float steps) that hold any of them are the ones it computes
+    raw = sess.download_field(hv.HV_FIELD_DENSITY_RAW)
+    touched = int(np.count_nonzero(raw))
+    rows = np.any(raw.reshape(2, w.n, w.n, w.n) != 0, axis=3)
+    pad = (-w.n) % 4
+    groups = np.any(np.pad(rows, ((0, 0), (0, 0), (0, pad))).reshape(2, w.n, -1, 4), axis=3)
+    force_frac = float(np.mean(groups)) if (prec == hv.HV_F32 and w.deposit_mode != hv.HV_DEPOSIT_SORTED) else None
     nbytes = step_bytes(w, its_p.mean(), ws_, float(np.mean([sor_checks(n, per_cycle) for n in its_p])),
-                        touched=touched)
+                        touched=touched, force_frac=force_frac)
     tot_ms = sum(v[0] for v in kt.values())
     kernels = {}
     for k, (kms, n) in kt.items():
@@ -864,6 +875,8 @@ def our_arm(args, world, rank, local):
                       "algorithmic_bytes": b, "gbs": b / (per / 1e3) / 1e9}
     if "particle" in kernels:
         kernels["particle"]["touched_nodes"] = touched
+    if "forces" in kernels and force_frac is not None:
+        kernels["forces"]["computed_row_groups"] = force_frac
     peak, peak_kind = peaks()
     sor_b = sum(step_bytes(w, n, ws_, sor_checks(n, per_cycle))["sor"] for n in its_p)
     sor_ms = kt["sor"][0]

@@ -134,6 +134,8 @@ struct SmoothFast {
     float *khat = nullptr;     // nx ny nz: the stencil's spectrum x term / (nx ny nz)
     void *tw = nullptr;        // 64 complex twiddles exp(-2 pi i m / 128)
     int *edge = nullptr;       // [nx]: nonzero densities found within the stencil of a face
+    unsigned *occ = nullptr;   // [2][nx] (128^3 transforms): bit q set when raw density of the species
+                               // lies in rows 4q..4q+3 of the x plane (written by the forward pass)
     void *wlist = nullptr;     // kWrapParticles float4: the particles depositing within the
                                // stencil of a face (grid coordinates, species), from the particle step
     double fft_term = 0.0;     // the term folded into khat

@@ -33,7 +33,9 @@ namespace {
 constexpr int kPBlock = 256;      // default threads per block of the particle step
 constexpr int kPBlockMax = 512;   // largest of the autotuner's candidates
 constexpr int kPGridMax = 16;     // most blocks per SM of the particle step
-constexpr int kForceRows = 8;     // y rows per thread of the forces kernel
+constexpr int kForceRows = 8;     // y rows per thread of the forces kernel on every row
+constexpr int kForceRowsGated = 4; // the same where only rows holding raw density are computed:
+                                   // shorter walks, as only about a fifth of the blocks work
 constexpr int kRing = 64;  // observable rows kept on the device
 
 // control words (Fused::ctl)
@@ -548,9 +550,13 @@ inline long long skyrme_threads(long long G) {
 // fifth of the rows of 208Pb on 128^3) leaves its forces as they were; the
 // gather multiplies any such finite value by a zero weight.  The end of a run
 // computes every row again for the plain-path view of the fields (raw null).
+// occ (128^3 FFT smoothing, rows = 4): the same test, already made by the
+// smoothing's forward pass while it read the raw densities, one bit per
+// group of four rows.
 template <typename T>
 __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U, const double *__restrict__ phi,
-                            T *F4, int *advance, const T *__restrict__ raw) {
+                            T *F4, int *advance, const T *__restrict__ raw, int rows,
+                            const unsigned *__restrict__ occ) {
     // the step's last kernel also advances the step counter (advance: the
     // control words; null for the initial solve)
     if (advance && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0) {
@@ -558,16 +564,18 @@ __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U
         advance[CTL_CLOSE] = 1;
     }
     // block (row group, x plane, species), threads along z: each thread walks
-    // kForceRows consecutive y rows at its z, keeping the y-1, y and y+1
-    // values of U + phi in registers, so a node loads five values, not seven
+    // `rows` consecutive y rows at its z, keeping the y-1, y and y+1 values
+    // of U + phi in registers, so a node loads five values, not seven
     const int ii = blockIdx.y;
     const bool prot = blockIdx.z == 0;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long sx = (long long)ny * nz, sy = nz;
     const T *Us = U + (prot ? 0 : g.G);
     auto u = [&](long long q) { return prot ? Us[q] + (T)phi[q] : Us[q]; };
-    const int j0 = blockIdx.x * kForceRows, j1 = min(j0 + kForceRows, ny);
-    if (raw) {
+    const int j0 = blockIdx.x * rows, j1 = min(j0 + rows, ny);
+    if (occ) {
+        if (!((occ[blockIdx.z * nx + ii] >> blockIdx.x) & 1u)) return;
+    } else if (raw) {
         // the block's rows are contiguous: (j1 - j0) nz values of its species
         const T *r = raw + (prot ? 0 : g.G) + (long long)ii * sx + (long long)j0 * sy;
         int any = 0;
@@ -606,10 +614,10 @@ __global__ void k_forces_f4(Geom g, T idx, T idy, T idz, const T *__restrict__ U
     }
 }
 
-// k_forces_f4's launch: one block per (group of kForceRows y rows, x plane,
+// k_forces_f4's launch: one block per (group of `rows` y rows, x plane,
 // species), threads along z
-inline dim3 forces_grid(const Geom &g) {
-    return dim3((unsigned)((g.ny + kForceRows - 1) / kForceRows), (unsigned)g.nx, 2u);
+inline dim3 forces_grid(const Geom &g, int rows) {
+    return dim3((unsigned)((g.ny + rows - 1) / rows), (unsigned)g.nx, 2u);
 }
 inline dim3 forces_block(const Geom &g) { return dim3((unsigned)std::min(128, (g.nz + 31) / 32 * 32)); }
 
@@ -807,8 +815,15 @@ hv_status enqueue_phase_c(hv_ctx *c) {
     const T *raw = (sizeof(T) == 4 && c->params.deposit_mode != HV_DEPOSIT_SORTED) ? s.rho_raw : nullptr;
     {
         ProfScope ps(c, HV_K_FORCES);
-        k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
-                                                                  reinterpret_cast<T *>(f.F4), ctl, raw);
+        const int rows = raw ? kForceRowsGated : kForceRows;
+        // the 128^3 FFT smoothing's occupancy bits: 32 groups of four rows
+        const unsigned *occ = (raw && f.smooth.fft128 && f.smooth.occ && smooth_fft_runs(c) &&
+                               g.ny == 32 * kForceRowsGated)
+                                  ? f.smooth.occ
+                                  : nullptr;
+        k_forces_f4<T><<<forces_grid(g, rows), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
+                                                                        reinterpret_cast<T *>(f.F4), ctl, raw,
+                                                                        rows, occ);
     }
     HV_CUDA(cudaGetLastError());
     return HV_OK;
@@ -889,9 +904,8 @@ hv_status initial_typed(hv_ctx *c) {
     HV_TRY(sor_fast_launch<T>(c, s.rho, ctl, nullptr, kRing, false));
     const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
             idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
-    k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, s.U, f.phi64,
-                                                                       reinterpret_cast<T *>(f.F4), nullptr,
-                                                                       nullptr);
+    k_forces_f4<T><<<forces_grid(g, kForceRows), forces_block(g), 0, c->stream>>>(
+        g, idx, idy, idz, s.U, f.phi64, reinterpret_cast<T *>(f.F4), nullptr, nullptr, kForceRows, nullptr);
     HV_CUDA(cudaGetLastError());
     int status[3] = {0, 0, 0};
     HV_CUDA(cudaMemcpyAsync(status, f.sor.status, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->stream));
@@ -1150,9 +1164,8 @@ hv_status run_end(hv_ctx *c, int n_steps, int exc) {
         // same U and phi (before the merge below adds phi to U)
         const T idx = T(1.0) / (T(2.0) * T(g.dmx) / g.nx), idy = T(1.0) / (T(2.0) * T(g.dmy) / g.ny),
                 idz = T(1.0) / (T(2.0) * T(g.dmz) / g.nz);
-        k_forces_f4<T><<<forces_grid(g), forces_block(g), 0, c->stream>>>(g, idx, idy, idz, S.U, f.phi64,
-                                                                           reinterpret_cast<T *>(f.F4), nullptr,
-                                                                           nullptr);
+        k_forces_f4<T><<<forces_grid(g, kForceRows), forces_block(g), 0, c->stream>>>(
+            g, idx, idy, idz, S.U, f.phi64, reinterpret_cast<T *>(f.F4), nullptr, nullptr, kForceRows, nullptr);
     }
     if (c->total > 0)
         k_close_kick<T><<<nblk(c->total, 256), 256, 0, c->stream>>>(g, c->protons, c->total, S.x, S.y, S.z, S.kx, S.ky,

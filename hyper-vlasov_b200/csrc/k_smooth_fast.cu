@@ -369,6 +369,8 @@ struct FftArgs {
     const float *khat;           // G: spectrum x term / G, z in bit-reversed order
     const float2 *tw;            // kFMaxN / 2 twiddles exp(-2 pi i m / kFMaxN)
     int *edge;                   // [nx]: nonzero densities within the stencil of a face, per x plane
+    unsigned *occ;               // 128^3 forward pass: [2][nx] row-group occupancy of the raw
+                                 // densities (bit q: rows 4q..4q+3), null when not wanted
     float post;                  // current term / the term folded into khat
 };
 
@@ -668,25 +670,38 @@ __device__ __forceinline__ void load_tw128(const float2 *tw64, float2 *tw) {
 // Pass 1 at 128^3, per x plane: forward along y (lines are z columns, loaded
 // straight from the densities: consecutive lanes, consecutive z), then along
 // z (lines are rows of the shared plane), stored through the plane so that
-// the store is coalesced.  Flags density within the stencil of a face.
+// the store is coalesced.  Flags density within the stencil of a face, and
+// records which groups of four y rows of the plane hold raw density of each
+// species (the forces kernel computes only those).
 __global__ void __launch_bounds__(kFThreads, 1) k_fft128_plane_fwd(const __grid_constant__ FftArgs a) {
     extern __shared__ __align__(16) float2 fs[];  // 128 rows of kFRow
     __shared__ float2 tw[kF128];
+    __shared__ unsigned s_occ[2];
     const int x = blockIdx.x, tid = threadIdx.x, line = tid & 127, j = tid >> 7, P = kF128 * kF128;
     load_tw128(a.tw, tw);
+    if (tid < 2) s_occ[tid] = 0u;
     const float *sp = a.src + (long long)x * P, *sn = sp + a.G;
     const bool zx_edge = x < a.A || x >= kF128 - a.A || line < a.W || line >= kF128 - a.W;
     int edge = 0;
+    // row groups y / 4 holding nonzero values of the warp's rows (a warp
+    // shares j, so its rows are those of every lane: warp-uniform masks)
+    unsigned op = 0u, on = 0u;
     float2 r[16];
 #pragma unroll
     for (int c = 0; c < 16; c++) {
         const int y = j + 8 * c;
         const float rp = __ldg(sp + y * kF128 + line), rn = __ldg(sn + y * kF128 + line);
         if ((rp != 0.0f || rn != 0.0f) && (zx_edge || y < a.B || y >= kF128 - a.B)) edge = 1;
+        if (__any_sync(0xffffffffu, rp != 0.0f)) op |= 1u << (y >> 2);
+        if (__any_sync(0xffffffffu, rn != 0.0f)) on |= 1u << (y >> 2);
         r[c] = make_float2(rp, rn);
     }
-    edge = __syncthreads_or(edge);  // also publishes tw
+    edge = __syncthreads_or(edge);  // also publishes tw and the cleared s_occ
     if (tid == 0) a.edge[x] = edge;
+    if (a.occ && (tid & 31) == 0) {
+        if (op) atomicOr(&s_occ[0], op);
+        if (on) atomicOr(&s_occ[1], on);
+    }
     fft128_line(r, j, fs + line, kFRow, tw);  // r[c] = V[ky = j + 8c][z = line]
     __syncthreads();
 #pragma unroll
@@ -701,6 +716,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fft128_plane_fwd(const __grid_
     __syncthreads();
     float2 *out = a.work + (long long)x * P;
     for (int e = tid; e < P; e += kFThreads) out[e] = fs[(e >> 7) * kFRow + (e & 127)];
+    if (a.occ && tid < 2) a.occ[tid * kF128 + x] = s_occ[tid];  // complete: barriers since the atomics
 }
 
 // Pass 2 at 128^3, per y: forward along x (lines are z columns, loaded and
@@ -928,6 +944,7 @@ hv_status smooth_fast_plan(hv_ctx *c) {
     HV_CUDA(cudaMalloc((void **)&f.khat, sizeof(float) * gg.G));
     HV_CUDA(cudaMalloc(&f.tw, sizeof(float2) * tw.size()));
     HV_CUDA(cudaMalloc((void **)&f.edge, sizeof(int) * nx));
+    HV_CUDA(cudaMalloc((void **)&f.occ, sizeof(unsigned) * 2 * nx));
     // the wrap correction's particle list
     HV_CUDA(cudaMalloc(&f.wlist, sizeof(float4) * kWrapParticles));
     // copies ordered on the context stream before the kernels that read
@@ -967,7 +984,7 @@ hv_status smooth_fast_plan(hv_ctx *c) {
 
 void smooth_fast_release(hv_ctx *c) {
     SmoothFast &f = c->fused.smooth;
-    void *ptrs[] = {f.fwork, f.khat, f.tw, f.edge, f.wlist};
+    void *ptrs[] = {f.fwork, f.khat, f.tw, f.edge, f.occ, f.wlist};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     f = SmoothFast();
@@ -1027,6 +1044,7 @@ hv_status smooth_fast_launch(hv_ctx *c, const float *rho_raw, float *rho, const 
         q.khat = f.khat;
         q.tw = reinterpret_cast<const float2 *>(f.tw);
         q.edge = f.edge;
+        q.occ = f.fft128 ? f.occ : nullptr;
         q.post = (float)(term / f.fft_term);
         a.edge = f.edge;
         // the wrap correction (in the march kernel's launch): the particle
