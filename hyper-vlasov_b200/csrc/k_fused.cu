@@ -35,7 +35,7 @@ constexpr int kPBlockMax = 512;   // largest of the autotuner's candidates
 constexpr int kPGridMax = 16;     // most blocks per SM of the particle step
 constexpr int kForceRows = 8;     // y rows per thread of the forces kernel on every row
 constexpr int kForceRowsGated = 4; // the same where only rows holding raw density are computed:
-                                   // shorter walks, as only about a fifth of the blocks work
+                                   // shorter walks, as few blocks work (an eighth on 208Pb 128^3)
 constexpr int kRing = 64;  // observable rows kept on the device
 
 // control words (Fused::ctl)
@@ -546,8 +546,8 @@ inline long long skyrme_threads(long long G) {
 // reads.  A gather weights the force at a node by the same CIC weight the
 // deposit of that position added to the node, so the only forces read with a
 // nonzero weight are those at nodes of nonzero raw density.  A block whose
-// rows hold no raw density (most of the grid: the nucleus covers about a
-// fifth of the rows of 208Pb on 128^3) leaves its forces as they were; the
+// rows hold no raw density (most of the grid: 12.8 % of the groups of four
+// rows hold density on 208Pb 2.08 M, 128^3) leaves its forces as they were; the
 // gather multiplies any such finite value by a zero weight.  The end of a run
 // computes every row again for the plain-path view of the fields (raw null).
 // occ (128^3 FFT smoothing, rows = 4): the same test, already made by the

@@ -336,8 +336,8 @@ def test_fused_runs_continue_across_calls_and_paths(hv):
 def test_forces_on_the_gathered_rows_only_keep_the_run(hv):
     """A float step with the atomic deposit computes the forces only on the
     row groups of the grid that hold raw density, the nodes its particles'
-    next gather reads with a nonzero weight (208Pb on 128^3: the nucleus
-    covers about a fifth of the rows); the end of a run computes every row
+    next gather reads with a nonzero weight (208Pb on 128^3: about an
+    eighth of the row groups hold density); the end of a run computes every row
     again for the plain-path view.  Twelve runs of one step each (every
     gather reading forces computed on every row) and one run of twelve steps
     give D(t) and particles equal to float rounding of the atomic deposit's
