@@ -230,6 +230,18 @@ def step_bytes(w, n_sor, wordsize=4, checks=2, touched=None, force_frac=None):
     }
 
 
+def row_group_fraction(raw, n, rows=4):
+    """Share of the forces kernel's work items that hold raw density: per
+    species and x plane, groups of `rows` consecutive y rows (the last group
+    shorter when n is not a multiple), a group counting when any node of its
+    rows has nonzero raw density.  raw: both species' n^3 grids, stacked."""
+    import numpy as np
+    occupied = np.any(np.asarray(raw).reshape(2, n, n, n) != 0, axis=3)
+    pad = (-n) % rows
+    groups = np.any(np.pad(occupied, ((0, 0), (0, 0), (0, pad))).reshape(2, n, -1, rows), axis=3)
+    return float(np.mean(groups))
+
+
 # ---------------------------------------------------------------- CPU arm
 def inputs_digest(arrays):
     """sha256 (first 16 hex digits) of the six input arrays' bytes, in order:
@@ -858,10 +870,8 @@ def our_arm(args, world, rank, local):
     # float steps) that hold any of them are the ones it computes
     raw = sess.download_field(hv.HV_FIELD_DENSITY_RAW)
     touched = int(np.count_nonzero(raw))
-    rows = np.any(raw.reshape(2, w.n, w.n, w.n) != 0, axis=3)
-    pad = (-w.n) % 4
-    groups = np.any(np.pad(rows, ((0, 0), (0, 0), (0, pad))).reshape(2, w.n, -1, 4), axis=3)
-    force_frac = float(np.mean(groups)) if (prec == hv.HV_F32 and w.deposit_mode != hv.HV_DEPOSIT_SORTED) else None
+    gated = prec == hv.HV_F32 and w.deposit_mode != hv.HV_DEPOSIT_SORTED
+    force_frac = row_group_fraction(raw, w.n, 4) if gated else None
     nbytes = step_bytes(w, its_p.mean(), ws_, float(np.mean([sor_checks(n, per_cycle) for n in its_p])),
                         touched=touched, force_frac=force_frac)
     tot_ms = sum(v[0] for v in kt.values())
