@@ -4,8 +4,9 @@
 
 One step = one time step of the 208Pb / 2.08M test particle / 128^3 (h = 0.25
 fm, dt = 0.2 fm/c) workload: CIC deposit, smoothing, Skyrme potential,
-red-black SOR Coulomb solve (omega 1.8 to relative residual 1e-6), forces,
-gather, leapfrog and the D(t) observables.  Inputs are synthetic (seeded
+red-black SOR Coulomb solve to relative residual 1e-6 (coarse-grid corrected
+cycles whose sweeps relax at omega 1.7; plain cycles at the workload's 1.8),
+forces, gather, leapfrog and the D(t) observables.  Inputs are synthetic (seeded
 uniform-sphere nucleus), resident on the device before timing.
 
 Our arm (default) prints one JSON line with:
@@ -80,6 +81,11 @@ def parse():
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--warm-start", choices=["previous", "extrapolate", "quadratic"], default="quadratic")
     ap.add_argument("--sor-exchange", choices=["auto", "flags"], default="auto")
+    ap.add_argument("--coarse-sweeps", type=int, default=0,
+                    help="red+black sweeps after each coarse-grid correction in the headline's session "
+                         "(0: the library's default, 12; e2e and the other legs keep the default)")
+    ap.add_argument("--coarse-omega", type=float, default=0.0,
+                    help="their relaxation in the headline's session (0: the library's default, 1.7)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -827,6 +833,10 @@ def our_arm(args, world, rank, local):
     sess = hv.Session.from_workload(w, prec, device=local)
     sess.set_fast_options(sor_warm_start=warm_mode, sor_exchange=hv.HV_SOR_EXCHANGE_FLAGS
                           if args.sor_exchange == "flags" else hv.HV_SOR_EXCHANGE_AUTO)
+    if args.coarse_sweeps > 0:
+        sess.set_fast_options(sor_coarse_sweeps=args.coarse_sweeps)
+    if args.coarse_omega > 0:
+        sess.set_fast_options(sor_coarse_omega=args.coarse_omega)
     sess.upload_particles(*parts)
     stream = torch.cuda.ExternalStream(sess.stream())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -956,7 +966,11 @@ def our_arm(args, world, rank, local):
         "dtype": args.precision, "data": "synthetic",
         "config": {"workload": w.name, "nucleus": f"208Pb (Z={w.Z}, N={w.N})", "particles": w.particles,
                    "grid": f"{w.n}^3", "h_fm": w.h, "dt_fm_c": w.dt,
-                   "sor": f"red-black omega {w.sor_omega} to relative residual {w.sor_tol:g}",
+                   "sor": (f"red-black SOR to relative residual {w.sor_tol:g} (FP64 test): omega {w.sor_omega} in "
+                           f"plain cycles; each coarse-grid corrected cycle smooths with {fo.sor_coarse_sweeps} "
+                           f"sweeps at omega {fo.sor_coarse_omega if fo.sor_coarse_omega > 0 else 1.7:g}"
+                           if (fo.sor_coarse and prec == hv.HV_F32) else
+                           f"red-black omega {w.sor_omega} to relative residual {w.sor_tol:g}"),
                    "warm_start": args.warm_start, "sor_exchange": args.sor_exchange, "path": "fused",
                    "precision": "f32 particles/grids, f64 phi, SOR residual and observable sums",
                    "parallelism": f"replicas x{world}",

@@ -796,8 +796,9 @@ void hv_fast_options_default(hv_fast_options *o) {
     o->sor_omega = 0.0;
     o->sor_wait_limit = 0;
     o->sor_coarse = 1;
-    o->sor_coarse_sweeps = 16;
+    o->sor_coarse_sweeps = 12;
     o->deposit_aggregate = 1;
+    o->sor_coarse_omega = 0.0;
 }
 
 hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
@@ -814,6 +815,8 @@ hv_status hv_ctx_set_fast_options(hv_ctx *c, const hv_fast_options *o) {
     if (o->sor_coarse < 0 || o->sor_coarse > 1 || o->sor_coarse_sweeps < 1 || o->sor_coarse_sweeps > 4096)
         return HV_ERR_BAD_ARG;
     if (o->deposit_aggregate < 0 || o->deposit_aggregate > 1) return HV_ERR_BAD_ARG;
+    if (!(o->sor_coarse_omega == 0.0 || (o->sor_coarse_omega > 0.0 && o->sor_coarse_omega < 2.0)))
+        return HV_ERR_BAD_ARG;
     HV_CUDA(cudaSetDevice(c->device));
     HV_CUDA(cudaStreamSynchronize(c->stream));
     if (c->fused.graph) {

@@ -49,6 +49,13 @@ namespace hv {
 namespace {
 
 constexpr int kSorThreads = 1024;
+// relaxation of the sweeps after each coarse-grid correction (default of
+// hv_fast_options.sor_coarse_omega).  In a NumPy model of the kernel's cycle
+// on successive 208Pb densities (quadratic start, rule 1e-6), 12 sweeps at
+// 1.7 ended every solve in two cycles on 48^3, 64^3, 96^3 and 128^3 grids
+// (final residual 2.3e-7 to 4.8e-7), where 16 sweeps at 1.8 took two cycles
+// at 128^3 (2.9e-7) and three elsewhere, and 12 at 1.8 took three.
+constexpr double kCoarseOmega = 1.7;
 // default bounds of the device-side waits (hv_fast_options.sor_wait_limit
 // replaces both): polls of a grid barrier or a neighbour's phase counter before
 // the wait gives up (~1 s), and polls of one tagged mirror entry
@@ -1719,6 +1726,20 @@ hv_status sor_fast_replan_rank(hv_ctx *c, int rank, int *count) {
 // The arguments of one solve and its kernel form: 0 phase counters, 1 the
 // generic tagged sweep, 2 and 3 the staged sweep for at most (1, 1, 2) and
 // (2, 1, 3) inner / perimeter / ghost quads per thread.
+// The update's coefficients for the cycles the arguments run: the sweeps of
+// a coarse-corrected cycle smooth what the coarse solve leaves (kCoarseOmega
+// unless set); plain cycles relax at the run's omega (or its override).
+template <typename T, typename S>
+static void set_relaxation(const hv_ctx *c, SorArgs<T, S> &a) {
+    const double omega = a.coarse ? (c->fast.sor_coarse_omega > 0.0 ? c->fast.sor_coarse_omega : kCoarseOmega)
+                                  : (c->fast.sor_omega > 0.0 ? c->fast.sor_omega : c->params.sor.omega);
+    a.cx = (S)(omega * a.dhx2i / a.ddiag);
+    a.cy = (S)(omega * a.dhy2i / a.ddiag);
+    a.cz = (S)(omega * a.dhz2i / a.ddiag);
+    a.cself = (S)(1.0 - omega);
+    a.src_scale = omega / a.ddiag;
+}
+
 template <typename T>
 static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, SorArgs<T, T> &a) {
     using S = T;
@@ -1745,12 +1766,6 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.dhy2i = 1.0 / (dy * dy);
     a.dhz2i = 1.0 / (dz * dz);
     a.ddiag = 2.0 * (a.dhx2i + a.dhy2i + a.dhz2i);
-    const double omega = c->fast.sor_omega > 0.0 ? c->fast.sor_omega : sp.omega;
-    a.cx = (S)(omega * a.dhx2i / a.ddiag);
-    a.cy = (S)(omega * a.dhy2i / a.ddiag);
-    a.cz = (S)(omega * a.dhz2i / a.ddiag);
-    a.cself = (S)(1.0 - omega);
-    a.src_scale = omega / a.ddiag;
     a.src_c = 4.0 * kPi * kE2;
     a.tol = sp.tol;
     a.max_iter = sp.max_iter;
@@ -1802,6 +1817,7 @@ static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int r
     a.hx = dx;
     a.hy = dy;
     a.hz = dz;
+    set_relaxation(c, a);
     return form;
 }
 
@@ -1884,7 +1900,10 @@ hv_status sor_wave_build(SorWave &w, const std::vector<hv_ctx *> &cs, const std:
     // the coarse-grid correction needs the staged sweep (its ghost buffer and
     // row tables); a wave of generic tagged sweeps runs plain cycles
     if (form == 1)
-        for (auto &a : args) a.coarse = 0;
+        for (int i = 0; i < n; i++) {
+            args[i].coarse = 0;
+            set_relaxation(cs[i], args[i]);
+        }
     int dev = 0;
     HV_CUDA(cudaGetDevice(&dev));
     cudaDeviceProp prop;

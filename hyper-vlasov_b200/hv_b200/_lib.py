@@ -67,7 +67,8 @@ class hv_fast_options(C.Structure):
     _fields_ = [("sor_warm_start", C.c_int), ("sor_inner_min", C.c_int), ("sor_inner_max", C.c_int),
                 ("sort_every", C.c_int), ("graph_steps", C.c_int), ("sor_exchange", C.c_int),
                 ("smooth_fft", C.c_int), ("sor_omega", C.c_double), ("sor_wait_limit", C.c_int),
-                ("sor_coarse", C.c_int), ("sor_coarse_sweeps", C.c_int), ("deposit_aggregate", C.c_int)]
+                ("sor_coarse", C.c_int), ("sor_coarse_sweeps", C.c_int), ("deposit_aggregate", C.c_int),
+                ("sor_coarse_omega", C.c_double)]
 
 
 HV_WARM_PREVIOUS = 0

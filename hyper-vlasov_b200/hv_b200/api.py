@@ -123,12 +123,13 @@ class Session:
     def set_fast_options(self, **kw):
         """Updates fields of hv_fast_options (sor_warm_start, sor_inner_min,
         sor_inner_max, sort_every, graph_steps, sor_exchange, smooth_fft, sor_omega,
-        sor_wait_limit, sor_coarse, sor_coarse_sweeps, deposit_aggregate)."""
+        sor_wait_limit, sor_coarse, sor_coarse_sweeps, deposit_aggregate,
+        sor_coarse_omega)."""
         o = self.fast_options()
         for k, v in kw.items():
             if not hasattr(o, k):
                 raise KeyError(k)
-            setattr(o, k, float(v) if k == "sor_omega" else int(v))
+            setattr(o, k, float(v) if k in ("sor_omega", "sor_coarse_omega") else int(v))
         L.check(self.lib.hv_ctx_set_fast_options(self._ctx, C.byref(o)), "hv_ctx_set_fast_options")
 
     def autotune(self, trial_steps=4):

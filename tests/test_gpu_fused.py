@@ -138,6 +138,40 @@ def test_first_steps_after_the_fused_initial_solve_start_from_solutions(hv):
     assert quad[1:].sum() < prev[1:].sum(), (quad, prev)
 
 
+@pytest.mark.parametrize("wname", ["208Pb-20.8k-128^3", "208Pb-104k-64^3"])
+def test_coarse_cycle_relaxation_keeps_the_rule_with_fewer_iterations(hv, wname):
+    """The sweeps after each coarse-grid correction relax at
+    hv_fast_options.sor_coarse_omega (default 1.7, 12 sweeps a cycle), not at
+    the run's omega: each cycle then removes at least as much of the residual
+    as 16 sweeps at the run's 1.8 did, so the solves end at the same FP64
+    rule in no more iterations.  D(t) and the Coulomb potential of the two
+    settings agree within 1e-6 relative, the tolerance of each solve."""
+    w = hv.WORKLOADS[wname]
+    p32 = hv.workload_particles(w, np.float32)
+    res = []
+    for opts in ({}, dict(sor_coarse_sweeps=16, sor_coarse_omega=w.sor_omega)):
+        with hv.Session.from_workload(w, hv.HV_F32) as s:
+            if opts:
+                s.set_fast_options(**opts)
+            fo = s.fast_options()
+            s.upload_particles(*p32)
+            s.initial_solve()
+            obs = s.run(10, hv.HV_PATH_FUSED)
+            res.append((fo, obs, s.download_field(hv.HV_FIELD_COULOMB)))
+    (f0, o0, c0), (f1, o1, c1) = res
+    assert f0.sor_coarse_sweeps == 12 and f0.sor_coarse_omega == 0.0
+    assert f1.sor_coarse_sweeps == 16 and f1.sor_coarse_omega == w.sor_omega
+    assert not np.any(o0["flags"] & 1) and not np.any(o1["flags"] & 1)
+    assert o0["sor_iterations"][2:].sum() <= o1["sor_iterations"][2:].sum(), (o0["sor_iterations"],
+                                                                             o1["sor_iterations"])
+    assert max_rel(o0["dipole"], o1["dipole"]) < 1e-6, max_rel(o0["dipole"], o1["dipole"])
+    assert max_rel(c0, c1) < 1e-6, max_rel(c0, c1)
+    with hv.Session.from_workload(w, hv.HV_F32) as s:
+        for bad in (-0.5, 2.0, 2.5):
+            with pytest.raises(hv.HVError):
+                s.set_fast_options(sor_coarse_omega=bad)
+
+
 def test_sor_omega_override_keeps_the_stopping_rule(hv):
     """hv_fast_options.sor_omega relaxes the fused sweeps differently; the
     FP64 residual test is unchanged, so D(t) stays within the float path's
