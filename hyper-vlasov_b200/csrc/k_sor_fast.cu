@@ -1723,9 +1723,6 @@ hv_status sor_fast_replan_rank(hv_ctx *c, int rank, int *count) {
     return st;
 }
 
-// The arguments of one solve and its kernel form: 0 phase counters, 1 the
-// generic tagged sweep, 2 and 3 the staged sweep for at most (1, 1, 2) and
-// (2, 1, 3) inner / perimeter / ghost quads per thread.
 // The update's coefficients for the cycles the arguments run: the sweeps of
 // a coarse-corrected cycle smooth what the coarse solve leaves (kCoarseOmega
 // unless set); plain cycles relax at the run's omega (or its override).
@@ -1740,6 +1737,9 @@ static void set_relaxation(const hv_ctx *c, SorArgs<T, S> &a) {
     a.src_scale = omega / a.ddiag;
 }
 
+// The arguments of one solve and its kernel form: 0 phase counters, 1 the
+// generic tagged sweep, 2 and 3 the staged sweep for at most (1, 1, 2) and
+// (2, 1, 3) inner / perimeter / ghost quads per thread.
 template <typename T>
 static int sor_fast_args(hv_ctx *c, const T *rho, int *ctl, int *its_ring, int ring, SorArgs<T, T> &a) {
     using S = T;
