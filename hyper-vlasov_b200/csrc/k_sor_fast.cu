@@ -54,7 +54,8 @@ constexpr int kSorThreads = 1024;
 // on successive 208Pb densities (quadratic start, rule 1e-6), 12 sweeps at
 // 1.7 ended every solve in two cycles on 48^3, 64^3, 96^3 and 128^3 grids
 // (final residual 2.3e-7 to 4.8e-7), where 16 sweeps at 1.8 took two cycles
-// at 128^3 (2.9e-7) and three elsewhere, and 12 at 1.8 took three.
+// at 128^3 (2.9e-7) and three on the other grids; measured on the GPU at
+// 128^3, 13 sweeps at 1.8 took three cycles in 999 of 1000 solves.
 constexpr double kCoarseOmega = 1.7;
 // default bounds of the device-side waits (hv_fast_options.sor_wait_limit
 // replaces both): polls of a grid barrier or a neighbour's phase counter before
