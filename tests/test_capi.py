@@ -103,6 +103,22 @@ def test_parameter_helpers(hv):
     assert lib.hv_version().startswith(b"hv_b200")
 
 
+def test_fast_option_defaults(hv):
+    """hv_fast_options_default gives the documented defaults of the fused
+    path (host only: no device needed)."""
+    from hv_b200 import _lib
+    lib = _lib.load()
+    o = _lib.hv_fast_options()
+    lib.hv_fast_options_default(C.byref(o))
+    assert o.sor_warm_start == _lib.HV_WARM_QUADRATIC
+    assert (o.sor_inner_min, o.sor_inner_max, o.sort_every, o.graph_steps) == (8, 256, 16, 8)
+    assert o.sor_exchange == _lib.HV_SOR_EXCHANGE_AUTO and o.smooth_fft == 1
+    assert o.sor_omega == 0.0 and o.sor_wait_limit == 0
+    # coarse-corrected cycles: 12 sweeps at the default relaxation (0: 1.7)
+    assert (o.sor_coarse, o.sor_coarse_sweeps, o.sor_coarse_omega) == (1, 12, 0.0)
+    assert o.deposit_aggregate == 1
+
+
 def test_workload_definitions(hv):
     w = hv.PB208_2M
     assert w.particles == 2_080_000 and w.n == 128 and w.h == 0.25 and w.d_max == 16.0
